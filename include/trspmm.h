@@ -1,0 +1,228 @@
+/*
+ * trspmm.h — C ABI of the B200-native routed FP16 SpMM library (libtrspmm.so).
+ *
+ * C = A·B with A a sparse adjacency in CSR (int32 indices), B a dense
+ * row-major FP16 feature matrix (n_cols x K), FP32 accumulation.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (TR_OK == 0); on failure
+ *    tr_last_error() returns a message for the calling thread.  Nothing
+ *    aborts the process and no device-side trap is used.
+ *  - "host" pointers are CPU memory; "device" pointers are CUDA device
+ *    memory of the current device.  `stream` is a cudaStream_t (NULL = the
+ *    legacy default stream).
+ *  - FP16 data is passed as uint16_t bit patterns (IEEE binary16).
+ *  - Device entry points never synchronise the stream and never allocate,
+ *    except where noted (plan construction, the reference-compatible host
+ *    entry points).
+ */
+#ifndef TRSPMM_H
+#define TRSPMM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  TR_OK = 0,
+  TR_ERR_ARG = 1,          /* invalid argument / malformed CSR or tables */
+  TR_ERR_CUDA = 2,         /* CUDA runtime error */
+  TR_ERR_TIMEOUT = 3,      /* a bounded device wait gave up (kernel returned early) */
+  TR_ERR_NOMEM = 4,
+  TR_ERR_UNSUPPORTED = 5   /* shape/alignment outside what the kernels implement */
+};
+
+enum { TR_OUT_F32 = 0, TR_OUT_F16 = 1 };
+
+/* Route-mask bits for tr_spmm_routed (all set = full product). */
+enum { TR_ROUTE_TC = 1, TR_ROUTE_SPTC = 2, TR_ROUTE_CUDA = 4, TR_ROUTE_ALL = 7 };
+
+const char* tr_last_error(void);
+int tr_version(void);
+/* Number of SMs and whether the tcgen05 path can run on the current device. */
+int tr_device_info(int* num_sms, int* cc_major, int* cc_minor);
+
+/* ------------------------------------------------------------------------
+ * Router: three-stage funnel (dense TC columns, 2:4 SPTC groups, CUDA-core
+ * residual) over 16-row windows.
+ * Replaces Libra5BlockOnline.block_sptc_2to4_online
+ * (TR-source/Block/block_online.cpp:545-549, return list :844-870).
+ * mode TR_ROUTE_COMPAT reproduces the reference's 29 tables bit for bit,
+ * including its per-row two-slot truncation of SPTC groups; TR_ROUTE_EXACT
+ * makes the same decisions but moves every truncated entry into the CUDA
+ * residual so the tables encode A exactly.
+ * ---------------------------------------------------------------------- */
+enum { TR_ROUTE_COMPAT = 0, TR_ROUTE_EXACT = 1 };
+
+typedef struct tr_route_params {
+  int32_t partsize_t;      /* TC sub-blocks per part (32) */
+  int32_t partsize_c;      /* CUDA nnz per part (32) */
+  int32_t shortsize;       /* CUDA "short" part limit (3) */
+  int32_t density;         /* TC column threshold (8) */
+  int32_t window;          /* rows per window, 1..16 (16) */
+  int32_t wide;            /* range-checked only, as in the reference */
+  float tc_min_util;       /* (0.0) */
+  float sptc_min_util;     /* accepted, unused (reference block_online.cpp:548) */
+  int32_t sptc_threshold;  /* accepted, unused (reference block_online.cpp:549) */
+  int32_t unit_min_nnz;    /* LIBRA_SPTC_UNIT_MIN_NNZ (2) */
+  int32_t skip_tc;         /* LIBRA_SKIP_TC (0) */
+  int32_t mode;            /* TR_ROUTE_COMPAT / TR_ROUTE_EXACT */
+  int32_t threads;         /* host threads, <= 0 = all */
+} tr_route_params;
+
+typedef struct tr_route tr_route;
+
+/* host: indptr[n_rows+1], indices[nnz], values[nnz] */
+int tr_route_build(const int32_t* indptr, const int32_t* indices, const float* values,
+                   int32_t n_rows, const tr_route_params* params, tr_route** out);
+/* Table idx in the reference's return order (0..28); `count` is in elements. */
+int tr_route_table(const tr_route* r, int idx, const void** data, int64_t* count);
+/* Seconds spent building the tables (the reference's 30th return). */
+double tr_route_seconds(const tr_route* r);
+void tr_route_free(tr_route* r);
+
+/* ------------------------------------------------------------------------
+ * Device plan: the routed operand laid out for the fused sm_100a kernel.
+ * Built once per graph (on the host from route tables, uploaded), reused
+ * by every forward / adjoint call.
+ * ---------------------------------------------------------------------- */
+typedef struct tr_plan tr_plan;
+
+typedef struct tr_plan_info {
+  int32_t n_rows, n_cols, n_windows;
+  int64_t nnz;             /* entries the plan multiplies */
+  int64_t tc_tiles;        /* 16x16 tensor-core tiles from the dense route */
+  int64_t sptc_tiles;      /* 16x16 2:4 tiles from the SPTC route */
+  int64_t residual_nnz;    /* CUDA-core entries */
+  int64_t device_bytes;    /* plan footprint in HBM */
+} tr_plan_info;
+
+/* Host route tables (pointer + element count each), in the reference's
+ * order; the pointers may be NULL when the count is 0. */
+typedef struct tr_tables {
+  const int32_t* t_row_offset;   int64_t n_t_row_offset;
+  const int32_t* t_block_offset; int64_t n_t_block_offset;
+  const int32_t* t_column;       int64_t n_t_column;
+  const uint16_t* t_value;       int64_t n_t_value;       /* FP16 */
+  const int32_t* t_window_row;   int64_t n_t_window_row;
+  const int64_t* t_binary;       int64_t n_t_binary;
+  const int32_t* c_row_offset;   int64_t n_c_row_offset;
+  const int32_t* c_row;          int64_t n_c_row;
+  const int32_t* c_column;       int64_t n_c_column;
+  const uint16_t* c_value;       int64_t n_c_value;       /* FP16 */
+  const int32_t* cs_row_offset;  int64_t n_cs_row_offset;
+  const int32_t* cs_row;         int64_t n_cs_row;
+  const int32_t* cs_column;      int64_t n_cs_column;
+  const uint16_t* cs_value;      int64_t n_cs_value;      /* FP16 */
+  const int32_t* s_tile_column;  int64_t n_s_tile_column; /* [tiles*16] */
+  const uint32_t* s_packed_a;    int64_t n_s_packed_a;    /* [tiles*64] half2 words */
+  const uint32_t* s_packed_meta; int64_t n_s_packed_meta; /* [tiles*8] */
+  const int32_t* s_window_tile_offset; int64_t n_s_window_tile_offset; /* [windows+1] */
+} tr_tables;
+
+int tr_plan_from_tables(const tr_tables* t, int32_t n_rows, int32_t n_cols, int32_t window,
+                        tr_plan** out);
+/* Route a CSR with this library's own router (exact mode) and build the
+ * plan in one step.  `values` are FP32 (rounded to FP16 in the plan). */
+int tr_plan_from_csr(const int32_t* indptr, const int32_t* indices, const float* values,
+                     int32_t n_rows, int32_t n_cols, const tr_route_params* params,
+                     tr_plan** out);
+int tr_plan_info_get(const tr_plan* p, tr_plan_info* info);
+void tr_plan_free(tr_plan* p);
+
+/* ------------------------------------------------------------------------
+ * Device compute (no allocation, no synchronisation).
+ * ---------------------------------------------------------------------- */
+
+/* Plain single-route CSR SpMM on CUDA cores (the baseline every routed
+ * number is compared with).  device: indptr[m+1], indices[nnz],
+ * values[nnz] FP16, b[n_cols*k] FP16, c[m*k] FP32 or FP16. */
+int tr_spmm_csr(const int32_t* indptr, const int32_t* indices, const uint16_t* values,
+                int32_t m, int32_t n_cols, int64_t nnz, const uint16_t* b, int32_t k,
+                void* c, int c_dtype, void* stream);
+
+/* Routed forward: C = A_plan · B.  route_mask restricts the routes computed
+ * (for per-route timing); C rows of the plan are fully overwritten. */
+int tr_spmm_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_dtype,
+                   int route_mask, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Reference-compatible entry points (host tensors in, FP32 host out; device
+ * memory allocated, copied and freed inside each call; `epoches` timed
+ * launches averaged as the reference does).
+ * ---------------------------------------------------------------------- */
+
+/* Replaces Libra6SpMMOnline.forward_fp16_tcu_cuda_sptc_mma_parallel_online
+ * (TR-source/SpMM/mGCN_online.cpp:760-800, returns :1130-1137).
+ * ms_out[0..4] = total, tc, cuda_long, cuda_short, sptc (average per epoch). */
+int tr_forward_fp16_tcu_cuda_sptc_mma_parallel_online(
+    const int32_t* t_row_offset, int64_t n_t_row_offset,
+    const int32_t* t_block_offset, int64_t n_t_block_offset,
+    const int32_t* t_column, int64_t n_t_column,
+    const uint16_t* t_value, int64_t n_t_value,
+    const int32_t* t_window_row, int64_t n_t_window_row,
+    const int32_t* t_atomic, int64_t n_t_atomic,
+    const int64_t* t_binary, int64_t n_t_binary,
+    const int32_t* c_row_offset, int64_t n_c_row_offset,
+    const int32_t* c_row, int64_t n_c_row,
+    const int32_t* c_atomic, int64_t n_c_atomic,
+    const int32_t* c_column, int64_t n_c_column,
+    const uint16_t* c_value, int64_t n_c_value,
+    const int32_t* c_row_offset_short, int64_t n_c_row_offset_short,
+    const int32_t* c_row_short, int64_t n_c_row_short,
+    const int32_t* c_atomic_short, int64_t n_c_atomic_short,
+    const int32_t* c_column_short, int64_t n_c_column_short,
+    const uint16_t* c_value_short, int64_t n_c_value_short,
+    const int32_t* s_column, int64_t n_s_column,
+    const float* s_value, int64_t n_s_value,
+    const int8_t* s_pos, int64_t n_s_pos,
+    const int32_t* s_offsets, int64_t n_s_offsets,
+    const int32_t* s_tile_window, int64_t n_s_tile_window,
+    const int32_t* s_tile_column, int64_t n_s_tile_column,
+    const int32_t* s_packed_a, int64_t n_s_packed_a,
+    const int32_t* s_packed_meta, int64_t n_s_packed_meta,
+    const int32_t* s_window_tile_offset, int64_t n_s_window_tile_offset,
+    const uint16_t* rhs_matrix, int64_t n_rhs_matrix,
+    int32_t parts_t, int32_t parts_c, int32_t partsize_c, int32_t parts_c_short,
+    int32_t window, int32_t dimN, int32_t mOri, int32_t kOri, int32_t epoches,
+    float* out, float* ms_out);
+
+/* Replaces Libra6SpMMOnline.forward_fp16_sptc_online (mGCN_online.cpp:202-400):
+ * the SPTC route alone from the unpacked group tables. */
+int tr_forward_fp16_sptc_online(
+    const int32_t* s_column, int64_t n_s_column,
+    const float* s_value, int64_t n_s_value,
+    const int8_t* s_pos, int64_t n_s_pos,
+    const int32_t* s_window, int64_t n_s_window,
+    const uint16_t* rhs_matrix, int64_t n_rhs_matrix,
+    int32_t window, int32_t dimN, int32_t mOri, int32_t kOri, int32_t epoches,
+    float* out, float* ms_out);
+
+/* Replaces Libra6SpMMOnline.forward_fp16_sptc_mma_online (mGCN_online.cpp:404-652):
+ * the SPTC route from the unpacked group tables plus per-window group offsets. */
+int tr_forward_fp16_sptc_mma_online(
+    const int32_t* s_column, int64_t n_s_column,
+    const float* s_value, int64_t n_s_value,
+    const int8_t* s_pos, int64_t n_s_pos,
+    const int32_t* s_offsets, int64_t n_s_offsets,
+    const uint16_t* rhs_matrix, int64_t n_rhs_matrix,
+    int32_t window, int32_t dimN, int32_t mOri, int32_t kOri, int32_t epoches,
+    float* out, float* ms_out);
+
+/* Replaces Libra6SpMMOnline.forward_fp16_sptc_mma_packed_online
+ * (mGCN_online.cpp:654-757): the SPTC route from the packed tiles. */
+int tr_forward_fp16_sptc_mma_packed_online(
+    const int32_t* s_tile_column, int64_t n_s_tile_column,
+    const int32_t* s_packed_a, int64_t n_s_packed_a,
+    const int32_t* s_packed_meta, int64_t n_s_packed_meta,
+    const int32_t* s_window_tile_offset, int64_t n_s_window_tile_offset,
+    const uint16_t* rhs_matrix, int64_t n_rhs_matrix,
+    int32_t window, int32_t dimN, int32_t mOri, int32_t kOri, int32_t epoches,
+    float* out, float* ms_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TRSPMM_H */

@@ -1,0 +1,23 @@
+"""ORACLE — test infrastructure only.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg may
+import this package, and only as the checker.  The shipped library never
+imports it.
+
+Contents
+  route()            CPU restatement of the reference router
+                     (TR-source/Block/block_online.cpp:545-871), via liboracle.so.
+  ref_route()        the reference router itself, compiled from its source into
+                     oracle/_ref (present only where it was built).
+  decode_tables()    rebuilds the matrix the 29 route tables encode (TC bitmap
+                     sub-blocks, SPTC groups, CUDA parts), i.e. the operand the
+                     reference's routed forward multiplies.
+  spmm_f64() / spmm_f16_f32() / sddmm_f64()   CSR arithmetic in C (OpenMP).
+"""
+from .core import (TABLE_NAMES, route, ref_route, ref_available, decode_tables,
+                   decode_sptc_tiles, spmm_f64, spmm_f16_f32, sddmm_f64, max_threads,
+                   lib_path)
+
+__all__ = ["TABLE_NAMES", "route", "ref_route", "ref_available", "decode_tables",
+           "decode_sptc_tiles", "spmm_f64", "spmm_f16_f32", "sddmm_f64", "max_threads",
+           "lib_path"]

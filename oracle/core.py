@@ -1,0 +1,290 @@
+"""ORACLE — test infrastructure only (see oracle/__init__.py)."""
+from __future__ import annotations
+
+import ctypes
+import glob
+import os
+import sys
+import time
+
+import numpy as np
+import scipy.sparse as sp
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+lib_path = os.path.join(HERE, "liboracle.so")
+
+# Return order of block_sptc_2to4_online (TR-source/Block/block_online.cpp:844-870).
+TABLE_NAMES = [
+    "t_row_offset", "t_block_offset", "t_column", "t_value", "t_window_row", "t_atomic",
+    "t_binary",
+    "c_row_offset", "c_row", "c_atomic", "c_column", "c_value",
+    "c_row_offset_short", "c_row_short", "c_atomic_short", "c_column_short", "c_value_short",
+    "s_column", "s_mask", "s_value", "s_pos", "s_window", "s_offsets",
+    "s_tile_window", "s_tile_group", "s_tile_column", "s_packed_a", "s_packed_meta",
+    "s_window_tile_offset", "duration",
+]
+_DTYPES = [np.int32, np.int32, np.int32, np.float32, np.int32, np.int32, np.int64,
+           np.int32, np.int32, np.int32, np.int32, np.float32,
+           np.int32, np.int32, np.int32, np.int32, np.float32,
+           np.int32, np.uint8, np.float32, np.int8, np.int32, np.int32,
+           np.int32, np.int32, np.int32, np.int32, np.int32, np.int32]
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(lib_path):
+            raise RuntimeError(f"oracle library missing: {lib_path} (run make -C oracle)")
+        L = ctypes.CDLL(lib_path)
+        P = ctypes.c_void_p
+        L.oracle_route.restype = P
+        L.oracle_route.argtypes = [P, P, P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                   ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int,
+                                   ctypes.c_int]
+        L.oracle_route_table.restype = ctypes.c_int
+        L.oracle_route_table.argtypes = [P, ctypes.c_int, ctypes.POINTER(P),
+                                         ctypes.POINTER(ctypes.c_long)]
+        L.oracle_route_free.argtypes = [P]
+        L.oracle_spmm_f64.argtypes = [P, P, P, ctypes.c_int, P, ctypes.c_int, P]
+        L.oracle_spmm_f16_f32.argtypes = [P, P, P, ctypes.c_int, P, ctypes.c_int, P, ctypes.c_int]
+        L.oracle_sddmm_f64.argtypes = [P, P, ctypes.c_int, P, P, ctypes.c_int, P]
+        L.oracle_max_threads.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _shape(tabs, window):
+    """Apply the reference's tensor shapes (block_online.cpp:786-792, 863-865)."""
+    g = tabs[21].shape[0]
+    t = tabs[23].shape[0]
+    tabs[17] = tabs[17].reshape(g, 4)
+    tabs[18] = tabs[18].reshape(g, window)
+    tabs[19] = tabs[19].reshape(g, window, 2)
+    tabs[20] = tabs[20].reshape(g, window, 2)
+    tabs[25] = tabs[25].reshape(t, 16)
+    tabs[26] = tabs[26].reshape(t, 8, 4, 2)
+    tabs[27] = tabs[27].reshape(t, 8)
+    return tabs
+
+
+def route(indptr, indices, values, partsize_t=32, partsize_c=32, shortsize=3, density=8,
+          window=16, wide=16, tc_min_util=0.0, sptc_min_util=0.5, sptc_threshold=12,
+          unit_min_nnz=None, skip_tc=None):
+    """Restated router; returns the reference's 30-item list as numpy arrays.
+
+    ``unit_min_nnz`` / ``skip_tc`` default to the reference's environment
+    switches LIBRA_SPTC_UNIT_MIN_NNZ (2) and LIBRA_SKIP_TC (off)
+    (block_online.cpp:564-567).  ``wide``, ``sptc_min_util`` and
+    ``sptc_threshold`` are accepted and unused, as in the reference."""
+    L = _load()
+    if unit_min_nnz is None:
+        unit_min_nnz = int(os.environ.get("LIBRA_SPTC_UNIT_MIN_NNZ", "2"))
+    if skip_tc is None:
+        skip_tc = os.environ.get("LIBRA_SKIP_TC", "0") in ("1", "true", "TRUE")
+    rp = np.ascontiguousarray(indptr, dtype=np.int32)
+    ci = np.ascontiguousarray(indices, dtype=np.int32)
+    vv = np.ascontiguousarray(values, dtype=np.float32)
+    t0 = time.perf_counter()
+    h = L.oracle_route(_ptr(rp), _ptr(ci), _ptr(vv), rp.shape[0] - 1, partsize_t, partsize_c,
+                       shortsize, density, window, float(tc_min_util), int(unit_min_nnz),
+                       int(bool(skip_tc)))
+    if not h:
+        raise ValueError("oracle_route rejected its arguments")
+    dur = time.perf_counter() - t0
+    out = []
+    try:
+        for i, dt in enumerate(_DTYPES):
+            data = ctypes.c_void_p()
+            n = ctypes.c_long()
+            L.oracle_route_table(h, i, ctypes.byref(data), ctypes.byref(n))
+            cnt = n.value // np.dtype(dt).itemsize
+            if cnt == 0:
+                out.append(np.zeros(0, dtype=dt))
+            else:
+                buf = (ctypes.c_char * n.value).from_address(data.value)
+                out.append(np.frombuffer(buf, dtype=dt, count=cnt).copy())
+    finally:
+        L.oracle_route_free(h)
+    out = _shape(out, window)
+    out.append(np.float32(dur))
+    return out
+
+
+def _ref_dir():
+    return os.path.join(HERE, "_ref")
+
+
+def ref_available():
+    return bool(glob.glob(os.path.join(_ref_dir(), "Libra5BlockOnline*.so")))
+
+
+def ref_route(indptr, indices, values, *args, quiet=True):
+    """The reference router compiled from its own source (oracle/_ref).
+
+    Same arguments as block_sptc_2to4_online; returns numpy arrays.  The
+    reference prints per-window diagnostics on stdout; ``quiet`` drops them."""
+    import torch
+    if _ref_dir() not in sys.path:
+        sys.path.insert(0, _ref_dir())
+    import Libra5BlockOnline  # noqa: E402  (built by oracle/Makefile)
+    rp = torch.from_numpy(np.ascontiguousarray(indptr, dtype=np.int32))
+    ci = torch.from_numpy(np.ascontiguousarray(indices, dtype=np.int32))
+    vv = torch.from_numpy(np.ascontiguousarray(values, dtype=np.float32))
+    if quiet:
+        sys.stdout.flush()
+        fd = os.dup(1)
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(devnull, 1)
+    try:
+        out = Libra5BlockOnline.block_sptc_2to4_online(rp, ci, vv, *args)
+    finally:
+        if quiet:
+            sys.stdout.flush()
+            os.dup2(fd, 1)
+            os.close(fd)
+            os.close(devnull)
+    return [t.numpy() for t in out]
+
+
+def _half(x):
+    return np.asarray(x, dtype=np.float32).astype(np.float16)
+
+
+def decode_sptc_tiles(tile_column, packed_a, packed_meta, window_tile_offset, window=16):
+    """COO (rows, cols, fp16 values) of the packed mma.sp tiles (block_online.cpp:797-841):
+    row group g, lane t -> half2 for rows g / g+8, chunk t, two positions from the meta
+    nibbles.  Zero-valued padding slots are dropped."""
+    rows, cols, vals = [], [], []
+    pa = np.asarray(packed_a).reshape(-1, 8, 4, 2).view(np.uint32)
+    pm = np.asarray(packed_meta).reshape(-1, 8).view(np.uint32)
+    tc = np.asarray(tile_column).reshape(-1, 16)
+    wto = np.asarray(window_tile_offset)
+    tile_win = np.repeat(np.arange(len(wto) - 1), np.diff(wto))
+    for t in range(tc.shape[0]):
+        w = int(tile_win[t])
+        for g in range(8):
+            meta = int(pm[t, g])
+            for ch in range(4):
+                for half_sel, r in ((0, g), (1, g + 8)):
+                    word = int(pa[t, g, ch, half_sel])
+                    nib = (meta >> (16 * half_sel + 4 * ch)) & 0xF
+                    for slot, pos in ((0, nib & 3), (1, (nib >> 2) & 3)):
+                        bits = (word >> (16 * slot)) & 0xFFFF
+                        v = np.array([bits], dtype=np.uint16).view(np.float16)[0]
+                        if v == 0:
+                            continue
+                        c = int(tc[t, ch * 4 + pos])
+                        rows.append(w * window + r)
+                        cols.append(c)
+                        vals.append(v)
+    return (np.array(rows, dtype=np.int64), np.array(cols, dtype=np.int64),
+            np.array(vals, dtype=np.float16))
+
+
+def decode_tables(tabs, n_rows, n_cols, window=16, sptc_from="pos"):
+    """Rebuild the routed operand from the reference's route tables.
+
+    Returns a dict of scipy CSR matrices with FP16-rounded values stored as
+    float64: 'tc', 'sptc', 'cuda' and 'all' (their sum).  ``sptc_from`` picks
+    the SPTC source: 'pos' decodes s_value/s_pos (what the scalar kernel
+    reads, mGCNkernel_online.cu:250-337); 'tiles' decodes the packed tiles
+    (what the mma.sp kernel reads)."""
+    T = dict(zip(TABLE_NAMES, tabs))
+    # TC sub-blocks: bit = row*8 + k in binary_lo (rows 0-7) / binary_hi (rows 8-15);
+    # values in bit order (block_online.cpp:462-488); part -> window via t_window_row.
+    r_l, c_l, v_l = [], [], []
+    t_row = T["t_row_offset"]
+    t_blk = T["t_block_offset"]
+    t_bin = T["t_binary"].view(np.uint64)
+    for p in range(len(t_row) - 1):
+        base_row = int(T["t_window_row"][p])
+        for s in range(int(t_row[p]), int(t_row[p + 1])):
+            lo, hi = int(t_bin[2 * s]), int(t_bin[2 * s + 1])
+            off = int(t_blk[s])
+            n = 0
+            for half_idx, word in ((0, lo), (1, hi)):
+                for bit in range(64):
+                    if (word >> bit) & 1:
+                        r = base_row + half_idx * 8 + bit // 8
+                        c = int(T["t_column"][s * 8 + bit % 8])
+                        r_l.append(r); c_l.append(c); v_l.append(T["t_value"][off + n])
+                        n += 1
+            assert n == int(t_blk[s + 1]) - off, "TC value count != bitmap popcount"
+    tc = sp.csr_matrix((_half(v_l).astype(np.float64), (r_l, c_l)), shape=(n_rows, n_cols))
+
+    if sptc_from == "pos":
+        cols4 = T["s_column"].reshape(-1, 4)
+        pos = T["s_pos"].reshape(cols4.shape[0], window, 2)
+        sval = T["s_value"].reshape(cols4.shape[0], window, 2)
+        g_idx, lr, slot = np.nonzero(pos >= 0)
+        rr = T["s_window"][g_idx].astype(np.int64) * window + lr
+        cc = cols4[g_idx, pos[g_idx, lr, slot]]
+        vv = _half(sval[g_idx, lr, slot]).astype(np.float64)
+        keep = rr < n_rows
+        sptc = sp.csr_matrix((vv[keep], (rr[keep], cc[keep])), shape=(n_rows, n_cols))
+    else:
+        rr, cc, vv = decode_sptc_tiles(T["s_tile_column"], T["s_packed_a"], T["s_packed_meta"],
+                                       T["s_window_tile_offset"], window)
+        sptc = sp.csr_matrix((vv.astype(np.float64), (rr, cc)), shape=(n_rows, n_cols))
+
+    rr, cc, vv = [], [], []
+    for pre in ("", "_short"):
+        off = T["c_row_offset" + pre]
+        rows = T["c_row" + pre]
+        cnt = np.diff(off)
+        rr.append(np.repeat(rows, cnt))
+        cc.append(T["c_column" + pre])
+        vv.append(_half(T["c_value" + pre]).astype(np.float64))
+    cuda = sp.csr_matrix((np.concatenate(vv), (np.concatenate(rr), np.concatenate(cc))),
+                         shape=(n_rows, n_cols))
+    total = (tc + sptc + cuda).tocsr()
+    return {"tc": tc, "sptc": sptc, "cuda": cuda, "all": total}
+
+
+def max_threads():
+    return _load().oracle_max_threads()
+
+
+def spmm_f64(indptr, indices, values, b):
+    """C = A·B in FP64 (C restatement, OpenMP)."""
+    L = _load()
+    rp = np.ascontiguousarray(indptr, dtype=np.int32)
+    ci = np.ascontiguousarray(indices, dtype=np.int32)
+    vv = np.ascontiguousarray(values, dtype=np.float64)
+    bb = np.ascontiguousarray(b, dtype=np.float64)
+    m, k = rp.shape[0] - 1, bb.shape[1]
+    c = np.empty((m, k), dtype=np.float64)
+    L.oracle_spmm_f64(_ptr(rp), _ptr(ci), _ptr(vv), m, _ptr(bb), k, _ptr(c))
+    return c
+
+
+def spmm_f16_f32(indptr, indices, values_f16, b_f16, threads=0, out=None):
+    """C = A·B with FP16 operands, FP32 accumulation (C restatement, OpenMP)."""
+    L = _load()
+    rp = np.ascontiguousarray(indptr, dtype=np.int32)
+    ci = np.ascontiguousarray(indices, dtype=np.int32)
+    vv = np.ascontiguousarray(values_f16, dtype=np.float16)
+    bb = np.ascontiguousarray(b_f16, dtype=np.float16)
+    m, k = rp.shape[0] - 1, bb.shape[1]
+    c = out if out is not None else np.empty((m, k), dtype=np.float32)
+    L.oracle_spmm_f16_f32(_ptr(rp), _ptr(ci), _ptr(vv), m, _ptr(bb), k, _ptr(c), int(threads))
+    return c
+
+
+def sddmm_f64(indptr, indices, dc, b):
+    """dval[e] = <dC[row(e)], B[col(e)]> in FP64."""
+    L = _load()
+    rp = np.ascontiguousarray(indptr, dtype=np.int32)
+    ci = np.ascontiguousarray(indices, dtype=np.int32)
+    g = np.ascontiguousarray(dc, dtype=np.float64)
+    bb = np.ascontiguousarray(b, dtype=np.float64)
+    out = np.empty(ci.shape[0], dtype=np.float64)
+    L.oracle_sddmm_f64(_ptr(rp), _ptr(ci), rp.shape[0] - 1, _ptr(g), _ptr(bb), g.shape[1],
+                       _ptr(out))
+    return out

@@ -1,0 +1,424 @@
+// extern "C" entry points of libtrspmm.so (declared in include/trspmm.h).
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/trspmm.h"
+#include "common.cuh"
+#include "plan.h"
+#include "router.h"
+#include "spmm.h"
+
+namespace trs {
+
+namespace {
+thread_local std::string g_error;
+}
+
+void set_error(const std::string& msg) { g_error = msg; }
+int fail(int code, const std::string& msg) {
+  g_error = msg;
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+  g_error = std::string(what) + ": " + cudaGetErrorString(e);
+  return TR_ERR_CUDA;
+}
+
+namespace {
+
+// Device buffer that frees itself.
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() { if (p) cudaFree(p); }
+  int alloc(size_t bytes) {
+    cudaError_t e = cudaMalloc(&p, bytes > 0 ? bytes : 1);
+    return e == cudaSuccess ? TR_OK : cuda_fail(e, "cudaMalloc");
+  }
+};
+
+struct PlanGuard {
+  tr_plan* p = nullptr;
+  ~PlanGuard() { if (p) tr_plan_free(p); }
+};
+
+// Reads and clears the plan's device error word.
+int check_plan_error(const tr_plan* p) {
+  int flag = 0;
+  TRS_CUDA(cudaMemcpy(&flag, p->view.err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag != kErrNone) {
+    cudaMemset(p->view.err, 0, sizeof(int));
+    return fail(TR_ERR_TIMEOUT, "routed kernel: a bounded tensor-core wait gave up");
+  }
+  return TR_OK;
+}
+
+// Times `epoches` launches of the plan after 10 warm-up launches (the
+// reference's protocol, mGCNkernel_online.cu:1604-1674), then leaves one
+// clean result in d_out.  ms = average per launch.
+int timed_routed(const tr_plan* p, const uint16_t* d_b, int32_t k, float* d_out, int mask,
+                 int epoches, float* ms) {
+  cudaStream_t s;
+  TRS_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int rc = TR_OK;
+  for (int i = 0; i < 10 && rc == TR_OK; ++i) rc = launch_routed(p, d_b, k, d_out, TR_OUT_F32, mask, s);
+  if (rc == TR_OK) {
+    cudaEventRecord(e0, s);
+    for (int i = 0; i < epoches && rc == TR_OK; ++i)
+      rc = launch_routed(p, d_b, k, d_out, TR_OUT_F32, mask, s);
+    cudaEventRecord(e1, s);
+  }
+  cudaError_t ce = cudaStreamSynchronize(s);
+  float t = 0.f;
+  if (rc == TR_OK && ce == cudaSuccess) {
+    cudaEventElapsedTime(&t, e0, e1);
+    *ms = t / (float)epoches;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamDestroy(s);
+  if (rc != TR_OK) return rc;
+  if (ce != cudaSuccess) return cuda_fail(ce, "routed kernel");
+  return check_plan_error(p);
+}
+
+// Common tail of the reference-compatible calls: upload B, run the plan
+// (timed), copy the FP32 result back.
+int run_compat(const HostPlan& hp, const uint16_t* rhs, int64_t n_rhs, int32_t dimN, int32_t mOri,
+               int32_t kOri, int32_t epoches, float* out, float* ms_out, bool per_route) {
+  if (n_rhs != (int64_t)kOri * dimN) return fail(TR_ERR_ARG, "rhs_matrix must have kOri * dimN elements");
+  tr_plan* p = nullptr;
+  int rc = plan_upload(hp, &p);
+  if (rc) return rc;
+  PlanGuard pg{p};
+  DevBuf db, dc;
+  if ((rc = db.alloc((size_t)n_rhs * 2))) return rc;
+  if ((rc = dc.alloc((size_t)mOri * dimN * 4))) return rc;
+  TRS_CUDA(cudaMemcpy(db.p, rhs, (size_t)n_rhs * 2, cudaMemcpyHostToDevice));
+  TRS_CUDA(cudaMemset(dc.p, 0, (size_t)mOri * dimN * 4));
+  float ms[5] = {0, 0, 0, 0, 0};
+  if (per_route) {
+    if ((rc = timed_routed(p, (uint16_t*)db.p, dimN, (float*)dc.p, TR_ROUTE_TC, epoches, &ms[1]))) return rc;
+    if ((rc = timed_routed(p, (uint16_t*)db.p, dimN, (float*)dc.p, TR_ROUTE_CUDA, epoches, &ms[2]))) return rc;
+    ms[3] = ms[2];
+    if ((rc = timed_routed(p, (uint16_t*)db.p, dimN, (float*)dc.p, TR_ROUTE_SPTC, epoches, &ms[4]))) return rc;
+  }
+  if ((rc = timed_routed(p, (uint16_t*)db.p, dimN, (float*)dc.p, TR_ROUTE_ALL, epoches, &ms[0]))) return rc;
+  TRS_CUDA(cudaMemcpy(out, dc.p, (size_t)mOri * dimN * 4, cudaMemcpyDeviceToHost));
+  if (ms_out) std::memcpy(ms_out, ms, sizeof(ms));
+  return TR_OK;
+}
+
+int check_common(int32_t window, int32_t dimN, int32_t mOri, int32_t kOri, int32_t epoches,
+                 int max_window) {
+  if (!(window > 0 && window <= max_window))
+    return fail(TR_ERR_ARG, "window must be in (0, " + std::to_string(max_window) + "]");
+  if (dimN <= 0) return fail(TR_ERR_ARG, "dimN must be positive");
+  if (mOri <= 0) return fail(TR_ERR_ARG, "mOri must be positive");
+  if (kOri <= 0) return fail(TR_ERR_ARG, "kOri must be positive");
+  if (epoches <= 0) return fail(TR_ERR_ARG, "epoches must be positive");
+  return TR_OK;
+}
+
+}  // namespace
+}  // namespace trs
+
+using namespace trs;
+
+struct tr_route {
+  RouteTables t;
+};
+
+extern "C" {
+
+const char* tr_last_error(void) { return g_error.c_str(); }
+int tr_version(void) { return 1; }
+
+int tr_device_info(int* num_sms, int* cc_major, int* cc_minor) {
+  int dev = 0;
+  TRS_CUDA(cudaGetDevice(&dev));
+  if (num_sms) TRS_CUDA(cudaDeviceGetAttribute(num_sms, cudaDevAttrMultiProcessorCount, dev));
+  if (cc_major) TRS_CUDA(cudaDeviceGetAttribute(cc_major, cudaDevAttrComputeCapabilityMajor, dev));
+  if (cc_minor) TRS_CUDA(cudaDeviceGetAttribute(cc_minor, cudaDevAttrComputeCapabilityMinor, dev));
+  return TR_OK;
+}
+
+int tr_route_build(const int32_t* indptr, const int32_t* indices, const float* values,
+                   int32_t n_rows, const tr_route_params* params, tr_route** out) {
+  if (!indptr || !params || !out) return fail(TR_ERR_ARG, "null argument");
+  std::unique_ptr<tr_route> r(new tr_route());
+  std::string err;
+  const int rc = build_route(indptr, indices, values, n_rows, *params, r->t, err);
+  if (rc) return fail(rc, err);
+  *out = r.release();
+  return TR_OK;
+}
+
+int tr_route_table(const tr_route* r, int idx, const void** data, int64_t* count) {
+  if (!r || !data || !count) return fail(TR_ERR_ARG, "null argument");
+  const RouteTables& T = r->t;
+#define TRS_T(i, v) case i: *data = T.v.data(); *count = (int64_t)T.v.size(); return TR_OK;
+  switch (idx) {
+    TRS_T(0, t_row_offset) TRS_T(1, t_block_offset) TRS_T(2, t_column) TRS_T(3, t_value)
+    TRS_T(4, t_window_row) TRS_T(5, t_atomic) TRS_T(6, t_binary)
+    TRS_T(7, c_row_offset) TRS_T(8, c_row) TRS_T(9, c_atomic) TRS_T(10, c_column) TRS_T(11, c_value)
+    TRS_T(12, cs_row_offset) TRS_T(13, cs_row) TRS_T(14, cs_atomic) TRS_T(15, cs_column)
+    TRS_T(16, cs_value) TRS_T(17, s_column) TRS_T(18, s_mask) TRS_T(19, s_value) TRS_T(20, s_pos)
+    TRS_T(21, s_window) TRS_T(22, s_offsets) TRS_T(23, s_tile_window) TRS_T(24, s_tile_group)
+    TRS_T(25, s_tile_column) TRS_T(26, s_packed_a) TRS_T(27, s_packed_meta)
+    TRS_T(28, s_window_tile_offset)
+    default: return fail(TR_ERR_ARG, "table index out of range");
+  }
+#undef TRS_T
+}
+
+double tr_route_seconds(const tr_route* r) { return r ? r->t.seconds : 0.0; }
+void tr_route_free(tr_route* r) { delete r; }
+
+int tr_plan_from_tables(const tr_tables* t, int32_t n_rows, int32_t n_cols, int32_t window,
+                        tr_plan** out) {
+  if (!t || !out) return fail(TR_ERR_ARG, "null argument");
+  HostPlan hp;
+  std::string err;
+  int rc = plan_from_tables(*t, n_rows, n_cols, window, hp, err);
+  if (rc) return fail(rc, err);
+  return plan_upload(hp, out);
+}
+
+int tr_plan_from_csr(const int32_t* indptr, const int32_t* indices, const float* values,
+                     int32_t n_rows, int32_t n_cols, const tr_route_params* params,
+                     tr_plan** out) {
+  if (!indptr || !params || !out) return fail(TR_ERR_ARG, "null argument");
+  tr_route_params p = *params;
+  if (p.window != 16) return fail(TR_ERR_UNSUPPORTED, "routed plans need window == 16");
+  RouteTables T;
+  std::string err;
+  int rc = build_route(indptr, indices, values, n_rows, p, T, err);
+  if (rc) return fail(rc, err);
+  for (int32_t c : T.c_column) if (c >= n_cols) return fail(TR_ERR_ARG, "column index >= n_cols");
+  std::vector<uint16_t> tv(T.t_value.size()), cv(T.c_value.size()), csv(T.cs_value.size());
+  auto h = [](float f) { _Float16 x = (_Float16)f; uint16_t b; std::memcpy(&b, &x, 2); return b; };
+  for (size_t i = 0; i < tv.size(); ++i) tv[i] = h(T.t_value[i]);
+  for (size_t i = 0; i < cv.size(); ++i) cv[i] = h(T.c_value[i]);
+  for (size_t i = 0; i < csv.size(); ++i) csv[i] = h(T.cs_value[i]);
+  tr_tables tt{};
+  tt.t_row_offset = T.t_row_offset.data(); tt.n_t_row_offset = (int64_t)T.t_row_offset.size();
+  tt.t_block_offset = T.t_block_offset.data(); tt.n_t_block_offset = (int64_t)T.t_block_offset.size();
+  tt.t_column = T.t_column.data(); tt.n_t_column = (int64_t)T.t_column.size();
+  tt.t_value = tv.data(); tt.n_t_value = (int64_t)tv.size();
+  tt.t_window_row = T.t_window_row.data(); tt.n_t_window_row = (int64_t)T.t_window_row.size();
+  tt.t_binary = T.t_binary.data(); tt.n_t_binary = (int64_t)T.t_binary.size();
+  tt.c_row_offset = T.c_row_offset.data(); tt.n_c_row_offset = (int64_t)T.c_row_offset.size();
+  tt.c_row = T.c_row.data(); tt.n_c_row = (int64_t)T.c_row.size();
+  tt.c_column = T.c_column.data(); tt.n_c_column = (int64_t)T.c_column.size();
+  tt.c_value = cv.data(); tt.n_c_value = (int64_t)cv.size();
+  tt.cs_row_offset = T.cs_row_offset.data(); tt.n_cs_row_offset = (int64_t)T.cs_row_offset.size();
+  tt.cs_row = T.cs_row.data(); tt.n_cs_row = (int64_t)T.cs_row.size();
+  tt.cs_column = T.cs_column.data(); tt.n_cs_column = (int64_t)T.cs_column.size();
+  tt.cs_value = csv.data(); tt.n_cs_value = (int64_t)csv.size();
+  tt.s_tile_column = T.s_tile_column.data(); tt.n_s_tile_column = (int64_t)T.s_tile_column.size();
+  tt.s_packed_a = reinterpret_cast<const uint32_t*>(T.s_packed_a.data());
+  tt.n_s_packed_a = (int64_t)T.s_packed_a.size();
+  tt.s_packed_meta = reinterpret_cast<const uint32_t*>(T.s_packed_meta.data());
+  tt.n_s_packed_meta = (int64_t)T.s_packed_meta.size();
+  tt.s_window_tile_offset = T.s_window_tile_offset.data();
+  tt.n_s_window_tile_offset = (int64_t)T.s_window_tile_offset.size();
+  HostPlan hp;
+  rc = plan_from_tables(tt, n_rows, n_cols, 16, hp, err);
+  if (rc) return fail(rc, err);
+  return plan_upload(hp, out);
+}
+
+int tr_plan_info_get(const tr_plan* p, tr_plan_info* info) {
+  if (!p || !info) return fail(TR_ERR_ARG, "null argument");
+  *info = p->info;
+  return TR_OK;
+}
+
+void tr_plan_free(tr_plan* p) {
+  if (!p) return;
+  if (p->block) cudaFree(p->block);
+  delete p;
+}
+
+int tr_spmm_csr(const int32_t* indptr, const int32_t* indices, const uint16_t* values, int32_t m,
+                int32_t n_cols, int64_t nnz, const uint16_t* b, int32_t k, void* c, int c_dtype,
+                void* stream) {
+  if (m < 0 || k < 0 || n_cols < 0 || nnz < 0) return fail(TR_ERR_ARG, "negative size");
+  if (c_dtype != TR_OUT_F32 && c_dtype != TR_OUT_F16) return fail(TR_ERR_ARG, "bad output dtype");
+  if (m > 0 && k > 0 && (!indptr || !b || !c || (nnz > 0 && (!indices || !values))))
+    return fail(TR_ERR_ARG, "null device pointer");
+  return launch_csr(indptr, indices, values, m, b, k, c, c_dtype, (cudaStream_t)stream);
+}
+
+int tr_spmm_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_dtype,
+                   int route_mask, void* stream) {
+  if (!p) return fail(TR_ERR_ARG, "null plan");
+  if (k < 0) return fail(TR_ERR_ARG, "negative K");
+  if (c_dtype != TR_OUT_F32 && c_dtype != TR_OUT_F16) return fail(TR_ERR_ARG, "bad output dtype");
+  if (p->view.n_rows > 0 && k > 0 && (!b || !c)) return fail(TR_ERR_ARG, "null device pointer");
+  return launch_routed(p, b, k, c, c_dtype, route_mask & TR_ROUTE_ALL, (cudaStream_t)stream);
+}
+
+int tr_forward_fp16_tcu_cuda_sptc_mma_parallel_online(
+    const int32_t* t_row_offset, int64_t n_t_row_offset, const int32_t* t_block_offset,
+    int64_t n_t_block_offset, const int32_t* t_column, int64_t n_t_column, const uint16_t* t_value,
+    int64_t n_t_value, const int32_t* t_window_row, int64_t n_t_window_row, const int32_t* t_atomic,
+    int64_t n_t_atomic, const int64_t* t_binary, int64_t n_t_binary, const int32_t* c_row_offset,
+    int64_t n_c_row_offset, const int32_t* c_row, int64_t n_c_row, const int32_t* c_atomic,
+    int64_t n_c_atomic, const int32_t* c_column, int64_t n_c_column, const uint16_t* c_value,
+    int64_t n_c_value, const int32_t* c_row_offset_short, int64_t n_c_row_offset_short,
+    const int32_t* c_row_short, int64_t n_c_row_short, const int32_t* c_atomic_short,
+    int64_t n_c_atomic_short, const int32_t* c_column_short, int64_t n_c_column_short,
+    const uint16_t* c_value_short, int64_t n_c_value_short, const int32_t* s_column,
+    int64_t n_s_column, const float* s_value, int64_t n_s_value, const int8_t* s_pos,
+    int64_t n_s_pos, const int32_t* s_offsets, int64_t n_s_offsets, const int32_t* s_tile_window,
+    int64_t n_s_tile_window, const int32_t* s_tile_column, int64_t n_s_tile_column,
+    const int32_t* s_packed_a, int64_t n_s_packed_a, const int32_t* s_packed_meta,
+    int64_t n_s_packed_meta, const int32_t* s_window_tile_offset, int64_t n_s_window_tile_offset,
+    const uint16_t* rhs_matrix, int64_t n_rhs_matrix, int32_t parts_t, int32_t parts_c,
+    int32_t partsize_c, int32_t parts_c_short, int32_t window, int32_t dimN, int32_t mOri,
+    int32_t kOri, int32_t epoches, float* out, float* ms_out) {
+  (void)t_atomic; (void)n_t_atomic; (void)c_atomic; (void)n_c_atomic; (void)c_atomic_short;
+  (void)n_c_atomic_short; (void)partsize_c; (void)s_value; (void)n_s_value; (void)s_pos; (void)n_s_pos;
+  int rc = check_common(window, dimN, mOri, kOri, epoches, 16);
+  if (rc) return rc;
+  // shape checks of mGCN_online.cpp:866-932
+  if (n_s_column % 4) return fail(TR_ERR_ARG, "s_column must have shape [groups, 4]");
+  if (n_s_offsets < 1) return fail(TR_ERR_ARG, "s_offsets must be 1-D with at least one item");
+  const int64_t groups = n_s_column / 4;
+  if (s_offsets[0] != 0) return fail(TR_ERR_ARG, "s_offsets must start with 0");
+  if (s_offsets[n_s_offsets - 1] != groups)
+    return fail(TR_ERR_ARG, "s_offsets end must equal group count");
+  int64_t tiles = 0;
+  for (int64_t w = 0; w + 1 < n_s_offsets; ++w) {
+    const int64_t gc = s_offsets[w + 1] - s_offsets[w];
+    if (gc < 0) return fail(TR_ERR_ARG, "s_offsets must be non-decreasing");
+    tiles += (gc + 3) / 4;
+  }
+  if (n_s_tile_column != n_s_tile_window * 16) return fail(TR_ERR_ARG, "s_tile_column tile count mismatch");
+  if (n_s_packed_a != n_s_tile_window * 64) return fail(TR_ERR_ARG, "s_packed_a tile count mismatch");
+  if (n_s_packed_meta != n_s_tile_window * 8) return fail(TR_ERR_ARG, "s_packed_meta tile count mismatch");
+  if (tiles != n_s_tile_window) return fail(TR_ERR_ARG, "packed tile count must match offsets-derived tile count");
+  if (parts_t != n_t_row_offset - 1 && !(parts_t == 0 && n_t_row_offset <= 1))
+    return fail(TR_ERR_ARG, "parts_t does not match t_row_offset");
+  if (parts_c != n_c_row_offset - 1 && !(parts_c == 0 && n_c_row_offset <= 1))
+    return fail(TR_ERR_ARG, "parts_c does not match c_row_offset");
+  if (parts_c_short != n_c_row_offset_short - 1 && !(parts_c_short == 0 && n_c_row_offset_short <= 1))
+    return fail(TR_ERR_ARG, "parts_c_short does not match c_row_offset_short");
+  if (window != 16) return fail(TR_ERR_UNSUPPORTED, "the routed tables assume 16-row windows");
+  tr_tables tt{};
+  tt.t_row_offset = t_row_offset; tt.n_t_row_offset = n_t_row_offset;
+  tt.t_block_offset = t_block_offset; tt.n_t_block_offset = n_t_block_offset;
+  tt.t_column = t_column; tt.n_t_column = n_t_column;
+  tt.t_value = t_value; tt.n_t_value = n_t_value;
+  tt.t_window_row = t_window_row; tt.n_t_window_row = n_t_window_row;
+  tt.t_binary = t_binary; tt.n_t_binary = n_t_binary;
+  tt.c_row_offset = c_row_offset; tt.n_c_row_offset = n_c_row_offset;
+  tt.c_row = c_row; tt.n_c_row = n_c_row;
+  tt.c_column = c_column; tt.n_c_column = n_c_column;
+  tt.c_value = c_value; tt.n_c_value = n_c_value;
+  tt.cs_row_offset = c_row_offset_short; tt.n_cs_row_offset = n_c_row_offset_short;
+  tt.cs_row = c_row_short; tt.n_cs_row = n_c_row_short;
+  tt.cs_column = c_column_short; tt.n_cs_column = n_c_column_short;
+  tt.cs_value = c_value_short; tt.n_cs_value = n_c_value_short;
+  tt.s_tile_column = s_tile_column; tt.n_s_tile_column = n_s_tile_column;
+  tt.s_packed_a = reinterpret_cast<const uint32_t*>(s_packed_a); tt.n_s_packed_a = n_s_packed_a;
+  tt.s_packed_meta = reinterpret_cast<const uint32_t*>(s_packed_meta); tt.n_s_packed_meta = n_s_packed_meta;
+  tt.s_window_tile_offset = s_window_tile_offset; tt.n_s_window_tile_offset = n_s_window_tile_offset;
+  HostPlan hp;
+  std::string err;
+  rc = plan_from_tables(tt, mOri, kOri, window, hp, err);
+  if (rc) return fail(rc, err);
+  return run_compat(hp, rhs_matrix, n_rhs_matrix, dimN, mOri, kOri, epoches, out, ms_out, true);
+}
+
+int tr_forward_fp16_sptc_online(const int32_t* s_column, int64_t n_s_column, const float* s_value,
+                                int64_t n_s_value, const int8_t* s_pos, int64_t n_s_pos,
+                                const int32_t* s_window, int64_t n_s_window,
+                                const uint16_t* rhs_matrix, int64_t n_rhs_matrix, int32_t window,
+                                int32_t dimN, int32_t mOri, int32_t kOri, int32_t epoches,
+                                float* out, float* ms_out) {
+  int rc = check_common(window, dimN, mOri, kOri, epoches, 1 << 30);
+  if (rc) return rc;
+  const int64_t groups = n_s_window;
+  if (n_s_column != groups * 4) return fail(TR_ERR_ARG, "s_column group count mismatch");
+  if (n_s_value != groups * window * 2) return fail(TR_ERR_ARG, "s_value group count mismatch");
+  if (n_s_pos != groups * window * 2) return fail(TR_ERR_ARG, "s_pos group count mismatch");
+  if (window != 16) return fail(TR_ERR_UNSUPPORTED, "the routed kernels need 16-row windows");
+  HostPlan hp;
+  std::string err;
+  rc = plan_from_groups(s_column, s_value, s_pos, groups, s_window, nullptr, 0, window, mOri, kOri,
+                        hp, err);
+  if (rc) return fail(rc, err);
+  float ms[5];
+  rc = run_compat(hp, rhs_matrix, n_rhs_matrix, dimN, mOri, kOri, epoches, out, ms, false);
+  if (rc == TR_OK && ms_out) ms_out[0] = ms[0];
+  return rc;
+}
+
+int tr_forward_fp16_sptc_mma_online(const int32_t* s_column, int64_t n_s_column,
+                                    const float* s_value, int64_t n_s_value, const int8_t* s_pos,
+                                    int64_t n_s_pos, const int32_t* s_offsets, int64_t n_s_offsets,
+                                    const uint16_t* rhs_matrix, int64_t n_rhs_matrix,
+                                    int32_t window, int32_t dimN, int32_t mOri, int32_t kOri,
+                                    int32_t epoches, float* out, float* ms_out) {
+  int rc = check_common(window, dimN, mOri, kOri, epoches, 16);
+  if (rc) return rc;
+  const int64_t groups = n_s_column / 4;
+  if (n_s_column % 4) return fail(TR_ERR_ARG, "s_column must have shape [groups, 4]");
+  if (n_s_value != groups * window * 2) return fail(TR_ERR_ARG, "s_value group count mismatch");
+  if (n_s_pos != groups * window * 2) return fail(TR_ERR_ARG, "s_pos group count mismatch");
+  if (window != 16) return fail(TR_ERR_UNSUPPORTED, "the routed kernels need 16-row windows");
+  HostPlan hp;
+  std::string err;
+  rc = plan_from_groups(s_column, s_value, s_pos, groups, nullptr, s_offsets, n_s_offsets, window,
+                        mOri, kOri, hp, err);
+  if (rc) return fail(rc, err);
+  float ms[5];
+  rc = run_compat(hp, rhs_matrix, n_rhs_matrix, dimN, mOri, kOri, epoches, out, ms, false);
+  if (rc == TR_OK && ms_out) ms_out[0] = ms[0];
+  return rc;
+}
+
+int tr_forward_fp16_sptc_mma_packed_online(const int32_t* s_tile_column, int64_t n_s_tile_column,
+                                           const int32_t* s_packed_a, int64_t n_s_packed_a,
+                                           const int32_t* s_packed_meta, int64_t n_s_packed_meta,
+                                           const int32_t* s_window_tile_offset,
+                                           int64_t n_s_window_tile_offset,
+                                           const uint16_t* rhs_matrix, int64_t n_rhs_matrix,
+                                           int32_t window, int32_t dimN, int32_t mOri,
+                                           int32_t kOri, int32_t epoches, float* out,
+                                           float* ms_out) {
+  int rc = check_common(window, dimN, mOri, kOri, epoches, 16);
+  if (rc) return rc;
+  if (n_s_tile_column % 16) return fail(TR_ERR_ARG, "s_tile_column must have shape [tiles, 16]");
+  const int64_t tiles = n_s_tile_column / 16;
+  if (n_s_packed_a != tiles * 64) return fail(TR_ERR_ARG, "s_packed_a tile count mismatch");
+  if (n_s_packed_meta != tiles * 8) return fail(TR_ERR_ARG, "s_packed_meta tile count mismatch");
+  if (n_s_window_tile_offset < 2)
+    return fail(TR_ERR_ARG, "s_window_tile_offset must be 1-D with at least 2 elements");
+  if (window != 16) return fail(TR_ERR_UNSUPPORTED, "the routed kernels need 16-row windows");
+  tr_tables tt{};
+  tt.s_tile_column = s_tile_column; tt.n_s_tile_column = n_s_tile_column;
+  tt.s_packed_a = reinterpret_cast<const uint32_t*>(s_packed_a); tt.n_s_packed_a = n_s_packed_a;
+  tt.s_packed_meta = reinterpret_cast<const uint32_t*>(s_packed_meta); tt.n_s_packed_meta = n_s_packed_meta;
+  tt.s_window_tile_offset = s_window_tile_offset; tt.n_s_window_tile_offset = n_s_window_tile_offset;
+  HostPlan hp;
+  std::string err;
+  rc = plan_from_tables(tt, mOri, kOri, window, hp, err);
+  if (rc) return fail(rc, err);
+  float ms[5];
+  rc = run_compat(hp, rhs_matrix, n_rhs_matrix, dimN, mOri, kOri, epoches, out, ms, false);
+  if (rc == TR_OK && ms_out) ms_out[0] = ms[0];
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,392 @@
+// sm_100a SpMM kernels.
+//
+//  csr_block_kernel   plain single-route CSR SpMM on CUDA cores: one CTA per
+//                     16-row block, its entries split evenly across 8 warps
+//                     (balanced even with power-law rows), 128-bit loads of
+//                     B rows, FP32 accumulation into a shared-memory block,
+//                     one coalesced store per output element.
+//  routed_kernel      the fused three-route forward: one CTA per 16-row
+//                     window.  The dense-TC and 2:4 tiles run on tcgen05
+//                     (B rows gathered into 128-byte-swizzled shared memory,
+//                     D^T[feature x row] accumulated in TMEM), the residual
+//                     runs on CUDA cores with the same engine as the plain
+//                     kernel, and the epilogue adds both and stores each
+//                     output element once (no atomics in global memory, no
+//                     separate 2:4 buffer, no merge kernel — compare
+//                     TR-source/SpMM/mGCNkernel_online.cu:1529-1727).
+//  generic kernels    any K (not a multiple of 8): scalar but still on the GPU.
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "plan.h"
+#include "spmm.h"
+
+namespace trs {
+namespace {
+
+constexpr int kBlockRows = 16;      // rows per window / row block
+constexpr int kWarps = 8;
+constexpr int kThreads = kWarps * 32;
+constexpr int kChunk = 128;         // features per pass (UMMA M)
+constexpr int kStages = 4;          // tiles gathered per MMA batch
+constexpr int kUnroll = 4;          // independent 16-byte B loads in flight per lane
+
+__device__ __forceinline__ void fma8(float (&acc)[8], float v, const uint4& b) {
+  const __half2* h = reinterpret_cast<const __half2*>(&b);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const float2 f = __half22float2(h[i]);
+    acc[2 * i] = fmaf(v, f.x, acc[2 * i]);
+    acc[2 * i + 1] = fmaf(v, f.y, acc[2 * i + 1]);
+  }
+}
+
+// Adds the CSR rows of one 16-row block (row pointer rp[0..16] in shared
+// memory, absolute entry indices) times B[:, f0 : f0+fc] into racc[16][kChunk]
+// (shared, FP32).  Entries are split evenly across the CTA's warps; inside a
+// warp, groups of L lanes (L*8 >= fc) each take one entry and load 16 bytes
+// of its B row per lane.  A lane group flushes its partial row with shared
+// atomics whenever its entries cross a row boundary.
+__device__ __forceinline__ void block_accumulate(const int* rp, const int32_t* __restrict__ col,
+                                                 const __half* __restrict__ val,
+                                                 const __half* __restrict__ B, int K, int f0,
+                                                 int fc, float* racc) {
+  int L = 1;
+  while (L * 8 < fc) L <<= 1;
+  const int G = 32 / L;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane / L, li = lane % L;
+  const bool active = li * 8 < fc;
+  const int e_begin = rp[0], e_end = rp[kBlockRows];
+  const int total = e_end - e_begin;
+  const int per = (total + kWarps - 1) / kWarps;
+  const int eb = e_begin + warp * per;
+  const int ee = min(e_end, eb + per);
+  if (eb >= ee) return;
+  float acc[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) acc[i] = 0.f;
+  int row = 0;
+  int cur = -1;
+  const __half* Bf = B + f0 + li * 8;
+  for (int e0 = eb + g; e0 < ee; e0 += G * kUnroll) {
+    int cidx[kUnroll];
+    float v[kUnroll];
+    uint4 bv[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int e = e0 + u * G;
+      cidx[u] = e < ee ? __ldg(col + e) : -1;
+      v[u] = e < ee ? __half2float(val[e]) : 0.f;
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      if (cidx[u] >= 0 && active)
+        bv[u] = __ldg(reinterpret_cast<const uint4*>(Bf + (size_t)cidx[u] * K));
+      else
+        bv[u] = make_uint4(0, 0, 0, 0);
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const int e = e0 + u * G;
+      if (e >= ee) break;
+      while (rp[row + 1] <= e) ++row;
+      if (row != cur) {
+        if (cur >= 0 && active) {
+          float* dst = racc + cur * kChunk + li * 8;
+#pragma unroll
+          for (int i = 0; i < 8; ++i) atomicAdd(dst + i, acc[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i) acc[i] = 0.f;
+        cur = row;
+      }
+      fma8(acc, v[u], bv[u]);
+    }
+  }
+  if (cur >= 0 && active) {
+    float* dst = racc + cur * kChunk + li * 8;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) atomicAdd(dst + i, acc[i]);
+  }
+}
+
+template <bool F16OUT>
+__device__ __forceinline__ void store_row_feature(void* C, int K, int64_t row, int f, float v) {
+  if (F16OUT)
+    reinterpret_cast<__half*>(C)[row * K + f] = __float2half_rn(v);
+  else
+    reinterpret_cast<float*>(C)[row * K + f] = v;
+}
+
+// ---------------------------------------------------------------------------
+// Plain CSR (single route)
+// ---------------------------------------------------------------------------
+template <bool F16OUT>
+__global__ void __launch_bounds__(kThreads) csr_block_kernel(
+    const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+    const __half* __restrict__ values, int M, const __half* __restrict__ B, int K, void* C) {
+  __shared__ __align__(16) float racc[kBlockRows * kChunk];
+  __shared__ int rp[kBlockRows + 1];
+  const int r0 = blockIdx.x * kBlockRows;
+  if (threadIdx.x <= kBlockRows) rp[threadIdx.x] = indptr[min(r0 + (int)threadIdx.x, M)];
+  for (int f0 = 0; f0 < K; f0 += kChunk) {
+    const int fc = min(kChunk, K - f0);
+    for (int i = threadIdx.x; i < kBlockRows * kChunk; i += kThreads) racc[i] = 0.f;
+    __syncthreads();
+    block_accumulate(rp, indices, values, B, K, f0, fc, racc);
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int f = (warp & 3) * 32 + lane;
+    if (f < fc) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int r = (warp >> 2) * 8 + i;
+        if (r0 + r < M) store_row_feature<F16OUT>(C, K, r0 + r, f0 + f, racc[r * kChunk + f]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Any K: one thread per (row, feature).
+template <bool F16OUT>
+__global__ void csr_generic_kernel(const int32_t* __restrict__ indptr,
+                                   const int32_t* __restrict__ indices,
+                                   const __half* __restrict__ values, int M,
+                                   const __half* __restrict__ B, int K, void* C) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)M * K) return;
+  const int r = (int)(idx / K), f = (int)(idx % K);
+  float acc = 0.f;
+  for (int e = indptr[r]; e < indptr[r + 1]; ++e)
+    acc = fmaf(__half2float(values[e]), __half2float(B[(int64_t)indices[e] * K + f]), acc);
+  store_row_feature<F16OUT>(C, K, r, f, acc);
+}
+
+// ---------------------------------------------------------------------------
+// Fused routed forward
+// ---------------------------------------------------------------------------
+// Shared memory (dynamic, 1024-aligned base):
+//   [kStages][4096]  A operand: 16 gathered B rows x 128 features, MN-major,
+//                    128-byte swizzle; atoms of 8 rows x 64 features:
+//                    (k, f) -> (k/8)*2048 + (f/64)*1024 + (k%8)*128 +
+//                              (((f%64)/8) ^ (k%8))*16 + (f%8)*2
+//   [kStages][512]   B operand: the 16x16 A tile (K-major, no swizzle)
+//   racc[16][128]    residual rows (FP32)
+//   rp[17], mbar, tmem base
+constexpr int kAOpBytes = 4096;
+constexpr int kBOpBytes = 512;
+constexpr int kSmemRouted = 1024 + kStages * (kAOpBytes + kBOpBytes) +
+                            kBlockRows * kChunk * 4 + 128;
+constexpr uint32_t kIdesc = umma_idesc_f16(128, 16, /*a MN-major*/ true, /*b MN-major*/ false);
+
+template <bool F16OUT>
+__global__ void __launch_bounds__(kThreads) routed_kernel(PlanView pv, const __half* __restrict__ B,
+                                                          int K, void* C, int route_mask) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint8_t* aop = smem;
+  uint8_t* bop = smem + kStages * kAOpBytes;
+  float* racc = reinterpret_cast<float*>(bop + kStages * kBOpBytes);
+  int* rp = reinterpret_cast<int*>(racc + kBlockRows * kChunk);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(rp + 18);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int w = pv.win_order[blockIdx.x];
+  const int r0 = w * kBlockRows;
+  const int M = pv.n_rows;
+
+  // tiles of the selected routes: [ta0, ta1) dense TC, [tb0, tb1) 2:4
+  int ta0 = pv.win_tile[w], ta1 = pv.win_split[w];
+  int tb0 = ta1, tb1 = pv.win_tile[w + 1];
+  if (!(route_mask & TR_ROUTE_TC)) ta1 = ta0;
+  if (!(route_mask & TR_ROUTE_SPTC)) tb1 = tb0;
+  const int nt = (ta1 - ta0) + (tb1 - tb0);
+  const bool do_res = (route_mask & TR_ROUTE_CUDA) != 0;
+
+  if (tid <= kBlockRows) {
+    const int64_t rr = (int64_t)w * kBlockRows + tid;
+    rp[tid] = do_res ? pv.res_ptr[rr] : 0;
+  }
+  uint32_t tmem = 0;
+  const uint32_t bar = smem_u32(mbar);
+  if (nt > 0) {
+    if (warp == 0) {
+      tmem_alloc(smem_u32(tmem_slot), 32);
+      tmem_relinquish();
+    }
+    if (tid == 0) {
+      mbar_init(bar, 1);
+      fence_mbar_init();
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (nt > 0) tmem = *tmem_slot;
+
+  uint32_t phase = 0;      // completed commits observed
+  bool pending = false;    // a commit not yet waited for
+  bool failed = false;
+
+  for (int f0 = 0; f0 < K; f0 += kChunk) {
+    const int fc = min(kChunk, K - f0);
+    // ---- tensor-core tiles ---------------------------------------------------
+    for (int tb = 0; tb < nt && !failed; tb += kStages) {
+      const int nb = min(kStages, nt - tb);
+      if (pending) {
+        // thread 0 observes the MMA completion; the barrier orders the rest
+        const bool ok = tid == 0 ? mbar_wait_bounded(bar, phase & 1) : true;
+        if (__syncthreads_or(!ok)) { failed = true; break; }
+        phase++;
+        pending = false;
+      }
+      for (int s = 0; s < nb; ++s) {
+        const int ti = tb + s;
+        const int t = ti < (ta1 - ta0) ? ta0 + ti : tb0 + (ti - (ta1 - ta0));
+        // 16 rows x 16 chunks of 16 bytes: one chunk per thread
+        const int k = tid >> 4, j = tid & 15;
+        const int c = __ldg(pv.tile_col + (int64_t)t * 16 + k);
+        const bool ok = c >= 0 && j * 8 < fc;
+        const __half* src = ok ? B + (int64_t)c * K + f0 + j * 8 : B;
+        const uint32_t dst = smem_u32(aop + s * kAOpBytes) + (k >> 3) * 2048 + (j >> 3) * 1024 +
+                             (k & 7) * 128 + (((j & 7) ^ (k & 7)) << 4);
+        cp_async16(dst, src, ok ? 16 : 0);
+        if (tid < 32) {
+          const uint16_t* asrc = pv.tile_a + (int64_t)t * 256 + tid * 8;
+          cp_async16(smem_u32(bop + s * kBOpBytes) + tid * 16, asrc, 16);
+        }
+      }
+      cp_async_commit();
+      cp_async_wait_all();
+      fence_proxy_async_smem();
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after();
+        for (int s = 0; s < nb; ++s) {
+          const uint64_t adesc = umma_smem_desc(smem_u32(aop + s * kAOpBytes), 1024, 2048, 2);
+          const uint64_t bdesc = umma_smem_desc(smem_u32(bop + s * kBOpBytes), 128, 256, 0);
+          umma_f16(tmem, adesc, bdesc, kIdesc, (tb + s) > 0 ? 1u : 0u);
+        }
+        umma_commit(bar);
+      }
+      pending = true;
+    }
+    // ---- CUDA-core residual --------------------------------------------------
+    for (int i = tid; i < kBlockRows * kChunk; i += kThreads) racc[i] = 0.f;
+    __syncthreads();
+    if (do_res)
+      block_accumulate(rp, pv.res_col, reinterpret_cast<const __half*>(pv.res_val), B, K, f0, fc,
+                       racc);
+    __syncthreads();
+    // ---- epilogue: D^T from TMEM + residual, one store per element ------------
+    float d[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) d[i] = 0.f;
+    if (nt > 0 && !failed) {
+      if (pending) {
+        const bool ok = tid == 0 ? mbar_wait_bounded(bar, phase & 1) : true;
+        if (__syncthreads_or(!ok)) failed = true;
+        else { phase++; pending = false; }
+      }
+      if (!failed) {
+        tc_fence_after();
+        const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)((warp >> 2) * 8);
+        tmem_ld_32x32b_x8(taddr, d);
+      }
+    }
+    const int f = (warp & 3) * 32 + lane;
+    if (f < fc) {
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const int r = (warp >> 2) * 8 + i;
+        if (r0 + r < M)
+          store_row_feature<F16OUT>(C, K, (int64_t)r0 + r, f0 + f, d[i] + racc[r * kChunk + f]);
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (failed) break;
+  }
+  if (failed && tid == 0) atomicExch(pv.err, kErrMbarTimeout);
+  if (nt > 0 && warp == 0) tmem_dealloc(tmem, 32);
+}
+
+// Any K: one thread per (window row, feature), scalar loads.
+template <bool F16OUT>
+__global__ void routed_generic_kernel(PlanView pv, const __half* __restrict__ B, int K, void* C,
+                                      int route_mask) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (int64_t)pv.n_rows * K) return;
+  const int row = (int)(idx / K), f = (int)(idx % K);
+  const int w = row / kBlockRows, n = row % kBlockRows;
+  float acc = 0.f;
+  const int tsplit = pv.win_split[w];
+  for (int t = pv.win_tile[w]; t < pv.win_tile[w + 1]; ++t) {
+    if (t < tsplit && !(route_mask & TR_ROUTE_TC)) continue;
+    if (t >= tsplit && !(route_mask & TR_ROUTE_SPTC)) continue;
+    for (int k = 0; k < 16; ++k) {
+      const int c = pv.tile_col[(int64_t)t * 16 + k];
+      if (c < 0) continue;
+      const uint16_t a = pv.tile_a[(int64_t)t * 256 + (n / 8) * 128 + (k / 8) * 64 + (n % 8) * 8 + k % 8];
+      acc = fmaf(__half2float(__ushort_as_half(a)), __half2float(B[(int64_t)c * K + f]), acc);
+    }
+  }
+  if (route_mask & TR_ROUTE_CUDA) {
+    for (int e = pv.res_ptr[row]; e < pv.res_ptr[row + 1]; ++e)
+      acc = fmaf(__half2float(__ushort_as_half(pv.res_val[e])),
+                 __half2float(B[(int64_t)pv.res_col[e] * K + f]), acc);
+  }
+  store_row_feature<F16OUT>(C, K, row, f, acc);
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+}  // namespace
+
+int launch_csr(const int32_t* indptr, const int32_t* indices, const uint16_t* values, int32_t m,
+               const uint16_t* b, int32_t k, void* c, int c_dtype, cudaStream_t stream) {
+  if (m == 0 || k == 0) return TR_OK;
+  const __half* vh = reinterpret_cast<const __half*>(values);
+  const __half* bh = reinterpret_cast<const __half*>(b);
+  const bool f16 = c_dtype == TR_OUT_F16;
+  if (k % 8 == 0 && aligned16(b)) {
+    const int blocks = (m + kBlockRows - 1) / kBlockRows;
+    if (f16) csr_block_kernel<true><<<blocks, kThreads, 0, stream>>>(indptr, indices, vh, m, bh, k, c);
+    else csr_block_kernel<false><<<blocks, kThreads, 0, stream>>>(indptr, indices, vh, m, bh, k, c);
+  } else {
+    const int64_t n = (int64_t)m * k;
+    const int blocks = (int)((n + 255) / 256);
+    if (f16) csr_generic_kernel<true><<<blocks, 256, 0, stream>>>(indptr, indices, vh, m, bh, k, c);
+    else csr_generic_kernel<false><<<blocks, 256, 0, stream>>>(indptr, indices, vh, m, bh, k, c);
+  }
+  TRS_CUDA(cudaGetLastError());
+  return TR_OK;
+}
+
+int launch_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_dtype,
+                  int route_mask, cudaStream_t stream) {
+  const PlanView& v = p->view;
+  if (v.n_rows == 0 || k == 0) return TR_OK;
+  const __half* bh = reinterpret_cast<const __half*>(b);
+  const bool f16 = c_dtype == TR_OUT_F16;
+  if (k % 8 == 0 && aligned16(b)) {
+    static_assert(kSmemRouted <= 48 * 1024, "routed kernel shared memory exceeds the default limit");
+    if (f16) routed_kernel<true><<<v.n_windows, kThreads, kSmemRouted, stream>>>(v, bh, k, c, route_mask);
+    else routed_kernel<false><<<v.n_windows, kThreads, kSmemRouted, stream>>>(v, bh, k, c, route_mask);
+  } else {
+    const int64_t n = (int64_t)v.n_rows * k;
+    const int blocks = (int)((n + 255) / 256);
+    if (f16) routed_generic_kernel<true><<<blocks, 256, 0, stream>>>(v, bh, k, c, route_mask);
+    else routed_generic_kernel<false><<<blocks, 256, 0, stream>>>(v, bh, k, c, route_mask);
+  }
+  TRS_CUDA(cudaGetLastError());
+  return TR_OK;
+}
+
+}  // namespace trs

@@ -1,0 +1,16 @@
+// Kernel launchers (spmm.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "plan.h"
+
+namespace trs {
+
+int launch_csr(const int32_t* indptr, const int32_t* indices, const uint16_t* values, int32_t m,
+               const uint16_t* b, int32_t k, void* c, int c_dtype, cudaStream_t stream);
+int launch_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_dtype,
+                  int route_mask, cudaStream_t stream);
+
+}  // namespace trs

@@ -1,0 +1,14 @@
+"""trspmm — B200-native three-way routed FP16 SpMM (host side).
+
+The compute lives in libtrspmm.so (CUDA for sm_100a, C ABI in
+include/trspmm.h); this package binds it with ctypes and mirrors the
+reference's Python-facing operators.  There is no CPU fallback: every entry
+point that computes raises if the library or a CUDA device is missing.
+"""
+from ._lib import (TR_OUT_F16, TR_OUT_F32, TR_ROUTE_ALL, TR_ROUTE_CUDA, TR_ROUTE_SPTC,
+                   TR_ROUTE_TC, EXPORTED, LIB_PATH, TrError, lib)
+from .core import TABLE_NAMES, Plan, route, spmm_csr, tables_struct
+
+__all__ = ["TR_OUT_F16", "TR_OUT_F32", "TR_ROUTE_ALL", "TR_ROUTE_CUDA", "TR_ROUTE_SPTC",
+           "TR_ROUTE_TC", "EXPORTED", "LIB_PATH", "TrError", "lib", "TABLE_NAMES", "Plan",
+           "route", "spmm_csr", "tables_struct"]

@@ -1,0 +1,236 @@
+"""Host-side API over libtrspmm: routing, device plans, forward SpMM.
+
+  route(...)              the three-stage router -> the reference's 30 tables
+  Plan.from_tables(...)   device plan from route tables (reference layout)
+  Plan.from_csr(...)      route with this library's router and build the plan
+  Plan.spmm(B)            routed forward C = A_plan . B on the GPU
+  spmm_csr(...)           the plain single-route CSR kernel
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import _lib
+from ._lib import (TR_OUT_F16, TR_OUT_F32, TR_ROUTE_ALL, TR_ROUTE_COMPAT, TR_ROUTE_EXACT,
+                   PlanInfo, RouteParams, Tables, check, lib)
+
+TABLE_NAMES = [
+    "t_row_offset", "t_block_offset", "t_column", "t_value", "t_window_row", "t_atomic",
+    "t_binary",
+    "c_row_offset", "c_row", "c_atomic", "c_column", "c_value",
+    "c_row_offset_short", "c_row_short", "c_atomic_short", "c_column_short", "c_value_short",
+    "s_column", "s_mask", "s_value", "s_pos", "s_window", "s_offsets",
+    "s_tile_window", "s_tile_group", "s_tile_column", "s_packed_a", "s_packed_meta",
+    "s_window_tile_offset", "duration",
+]
+_DTYPES = [np.int32, np.int32, np.int32, np.float32, np.int32, np.int32, np.int64,
+           np.int32, np.int32, np.int32, np.int32, np.float32,
+           np.int32, np.int32, np.int32, np.int32, np.float32,
+           np.int32, np.uint8, np.float32, np.int8, np.int32, np.int32,
+           np.int32, np.int32, np.int32, np.int32, np.int32, np.int32]
+
+
+def _vp(a):
+    return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else ctypes.c_void_p(0)
+
+
+def _params(partsize_t=32, partsize_c=32, shortsize=3, density=8, window=16, wide=16,
+            tc_min_util=0.0, sptc_min_util=0.5, sptc_threshold=12, unit_min_nnz=None,
+            skip_tc=None, mode="compat", threads=0):
+    if unit_min_nnz is None:
+        unit_min_nnz = int(os.environ.get("LIBRA_SPTC_UNIT_MIN_NNZ", "2"))
+    if skip_tc is None:
+        skip_tc = os.environ.get("LIBRA_SKIP_TC", "0") in ("1", "true", "TRUE")
+    m = {"compat": TR_ROUTE_COMPAT, "exact": TR_ROUTE_EXACT}[mode]
+    return RouteParams(int(partsize_t), int(partsize_c), int(shortsize), int(density), int(window),
+                       int(wide), float(tc_min_util), float(sptc_min_util), int(sptc_threshold),
+                       int(unit_min_nnz), int(bool(skip_tc)), m, int(threads))
+
+
+def route(indptr, indices, values, partsize_t=32, partsize_c=32, shortsize=3, density=8,
+          window=16, wide=16, tc_min_util=0.0, sptc_min_util=0.5, sptc_threshold=12,
+          mode="compat", unit_min_nnz=None, skip_tc=None, threads=0):
+    """Route a CSR matrix; returns the 30 tables of block_sptc_2to4_online
+    (TR-source/Block/block_online.cpp:844-870) as numpy arrays, the last being
+    the routing time in seconds (float32)."""
+    L = lib()
+    rp = np.ascontiguousarray(indptr, dtype=np.int32)
+    ci = np.ascontiguousarray(indices, dtype=np.int32)
+    vv = np.ascontiguousarray(values, dtype=np.float32)
+    prm = _params(partsize_t, partsize_c, shortsize, density, window, wide, tc_min_util,
+                  sptc_min_util, sptc_threshold, unit_min_nnz, skip_tc, mode, threads)
+    h = ctypes.c_void_p()
+    check(L.tr_route_build(_vp(rp), _vp(ci), _vp(vv), rp.shape[0] - 1, ctypes.byref(prm),
+                           ctypes.byref(h)))
+    try:
+        out = []
+        for i, dt in enumerate(_DTYPES):
+            data = ctypes.c_void_p()
+            n = ctypes.c_int64()
+            check(L.tr_route_table(h, i, ctypes.byref(data), ctypes.byref(n)))
+            if n.value == 0:
+                out.append(np.zeros(0, dtype=dt))
+            else:
+                nbytes = n.value * np.dtype(dt).itemsize
+                buf = (ctypes.c_char * nbytes).from_address(data.value)
+                out.append(np.frombuffer(buf, dtype=dt, count=n.value).copy())
+        seconds = L.tr_route_seconds(h)
+    finally:
+        L.tr_route_free(h)
+    g = out[21].shape[0]
+    t = out[23].shape[0]
+    out[17] = out[17].reshape(g, 4)
+    out[18] = out[18].reshape(g, window)
+    out[19] = out[19].reshape(g, window, 2)
+    out[20] = out[20].reshape(g, window, 2)
+    out[25] = out[25].reshape(t, 16)
+    out[26] = out[26].reshape(t, 8, 4, 2)
+    out[27] = out[27].reshape(t, 8)
+    out.append(np.float32(seconds))
+    return out
+
+
+def _half_bits(x):
+    a = np.ascontiguousarray(x)
+    if a.dtype != np.float16:
+        a = a.astype(np.float32).astype(np.float16)
+    return a.view(np.uint16)
+
+
+def _np(x, dtype):
+    if hasattr(x, "detach"):
+        x = x.detach().cpu().numpy()
+    return np.ascontiguousarray(x, dtype=dtype)
+
+
+def tables_struct(tabs):
+    """ctypes Tables struct over a 30-table list (values rounded to FP16);
+    returns (struct, keepalive list)."""
+    T = dict(zip(TABLE_NAMES, tabs))
+    keep = {
+        "t_row_offset": _np(T["t_row_offset"], np.int32),
+        "t_block_offset": _np(T["t_block_offset"], np.int32),
+        "t_column": _np(T["t_column"], np.int32),
+        "t_value": _half_bits(_np(T["t_value"], None)),
+        "t_window_row": _np(T["t_window_row"], np.int32),
+        "t_binary": _np(T["t_binary"], np.int64),
+        "c_row_offset": _np(T["c_row_offset"], np.int32),
+        "c_row": _np(T["c_row"], np.int32),
+        "c_column": _np(T["c_column"], np.int32),
+        "c_value": _half_bits(_np(T["c_value"], None)),
+        "cs_row_offset": _np(T["c_row_offset_short"], np.int32),
+        "cs_row": _np(T["c_row_short"], np.int32),
+        "cs_column": _np(T["c_column_short"], np.int32),
+        "cs_value": _half_bits(_np(T["c_value_short"], None)),
+        "s_tile_column": _np(T["s_tile_column"], np.int32).ravel(),
+        "s_packed_a": _np(T["s_packed_a"], np.int32).ravel(),
+        "s_packed_meta": _np(T["s_packed_meta"], np.int32).ravel(),
+        "s_window_tile_offset": _np(T["s_window_tile_offset"], np.int32),
+    }
+    st = Tables()
+    for name, arr in keep.items():
+        setattr(st, name, arr.ctypes.data if arr.size else None)
+        setattr(st, "n_" + name, int(arr.size))
+    return st, keep
+
+
+class Plan:
+    """Routed operand resident in HBM (see csrc/plan.h for its layout)."""
+
+    def __init__(self, handle):
+        self._h = handle
+        info = PlanInfo()
+        check(lib().tr_plan_info_get(self._h, ctypes.byref(info)))
+        self.info = {f: getattr(info, f) for f, _ in PlanInfo._fields_}
+        self.n_rows = info.n_rows
+        self.n_cols = info.n_cols
+
+    @classmethod
+    def from_tables(cls, tabs, n_rows, n_cols, window=16):
+        st, keep = tables_struct(tabs)
+        h = ctypes.c_void_p()
+        check(lib().tr_plan_from_tables(ctypes.byref(st), int(n_rows), int(n_cols), int(window),
+                                        ctypes.byref(h)))
+        del keep
+        return cls(h)
+
+    @classmethod
+    def from_csr(cls, indptr, indices, values, n_rows, n_cols, mode="exact", **route_kw):
+        rp = np.ascontiguousarray(indptr, dtype=np.int32)
+        ci = np.ascontiguousarray(indices, dtype=np.int32)
+        vv = np.ascontiguousarray(values, dtype=np.float32)
+        prm = _params(mode=mode, **route_kw)
+        h = ctypes.c_void_p()
+        check(lib().tr_plan_from_csr(_vp(rp), _vp(ci), _vp(vv), int(n_rows), int(n_cols),
+                                     ctypes.byref(prm), ctypes.byref(h)))
+        return cls(h)
+
+    def spmm(self, b, out=None, out_dtype=None, route_mask=TR_ROUTE_ALL, stream=None):
+        """C = A_plan . B for a CUDA FP16 tensor B [n_cols, K]."""
+        import torch
+        _check_b(b, self.n_cols)
+        k = b.shape[1]
+        if out is None:
+            out = torch.empty((self.n_rows, k), dtype=out_dtype or torch.float32, device=b.device)
+        _check_out(out, self.n_rows, k)
+        s = stream if stream is not None else torch.cuda.current_stream(b.device).cuda_stream
+        check(lib().tr_spmm_routed(self._h, ctypes.c_void_p(b.data_ptr()), int(k),
+                                   ctypes.c_void_p(out.data_ptr()), _odt(out), int(route_mask),
+                                   ctypes.c_void_p(s)))
+        return out
+
+    def close(self):
+        if self._h:
+            lib().tr_plan_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _odt(out):
+    import torch
+    if out.dtype == torch.float32:
+        return TR_OUT_F32
+    if out.dtype == torch.float16:
+        return TR_OUT_F16
+    raise TypeError("output must be float32 or float16")
+
+
+def _check_b(b, n_cols):
+    import torch
+    if not (b.is_cuda and b.dtype == torch.float16 and b.dim() == 2 and b.is_contiguous()):
+        raise RuntimeError("B must be a contiguous 2-D float16 CUDA tensor")
+    if b.shape[0] != n_cols:
+        raise RuntimeError(f"B has {b.shape[0]} rows, the matrix has {n_cols} columns")
+
+
+def _check_out(out, m, k):
+    if not (out.is_cuda and out.is_contiguous() and tuple(out.shape) == (m, k)):
+        raise RuntimeError(f"out must be a contiguous CUDA tensor of shape ({m}, {k})")
+
+
+def spmm_csr(indptr, indices, values, b, n_rows, out=None, out_dtype=None, stream=None):
+    """Plain CSR SpMM (single CUDA-core route) on CUDA tensors: int32
+    indptr/indices, FP16 values, FP16 B [n_cols, K]."""
+    import torch
+    _check_b(b, b.shape[0])
+    k = b.shape[1]
+    if out is None:
+        out = torch.empty((n_rows, k), dtype=out_dtype or torch.float32, device=b.device)
+    _check_out(out, n_rows, k)
+    for t, dt in ((indptr, torch.int32), (indices, torch.int32), (values, torch.float16)):
+        if not (t.is_cuda and t.dtype == dt and t.is_contiguous()):
+            raise RuntimeError("indptr/indices must be int32 and values float16 contiguous CUDA tensors")
+    s = stream if stream is not None else torch.cuda.current_stream(b.device).cuda_stream
+    check(lib().tr_spmm_csr(ctypes.c_void_p(indptr.data_ptr()), ctypes.c_void_p(indices.data_ptr()),
+                            ctypes.c_void_p(values.data_ptr()), int(n_rows), int(b.shape[0]),
+                            int(indices.numel()), ctypes.c_void_p(b.data_ptr()), int(k),
+                            ctypes.c_void_p(out.data_ptr()), _odt(out), ctypes.c_void_p(s)))
+    return out
