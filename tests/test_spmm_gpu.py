@@ -172,10 +172,15 @@ def test_bad_device_arguments_raise(cuda):
         plan.spmm(torch.zeros((41, 8), dtype=torch.float16, device=cuda))
     with pytest.raises(RuntimeError):
         plan.spmm(torch.zeros((40, 8), dtype=torch.float32, device=cuda))
-    bad = trspmm.route(g.indptr, g.indices, g.values)
-    bad[10] = bad[10] + 1000          # CUDA columns out of range
-    with pytest.raises(RuntimeError, match="out of range"):
-        trspmm.Plan.from_tables(bad, g.n_rows, g.n_cols)
+    tabs = trspmm.route(g.indptr, g.indices, g.values)
+    for idx in (10, 15, 25):          # CUDA long / short / SPTC tile columns out of range
+        if tabs[idx].size == 0:
+            continue
+        bad = list(tabs)
+        bad[idx] = np.where(tabs[idx] >= 0, tabs[idx] + 1000, tabs[idx]).astype(np.int32)
+        with pytest.raises(RuntimeError, match="out of range"):
+            trspmm.Plan.from_tables(bad, g.n_rows, g.n_cols)
+    assert tabs[25].size > 0
 
 
 def test_large_routed_workload_properties(cuda):

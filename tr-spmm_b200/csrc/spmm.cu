@@ -29,7 +29,6 @@ constexpr int kBlockRows = 16;      // rows per window / row block
 constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
 constexpr int kChunk = 128;         // features per pass (UMMA M)
-constexpr int kStages = 4;          // tiles gathered per MMA batch
 constexpr int kUnroll = 4;          // independent 16-byte B loads in flight per lane
 
 __device__ __forceinline__ void fma8(float (&acc)[8], float v, const uint4& b) {
@@ -42,27 +41,39 @@ __device__ __forceinline__ void fma8(float (&acc)[8], float v, const uint4& b) {
   }
 }
 
-// Adds the CSR rows of one 16-row block (row pointer rp[0..16] in shared
-// memory, absolute entry indices) times B[:, f0 : f0+fc] into racc[16][kChunk]
-// (shared, FP32).  Entries are split evenly across the CTA's warps; inside a
-// warp, groups of L lanes (L*8 >= fc) each take one entry and load 16 bytes
-// of its B row per lane.  A lane group flushes its partial row with shared
-// atomics whenever its entries cross a row boundary.
-__device__ __forceinline__ void block_accumulate(const int* rp, const int32_t* __restrict__ col,
-                                                 const __half* __restrict__ val,
-                                                 const __half* __restrict__ B, int K, int f0,
-                                                 int fc, float* racc) {
+// Staged CUDA-core engine.  The entries of a 16-row block (row pointer rp[]
+// in shared memory, absolute entry indices) are processed in chunks of up to
+// kStage entries: each chunk's column indices and values are first copied
+// into shared memory in one coalesced pass (one exposed memory latency per
+// chunk instead of one per batch of B loads), then every warp takes an even
+// share of the chunk.  Inside a warp, groups of L lanes (L*8 >= fc) each take
+// one entry and load 16 bytes of its B row per lane, kUnroll entries per lane
+// group in flight.  A lane group accumulates in FP32 registers and flushes
+// its partial row into racc[16][kChunk] (shared, FP32) with shared atomics
+// when its entries cross a row boundary.
+constexpr int kStage = 1024;
+
+__device__ __forceinline__ void stage_chunk(const int32_t* __restrict__ col,
+                                            const __half* __restrict__ val, int e0, int n,
+                                            int* scol, float* sval) {
+  for (int i = threadIdx.x; i < n; i += kThreads) {
+    scol[i] = __ldg(col + e0 + i);
+    sval[i] = __half2float(val[e0 + i]);
+  }
+}
+
+__device__ __forceinline__ void accumulate_chunk(const int* rp, int e0, int n, const int* scol,
+                                                 const float* sval, const __half* __restrict__ B,
+                                                 int K, int f0, int fc, float* racc) {
   int L = 1;
   while (L * 8 < fc) L <<= 1;
   const int G = 32 / L;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int g = lane / L, li = lane % L;
   const bool active = li * 8 < fc;
-  const int e_begin = rp[0], e_end = rp[kBlockRows];
-  const int total = e_end - e_begin;
-  const int per = (total + kWarps - 1) / kWarps;
-  const int eb = e_begin + warp * per;
-  const int ee = min(e_end, eb + per);
+  const int per = (n + kWarps - 1) / kWarps;
+  const int eb = warp * per;
+  const int ee = min(n, eb + per);
   if (eb >= ee) return;
   float acc[8];
 #pragma unroll
@@ -70,45 +81,55 @@ __device__ __forceinline__ void block_accumulate(const int* rp, const int32_t* _
   int row = 0;
   int cur = -1;
   const __half* Bf = B + f0 + li * 8;
-  for (int e0 = eb + g; e0 < ee; e0 += G * kUnroll) {
-    int cidx[kUnroll];
-    float v[kUnroll];
+  for (int i0 = eb + g; i0 < ee; i0 += G * kUnroll) {
     uint4 bv[kUnroll];
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
-      const int e = e0 + u * G;
-      cidx[u] = e < ee ? __ldg(col + e) : -1;
-      v[u] = e < ee ? __half2float(val[e]) : 0.f;
-    }
-#pragma unroll
-    for (int u = 0; u < kUnroll; ++u) {
-      if (cidx[u] >= 0 && active)
-        bv[u] = __ldg(reinterpret_cast<const uint4*>(Bf + (size_t)cidx[u] * K));
+      const int i = i0 + u * G;
+      const int c = i < ee ? scol[i] : -1;
+      if (c >= 0 && active)
+        bv[u] = __ldg(reinterpret_cast<const uint4*>(Bf + (size_t)c * K));
       else
         bv[u] = make_uint4(0, 0, 0, 0);
     }
 #pragma unroll
     for (int u = 0; u < kUnroll; ++u) {
-      const int e = e0 + u * G;
-      if (e >= ee) break;
+      const int i = i0 + u * G;
+      if (i >= ee) break;
+      const int e = e0 + i;
       while (rp[row + 1] <= e) ++row;
       if (row != cur) {
         if (cur >= 0 && active) {
           float* dst = racc + cur * kChunk + li * 8;
 #pragma unroll
-          for (int i = 0; i < 8; ++i) atomicAdd(dst + i, acc[i]);
+          for (int q = 0; q < 8; ++q) atomicAdd(dst + q, acc[q]);
         }
 #pragma unroll
-        for (int i = 0; i < 8; ++i) acc[i] = 0.f;
+        for (int q = 0; q < 8; ++q) acc[q] = 0.f;
         cur = row;
       }
-      fma8(acc, v[u], bv[u]);
+      fma8(acc, sval[i], bv[u]);
     }
   }
   if (cur >= 0 && active) {
     float* dst = racc + cur * kChunk + li * 8;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) atomicAdd(dst + i, acc[i]);
+    for (int q = 0; q < 8; ++q) atomicAdd(dst + q, acc[q]);
+  }
+}
+
+// All entries of the block, chunk by chunk (every thread of the CTA calls it).
+__device__ __forceinline__ void block_accumulate(const int* rp, const int32_t* __restrict__ col,
+                                                 const __half* __restrict__ val,
+                                                 const __half* __restrict__ B, int K, int f0,
+                                                 int fc, float* racc, int* scol, float* sval) {
+  const int e_begin = rp[0], e_end = rp[kBlockRows];
+  for (int c0 = e_begin; c0 < e_end; c0 += kStage) {
+    const int n = min(kStage, e_end - c0);
+    __syncthreads();                       // previous chunk fully consumed
+    stage_chunk(col, val, c0, n, scol, sval);
+    __syncthreads();
+    accumulate_chunk(rp, c0, n, scol, sval, B, K, f0, fc, racc);
   }
 }
 
@@ -128,6 +149,8 @@ __global__ void __launch_bounds__(kThreads) csr_block_kernel(
     const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
     const __half* __restrict__ values, int M, const __half* __restrict__ B, int K, void* C) {
   __shared__ __align__(16) float racc[kBlockRows * kChunk];
+  __shared__ int scol[kStage];
+  __shared__ float sval[kStage];
   __shared__ int rp[kBlockRows + 1];
   const int r0 = blockIdx.x * kBlockRows;
   if (threadIdx.x <= kBlockRows) rp[threadIdx.x] = indptr[min(r0 + (int)threadIdx.x, M)];
@@ -135,7 +158,7 @@ __global__ void __launch_bounds__(kThreads) csr_block_kernel(
     const int fc = min(kChunk, K - f0);
     for (int i = threadIdx.x; i < kBlockRows * kChunk; i += kThreads) racc[i] = 0.f;
     __syncthreads();
-    block_accumulate(rp, indices, values, B, K, f0, fc, racc);
+    block_accumulate(rp, indices, values, B, K, f0, fc, racc, scol, sval);
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int f = (warp & 3) * 32 + lane;
@@ -169,31 +192,41 @@ __global__ void csr_generic_kernel(const int32_t* __restrict__ indptr,
 // Fused routed forward
 // ---------------------------------------------------------------------------
 // Shared memory (dynamic, 1024-aligned base):
-//   [kStages][4096]  A operand: 16 gathered B rows x 128 features, MN-major,
-//                    128-byte swizzle; atoms of 8 rows x 64 features:
+//   aop[2][kHalf][4096] A operand: 16 gathered B rows x 128 features,
+//                    MN-major, 128-byte swizzle; atoms of 8 rows x 64 features:
 //                    (k, f) -> (k/8)*2048 + (f/64)*1024 + (k%8)*128 +
 //                              (((f%64)/8) ^ (k%8))*16 + (f%8)*2
-//   [kStages][512]   B operand: the 16x16 A tile (K-major, no swizzle)
+//   bop[2][kHalf][512]  B operand: the 16x16 A tile (K-major, no swizzle)
 //   racc[16][128]    residual rows (FP32)
-//   rp[17], mbar, tmem base
+//   scol/sval[kStage] staged indices: the window's tile columns while the
+//                    tensor-core tiles are gathered, then residual entries
+//   rp[17], mbar[2], tmem base
+// Tiles go through a two-deep pipeline of batches of kHalf tiles: the
+// cp.async gathers of batch b+1 are in flight while batch b waits for its
+// copies and its MMAs run; each half of the stage buffers has its own
+// mbarrier that the MMA commit arrives on.
+constexpr int kHalf = 4;
 constexpr int kAOpBytes = 4096;
 constexpr int kBOpBytes = 512;
-constexpr int kSmemRouted = 1024 + kStages * (kAOpBytes + kBOpBytes) +
-                            kBlockRows * kChunk * 4 + 128;
+constexpr int kTileColCap = kStage / 16;    // tiles whose columns fit the staging buffer
+constexpr int kSmemRouted = 1024 + 2 * kHalf * (kAOpBytes + kBOpBytes) + kBlockRows * kChunk * 4 +
+                            kStage * 8 + 128;
 constexpr uint32_t kIdesc = umma_idesc_f16(128, 16, /*a MN-major*/ true, /*b MN-major*/ false);
 
 template <bool F16OUT>
-__global__ void __launch_bounds__(kThreads) routed_kernel(PlanView pv, const __half* __restrict__ B,
+__global__ void __launch_bounds__(kThreads, 3) routed_kernel(PlanView pv, const __half* __restrict__ B,
                                                           int K, void* C, int route_mask) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint8_t* aop = smem;
-  uint8_t* bop = smem + kStages * kAOpBytes;
-  float* racc = reinterpret_cast<float*>(bop + kStages * kBOpBytes);
-  int* rp = reinterpret_cast<int*>(racc + kBlockRows * kChunk);
+  uint8_t* bop = smem + 2 * kHalf * kAOpBytes;
+  float* racc = reinterpret_cast<float*>(bop + 2 * kHalf * kBOpBytes);
+  int* scol = reinterpret_cast<int*>(racc + kBlockRows * kChunk);
+  float* sval = reinterpret_cast<float*>(scol + kStage);
+  int* rp = reinterpret_cast<int*>(sval + kStage);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(rp + 18);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int w = pv.win_order[blockIdx.x];
@@ -205,7 +238,8 @@ __global__ void __launch_bounds__(kThreads) routed_kernel(PlanView pv, const __h
   int tb0 = ta1, tb1 = pv.win_tile[w + 1];
   if (!(route_mask & TR_ROUTE_TC)) ta1 = ta0;
   if (!(route_mask & TR_ROUTE_SPTC)) tb1 = tb0;
-  const int nt = (ta1 - ta0) + (tb1 - tb0);
+  const int n_tc = ta1 - ta0;
+  const int nt = n_tc + (tb1 - tb0);
   const bool do_res = (route_mask & TR_ROUTE_CUDA) != 0;
 
   if (tid <= kBlockRows) {
@@ -213,14 +247,14 @@ __global__ void __launch_bounds__(kThreads) routed_kernel(PlanView pv, const __h
     rp[tid] = do_res ? pv.res_ptr[rr] : 0;
   }
   uint32_t tmem = 0;
-  const uint32_t bar = smem_u32(mbar);
   if (nt > 0) {
     if (warp == 0) {
       tmem_alloc(smem_u32(tmem_slot), 32);
       tmem_relinquish();
     }
     if (tid == 0) {
-      mbar_init(bar, 1);
+      mbar_init(smem_u32(&mbar[0]), 1);
+      mbar_init(smem_u32(&mbar[1]), 1);
       fence_mbar_init();
     }
   }
@@ -229,75 +263,102 @@ __global__ void __launch_bounds__(kThreads) routed_kernel(PlanView pv, const __h
   tc_fence_after();
   if (nt > 0) tmem = *tmem_slot;
 
-  uint32_t phase = 0;      // completed commits observed
-  bool pending = false;    // a commit not yet waited for
+  // commits issued / waited per mbarrier; every commit is waited for, in order
+  uint32_t issued[2] = {0, 0}, waited[2] = {0, 0};
   bool failed = false;
+  // Waits for all outstanding commits on barrier h (thread 0 spins, bounded;
+  // the barrier broadcasts the outcome so the CTA stays uniform).
+  auto drain = [&](int h) -> bool {
+    bool ok = true;
+    if (tid == 0)
+      while (ok && waited[h] < issued[h]) {
+        ok = mbar_wait_bounded(smem_u32(&mbar[h]), waited[h] & 1);
+        waited[h]++;
+      }
+    waited[h] = issued[h];
+    return !__syncthreads_or(!ok);
+  };
 
-  for (int f0 = 0; f0 < K; f0 += kChunk) {
+  for (int f0 = 0; f0 < K && !failed; f0 += kChunk) {
     const int fc = min(kChunk, K - f0);
-    // ---- tensor-core tiles ---------------------------------------------------
-    for (int tb = 0; tb < nt && !failed; tb += kStages) {
-      const int nb = min(kStages, nt - tb);
-      if (pending) {
-        // thread 0 observes the MMA completion; the barrier orders the rest
-        const bool ok = tid == 0 ? mbar_wait_bounded(bar, phase & 1) : true;
-        if (__syncthreads_or(!ok)) { failed = true; break; }
-        phase++;
-        pending = false;
-      }
-      for (int s = 0; s < nb; ++s) {
-        const int ti = tb + s;
-        const int t = ti < (ta1 - ta0) ? ta0 + ti : tb0 + (ti - (ta1 - ta0));
-        // 16 rows x 16 chunks of 16 bytes: one chunk per thread
-        const int k = tid >> 4, j = tid & 15;
-        const int c = __ldg(pv.tile_col + (int64_t)t * 16 + k);
-        const bool ok = c >= 0 && j * 8 < fc;
-        const __half* src = ok ? B + (int64_t)c * K + f0 + j * 8 : B;
-        const uint32_t dst = smem_u32(aop + s * kAOpBytes) + (k >> 3) * 2048 + (j >> 3) * 1024 +
-                             (k & 7) * 128 + (((j & 7) ^ (k & 7)) << 4);
-        cp_async16(dst, src, ok ? 16 : 0);
-        if (tid < 32) {
-          const uint16_t* asrc = pv.tile_a + (int64_t)t * 256 + tid * 8;
-          cp_async16(smem_u32(bop + s * kBOpBytes) + tid * 16, asrc, 16);
-        }
-      }
-      cp_async_commit();
-      cp_async_wait_all();
-      fence_proxy_async_smem();
+    // ---- tensor-core tiles, in rounds whose columns fit the staging buffer ----
+    bool first_mma = true;
+    for (int rb = 0; rb < nt && !failed; rb += kTileColCap) {
+      const int nr = min(kTileColCap, nt - rb);
       __syncthreads();
-      if (tid == 0) {
-        tc_fence_after();
-        for (int s = 0; s < nb; ++s) {
-          const uint64_t adesc = umma_smem_desc(smem_u32(aop + s * kAOpBytes), 1024, 2048, 2);
-          const uint64_t bdesc = umma_smem_desc(smem_u32(bop + s * kBOpBytes), 128, 256, 0);
-          umma_f16(tmem, adesc, bdesc, kIdesc, (tb + s) > 0 ? 1u : 0u);
-        }
-        umma_commit(bar);
+      for (int i = tid; i < nr * 16; i += kThreads) {
+        const int ti = rb + i / 16;
+        const int t = ti < n_tc ? ta0 + ti : tb0 + (ti - n_tc);
+        scol[i] = __ldg(pv.tile_col + (int64_t)t * 16 + (i & 15));
       }
-      pending = true;
+      __syncthreads();
+      const int nbat = (nr + kHalf - 1) / kHalf;
+      auto issue = [&](int b) {
+        const int h = b & 1;
+        const int nb = min(kHalf, nr - b * kHalf);
+        for (int s = 0; s < nb; ++s) {
+          const int li = b * kHalf + s;                     // tile within the round
+          const int ti = rb + li;
+          const int t = ti < n_tc ? ta0 + ti : tb0 + (ti - n_tc);
+          const int k = tid >> 4, j = tid & 15;             // row k, 16-byte chunk j
+          const int c = scol[li * 16 + k];
+          const bool ok = c >= 0 && j * 8 < fc;
+          const __half* src = ok ? B + (int64_t)c * K + f0 + j * 8 : B;
+          const uint32_t dst = smem_u32(aop + (h * kHalf + s) * kAOpBytes) + (k >> 3) * 2048 +
+                               (j >> 3) * 1024 + (k & 7) * 128 + (((j & 7) ^ (k & 7)) << 4);
+          cp_async16(dst, src, ok ? 16 : 0);
+          if (tid < 32)
+            cp_async16(smem_u32(bop + (h * kHalf + s) * kBOpBytes) + tid * 16,
+                       pv.tile_a + (int64_t)t * 256 + tid * 8, 16);
+        }
+        cp_async_commit();
+      };
+      if (!drain(0) || !drain(1)) { failed = true; break; }   // stage buffers free
+      issue(0);
+      for (int b = 0; b < nbat; ++b) {
+        if (b + 1 < nbat) {
+          if (!drain((b + 1) & 1)) { failed = true; break; }   // MMAs of batch b-1 done
+          issue(b + 1);
+          asm volatile("cp.async.wait_group 1;\n" ::: "memory");
+        } else {
+          cp_async_wait_all();
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+          const int h = b & 1;
+          const int nb = min(kHalf, nr - b * kHalf);
+          tc_fence_after();
+          for (int s = 0; s < nb; ++s) {
+            const uint64_t adesc =
+                umma_smem_desc(smem_u32(aop + (h * kHalf + s) * kAOpBytes), 1024, 2048, 2);
+            const uint64_t bdesc =
+                umma_smem_desc(smem_u32(bop + (h * kHalf + s) * kBOpBytes), 128, 256, 0);
+            umma_f16(tmem, adesc, bdesc, kIdesc, first_mma ? 0u : 1u);
+            first_mma = false;
+          }
+          umma_commit(smem_u32(&mbar[h]));
+        }
+        first_mma = false;
+        issued[b & 1]++;
+      }
     }
+    if (failed) break;
     // ---- CUDA-core residual --------------------------------------------------
     for (int i = tid; i < kBlockRows * kChunk; i += kThreads) racc[i] = 0.f;
-    __syncthreads();
     if (do_res)
       block_accumulate(rp, pv.res_col, reinterpret_cast<const __half*>(pv.res_val), B, K, f0, fc,
-                       racc);
+                       racc, scol, sval);
     __syncthreads();
     // ---- epilogue: D^T from TMEM + residual, one store per element ------------
     float d[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) d[i] = 0.f;
-    if (nt > 0 && !failed) {
-      if (pending) {
-        const bool ok = tid == 0 ? mbar_wait_bounded(bar, phase & 1) : true;
-        if (__syncthreads_or(!ok)) failed = true;
-        else { phase++; pending = false; }
-      }
-      if (!failed) {
-        tc_fence_after();
-        const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)((warp >> 2) * 8);
-        tmem_ld_32x32b_x8(taddr, d);
-      }
+    if (nt > 0) {
+      if (!drain(0) || !drain(1)) { failed = true; break; }
+      tc_fence_after();
+      const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)((warp >> 2) * 8);
+      tmem_ld_32x32b_x8(taddr, d);
     }
     const int f = (warp & 3) * 32 + lane;
     if (f < fc) {
@@ -311,9 +372,12 @@ __global__ void __launch_bounds__(kThreads) routed_kernel(PlanView pv, const __h
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (failed) break;
   }
-  if (failed && tid == 0) atomicExch(pv.err, kErrMbarTimeout);
+  if (failed) {
+    cp_async_wait_all();
+    if (tid == 0) atomicExch(pv.err, kErrMbarTimeout);
+  }
+  __syncthreads();
   if (nt > 0 && warp == 0) tmem_dealloc(tmem, 32);
 }
 
@@ -376,7 +440,12 @@ int launch_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c
   const __half* bh = reinterpret_cast<const __half*>(b);
   const bool f16 = c_dtype == TR_OUT_F16;
   if (k % 8 == 0 && aligned16(b)) {
-    static_assert(kSmemRouted <= 48 * 1024, "routed kernel shared memory exceeds the default limit");
+    static bool attr[2] = {false, false};
+    if (!attr[f16]) {
+      if (f16) TRS_CUDA(cudaFuncSetAttribute(routed_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemRouted));
+      else TRS_CUDA(cudaFuncSetAttribute(routed_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemRouted));
+      attr[f16] = true;
+    }
     if (f16) routed_kernel<true><<<v.n_windows, kThreads, kSmemRouted, stream>>>(v, bh, k, c, route_mask);
     else routed_kernel<false><<<v.n_windows, kThreads, kSmemRouted, stream>>>(v, bh, k, c, route_mask);
   } else {
