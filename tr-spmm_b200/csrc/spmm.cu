@@ -22,6 +22,10 @@
 #include "plan.h"
 #include "spmm.h"
 
+#ifndef TRS_MIXED_FMA
+#define TRS_MIXED_FMA 1
+#endif
+
 namespace trs {
 namespace {
 
@@ -31,40 +35,50 @@ constexpr int kThreads = kWarps * 32;
 constexpr int kChunk = 128;         // features per pass (UMMA M)
 constexpr int kUnroll = 4;          // independent 16-byte B loads in flight per lane
 
-__device__ __forceinline__ void fma8(float (&acc)[8], float v, const uint4& b) {
-  const __half2* h = reinterpret_cast<const __half2*>(&b);
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const float2 f = __half22float2(h[i]);
-    acc[2 * i] = fmaf(v, f.x, acc[2 * i]);
-    acc[2 * i + 1] = fmaf(v, f.y, acc[2 * i + 1]);
-  }
-}
-
 // Staged CUDA-core engine.  The entries of a 16-row block (row pointer rp[]
 // in shared memory, absolute entry indices) are processed in chunks of up to
-// kStage entries: each chunk's column indices and values are first copied
-// into shared memory in one coalesced pass (one exposed memory latency per
-// chunk instead of one per batch of B loads), then every warp takes an even
-// share of the chunk.  Inside a warp, groups of L lanes (L*8 >= fc) each take
-// one entry and load 16 bytes of its B row per lane, kUnroll entries per lane
-// group in flight.  A lane group accumulates in FP32 registers and flushes
-// its partial row into racc[16][kChunk] (shared, FP32) with shared atomics
-// when its entries cross a row boundary.
+// kStage entries: each chunk's (column, value) pairs are first copied into
+// shared memory in one coalesced pass (one exposed memory latency per chunk,
+// not one per batch of B loads).  Every warp then takes an even share of the
+// chunk and walks it one row run at a time, so the inner loop has no row
+// tracking and no divergence: groups of L lanes (L*8 >= fc) each take one
+// entry and load 16 bytes of its B row per lane, kUnroll entries per lane
+// group in flight, tails predicated (value 0, a valid column).  At the end of
+// a run the lane groups are reduced with shuffles and one group adds the
+// row's partial sum into racc[16][kChunk] (shared, FP32) with shared atomics
+// (a row can be split across warps).
 constexpr int kStage = 1024;
+
+// acc[0..7] += v * b[0..7]; FP16 operands, FP32 accumulation.  The product
+// of two FP16 numbers is exact in FP32, so the mixed-precision FMA
+// (fma.rn.f32.f16) equals converting both operands and using fmaf.
+__device__ __forceinline__ void fma8h(float (&acc)[8], uint16_t v, const uint4& b) {
+  const uint32_t w[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint16_t lo = (uint16_t)(w[i] & 0xFFFFu), hi = (uint16_t)(w[i] >> 16);
+#if TRS_MIXED_FMA
+    asm("fma.rn.f32.f16 %0, %1, %2, %0;" : "+f"(acc[2 * i]) : "h"(lo), "h"(v));
+    asm("fma.rn.f32.f16 %0, %1, %2, %0;" : "+f"(acc[2 * i + 1]) : "h"(hi), "h"(v));
+#else
+    const float fv = __half2float(__ushort_as_half(v));
+    acc[2 * i] = fmaf(__half2float(__ushort_as_half(lo)), fv, acc[2 * i]);
+    acc[2 * i + 1] = fmaf(__half2float(__ushort_as_half(hi)), fv, acc[2 * i + 1]);
+#endif
+  }
+}
 
 __device__ __forceinline__ void stage_chunk(const int32_t* __restrict__ col,
                                             const __half* __restrict__ val, int e0, int n,
-                                            int* scol, float* sval) {
-  for (int i = threadIdx.x; i < n; i += kThreads) {
-    scol[i] = __ldg(col + e0 + i);
-    sval[i] = __half2float(val[e0 + i]);
-  }
+                                            int2* sent) {
+  const uint16_t* v16 = reinterpret_cast<const uint16_t*>(val);
+  for (int i = threadIdx.x; i < n; i += kThreads)
+    sent[i] = make_int2(__ldg(col + e0 + i), (int)__ldg(v16 + e0 + i));
 }
 
-__device__ __forceinline__ void accumulate_chunk(const int* rp, int e0, int n, const int* scol,
-                                                 const float* sval, const __half* __restrict__ B,
-                                                 int K, int f0, int fc, float* racc) {
+__device__ __forceinline__ void accumulate_chunk(const int* rp, int e0, int n, const int2* sent,
+                                                 const __half* __restrict__ B, int K, int f0,
+                                                 int fc, float* racc) {
   int L = 1;
   while (L * 8 < fc) L <<= 1;
   const int G = 32 / L;
@@ -75,46 +89,38 @@ __device__ __forceinline__ void accumulate_chunk(const int* rp, int e0, int n, c
   const int eb = warp * per;
   const int ee = min(n, eb + per);
   if (eb >= ee) return;
-  float acc[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) acc[i] = 0.f;
+  const __half* Bf = B + f0 + (active ? li * 8 : 0);
   int row = 0;
-  int cur = -1;
-  const __half* Bf = B + f0 + li * 8;
-  for (int i0 = eb + g; i0 < ee; i0 += G * kUnroll) {
-    uint4 bv[kUnroll];
+  while (rp[row + 1] - e0 <= eb) ++row;            // warp-uniform
+  const int c_safe = sent[eb].x;                   // a valid column for predicated tails
+  for (int i = eb; i < ee;) {
+    const int rend = min(ee, rp[row + 1] - e0);
+    float acc[8];
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) {
-      const int i = i0 + u * G;
-      const int c = i < ee ? scol[i] : -1;
-      if (c >= 0 && active)
-        bv[u] = __ldg(reinterpret_cast<const uint4*>(Bf + (size_t)c * K));
-      else
-        bv[u] = make_uint4(0, 0, 0, 0);
-    }
+    for (int q = 0; q < 8; ++q) acc[q] = 0.f;
+    for (int j0 = i + g; j0 < rend; j0 += G * kUnroll) {
+      uint4 bv[kUnroll];
+      uint16_t vv[kUnroll];
 #pragma unroll
-    for (int u = 0; u < kUnroll; ++u) {
-      const int i = i0 + u * G;
-      if (i >= ee) break;
-      const int e = e0 + i;
-      while (rp[row + 1] <= e) ++row;
-      if (row != cur) {
-        if (cur >= 0 && active) {
-          float* dst = racc + cur * kChunk + li * 8;
-#pragma unroll
-          for (int q = 0; q < 8; ++q) atomicAdd(dst + q, acc[q]);
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) acc[q] = 0.f;
-        cur = row;
+      for (int u = 0; u < kUnroll; ++u) {
+        const int j = j0 + u * G;
+        const int2 en = j < rend ? sent[j] : make_int2(c_safe, 0);
+        vv[u] = (uint16_t)en.y;
+        bv[u] = __ldg(reinterpret_cast<const uint4*>(Bf + (size_t)en.x * K));
       }
-      fma8(acc, sval[i], bv[u]);
-    }
-  }
-  if (cur >= 0 && active) {
-    float* dst = racc + cur * kChunk + li * 8;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) atomicAdd(dst + q, acc[q]);
+      for (int u = 0; u < kUnroll; ++u) fma8h(acc, vv[u], bv[u]);
+    }
+    for (int off = L; off < 32; off <<= 1)
+#pragma unroll
+      for (int q = 0; q < 8; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+    if (g == 0 && active) {
+      float* dst = racc + row * kChunk + li * 8;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) atomicAdd(dst + q, acc[q]);
+    }
+    i = rend;
+    while (row < kBlockRows - 1 && rp[row + 1] - e0 <= i) ++row;
   }
 }
 
@@ -122,14 +128,14 @@ __device__ __forceinline__ void accumulate_chunk(const int* rp, int e0, int n, c
 __device__ __forceinline__ void block_accumulate(const int* rp, const int32_t* __restrict__ col,
                                                  const __half* __restrict__ val,
                                                  const __half* __restrict__ B, int K, int f0,
-                                                 int fc, float* racc, int* scol, float* sval) {
+                                                 int fc, float* racc, int2* sent) {
   const int e_begin = rp[0], e_end = rp[kBlockRows];
   for (int c0 = e_begin; c0 < e_end; c0 += kStage) {
     const int n = min(kStage, e_end - c0);
     __syncthreads();                       // previous chunk fully consumed
-    stage_chunk(col, val, c0, n, scol, sval);
+    stage_chunk(col, val, c0, n, sent);
     __syncthreads();
-    accumulate_chunk(rp, c0, n, scol, sval, B, K, f0, fc, racc);
+    accumulate_chunk(rp, c0, n, sent, B, K, f0, fc, racc);
   }
 }
 
@@ -145,12 +151,11 @@ __device__ __forceinline__ void store_row_feature(void* C, int K, int64_t row, i
 // Plain CSR (single route)
 // ---------------------------------------------------------------------------
 template <bool F16OUT>
-__global__ void __launch_bounds__(kThreads) csr_block_kernel(
+__global__ void __launch_bounds__(kThreads, 4) csr_block_kernel(
     const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
     const __half* __restrict__ values, int M, const __half* __restrict__ B, int K, void* C) {
   __shared__ __align__(16) float racc[kBlockRows * kChunk];
-  __shared__ int scol[kStage];
-  __shared__ float sval[kStage];
+  __shared__ int2 sent[kStage];
   __shared__ int rp[kBlockRows + 1];
   const int r0 = blockIdx.x * kBlockRows;
   if (threadIdx.x <= kBlockRows) rp[threadIdx.x] = indptr[min(r0 + (int)threadIdx.x, M)];
@@ -158,7 +163,7 @@ __global__ void __launch_bounds__(kThreads) csr_block_kernel(
     const int fc = min(kChunk, K - f0);
     for (int i = threadIdx.x; i < kBlockRows * kChunk; i += kThreads) racc[i] = 0.f;
     __syncthreads();
-    block_accumulate(rp, indices, values, B, K, f0, fc, racc, scol, sval);
+    block_accumulate(rp, indices, values, B, K, f0, fc, racc, sent);
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int f = (warp & 3) * 32 + lane;
@@ -222,9 +227,9 @@ __global__ void __launch_bounds__(kThreads, 3) routed_kernel(PlanView pv, const 
   uint8_t* aop = smem;
   uint8_t* bop = smem + 2 * kHalf * kAOpBytes;
   float* racc = reinterpret_cast<float*>(bop + 2 * kHalf * kBOpBytes);
-  int* scol = reinterpret_cast<int*>(racc + kBlockRows * kChunk);
-  float* sval = reinterpret_cast<float*>(scol + kStage);
-  int* rp = reinterpret_cast<int*>(sval + kStage);
+  int2* sent = reinterpret_cast<int2*>(racc + kBlockRows * kChunk);
+  int* scol = reinterpret_cast<int*>(sent);          // tile columns while gathering tiles
+  int* rp = reinterpret_cast<int*>(sent + kStage);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(rp + 18);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
 
@@ -348,7 +353,7 @@ __global__ void __launch_bounds__(kThreads, 3) routed_kernel(PlanView pv, const 
     for (int i = tid; i < kBlockRows * kChunk; i += kThreads) racc[i] = 0.f;
     if (do_res)
       block_accumulate(rp, pv.res_col, reinterpret_cast<const __half*>(pv.res_val), B, K, f0, fc,
-                       racc, scol, sval);
+                       racc, sent);
     __syncthreads();
     // ---- epilogue: D^T from TMEM + residual, one store per element ------------
     float d[8];
