@@ -202,3 +202,29 @@ def test_large_routed_workload_properties(cuda):
     rows = np.random.default_rng(0).choice(g.n_rows, 2000, replace=False)
     ref = A[rows] @ b.astype(np.float64)
     assert rel_err(out.cpu().numpy()[rows], ref) <= TOL32
+
+
+def test_blocks_with_fewer_entries_than_warps(cuda):
+    """Row blocks / windows holding 1-7 entries (fewer than the CTA's 8 warps),
+    through the plain kernel and every route of the routed kernel."""
+    rng = np.random.default_rng(11)
+    n = 160
+    rows = np.repeat(np.arange(0, n, 16), 3) + rng.integers(0, 16, size=3 * (n // 16))
+    cols = rng.integers(0, 300, size=rows.shape[0])
+    key = np.unique(rows.astype(np.int64) * 300 + cols)
+    r, c = key // 300, (key % 300).astype(np.int32)
+    indptr = np.zeros(n + 1, np.int64)
+    indptr[1:] = np.cumsum(np.bincount(r, minlength=n))
+    g = graphs.Graph(indptr.astype(np.int32), c, rng.uniform(-1, 1, c.shape[0]).astype(np.float32),
+                     n, 300)
+    A = half_csr(g.indptr, g.indices, g.values, n, 300)
+    for k in (64, 128, 256):
+        b = graphs.dense_features(300, k, seed=k)
+        ip, ix, iv, bd = _dev(g, b, cuda)
+        out = trspmm.spmm_csr(ip, ix, iv, bd, n)
+        plan = trspmm.Plan.from_csr(g.indptr, g.indices, g.values, n, 300)
+        outs = [plan.spmm(bd, route_mask=m) for m in (trspmm.TR_ROUTE_CUDA, trspmm.TR_ROUTE_ALL)]
+        torch.cuda.synchronize()
+        ref = spmm_ref(A, b)
+        assert rel_err(out.cpu().numpy(), ref) <= TOL32
+        assert rel_err(outs[1].cpu().numpy(), ref) <= TOL32

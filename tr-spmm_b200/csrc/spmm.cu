@@ -33,24 +33,21 @@ constexpr int kBlockRows = 16;      // rows per window / row block
 constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
 constexpr int kChunk = 128;         // features per pass (UMMA M)
+constexpr int kUnroll = 4;          // independent 16-byte B loads in flight per lane
 
 // Staged CUDA-core engine.  The entries of a 16-row block (row pointer rp[]
 // in shared memory, absolute entry indices) are processed in chunks of up to
-// kStage entries: each chunk's (column, value, local row) triples are first
-// copied into shared memory in one coalesced pass.  Every warp then takes an
-// even share of the chunk.  Inside a warp, groups of L lanes (L*8 >= fc) each
-// take one entry per batch; a lane copies its 16-byte piece of the entry's B
-// row into a per-warp ring of kRing batches with cp.async (L2 evict_last, so
-// the feature matrix stays resident while indices and outputs stream past),
-// so kRing batches of gathers are in flight per warp without holding
-// registers.  A lane reads back only the bytes it copied itself, so
-// cp.async.wait_group alone orders the ring.  Accumulation is FP32 in
-// registers (mixed-precision FMA); a lane group adds its partial row into
-// racc[16][kChunk] (shared, FP32) with shared atomics when its entries move
-// to another row.
+// kStage entries: each chunk's (column, value) pairs are first copied into
+// shared memory in one coalesced pass (one exposed memory latency per chunk,
+// not one per batch of B loads).  Every warp then takes an even share of the
+// chunk and walks it one row run at a time, so the inner loop has no row
+// tracking and no divergence: groups of L lanes (L*8 >= fc) each take one
+// entry and load 16 bytes of its B row per lane, kUnroll entries per lane
+// group in flight, tails predicated (value 0, a valid column).  At the end of
+// a run the lane groups are reduced with shuffles and one group adds the
+// row's partial sum into racc[16][kChunk] (shared, FP32) with shared atomics
+// (a row can be split across warps).
 constexpr int kStage = 1024;
-constexpr int kRing = 8;                       // batches in flight per warp
-constexpr int kRingBytes = kRing * 512;        // per warp (32 lanes x 16 bytes per batch)
 
 // acc[0..7] += v * b[0..7]; FP16 operands, FP32 accumulation.  The product
 // of two FP16 numbers is exact in FP32, so the mixed-precision FMA
@@ -71,25 +68,17 @@ __device__ __forceinline__ void fma8h(float (&acc)[8], uint16_t v, const uint4& 
   }
 }
 
-// (column, value bits | local row << 16) of entries [e0, e0+n) into sent[].
-__device__ __forceinline__ void stage_chunk(const int* rp, const int32_t* __restrict__ col,
+__device__ __forceinline__ void stage_chunk(const int32_t* __restrict__ col,
                                             const __half* __restrict__ val, int e0, int n,
                                             int2* sent) {
   const uint16_t* v16 = reinterpret_cast<const uint16_t*>(val);
-  const uint64_t pol = l2_policy_evict_first();
-  for (int i = threadIdx.x; i < n; i += kThreads) {
-    const int e = e0 + i;
-    int r = 0;
-#pragma unroll
-    for (int step = 8; step >= 1; step >>= 1)        // last row with rp[r] <= e
-      if (r + step < kBlockRows && rp[r + step] <= e) r += step;
-    sent[i] = make_int2(ld_stream_i32(col + e, pol), (int)ld_stream_u16(v16 + e, pol) | (r << 16));
-  }
+  for (int i = threadIdx.x; i < n; i += kThreads)
+    sent[i] = make_int2(__ldg(col + e0 + i), (int)__ldg(v16 + e0 + i));
 }
 
-__device__ __forceinline__ void accumulate_chunk(int n, const int2* sent,
+__device__ __forceinline__ void accumulate_chunk(const int* rp, int e0, int n, const int2* sent,
                                                  const __half* __restrict__ B, int K, int f0,
-                                                 int fc, float* racc, uint8_t* ring) {
+                                                 int fc, float* racc) {
   int L = 1;
   while (L * 8 < fc) L <<= 1;
   const int G = 32 / L;
@@ -100,53 +89,38 @@ __device__ __forceinline__ void accumulate_chunk(int n, const int2* sent,
   const int eb = warp * per;
   const int ee = min(n, eb + per);
   if (eb >= ee) return;
-  const int nb = (ee - eb + G - 1) / G;               // batches of this warp
-  const uint64_t pol = l2_policy_evict_last();
-  const uint32_t slot0 = smem_u32(ring + warp * kRingBytes + lane * 16);
   const __half* Bf = B + f0 + (active ? li * 8 : 0);
-  auto issue = [&](int b) {
-    const int j = eb + b * G + g;
-    const bool ok = b < nb && j < ee && active;
-    const int c = ok ? sent[j].x : 0;
-    cp_async16_hint(slot0 + (b % kRing) * 512, ok ? (const void*)(Bf + (size_t)c * K) : (const void*)B,
-                    ok ? 16 : 0, pol);
-    cp_async_commit();
-  };
+  int row = 0;
+  while (rp[row + 1] - e0 <= eb) ++row;            // warp-uniform
+  const int c_safe = sent[eb].x;                   // a valid column for predicated tails
+  for (int i = eb; i < ee;) {
+    const int rend = min(ee, rp[row + 1] - e0);
+    float acc[8];
 #pragma unroll
-  for (int b = 0; b < kRing; ++b) issue(b);
-  float acc[8];
+    for (int q = 0; q < 8; ++q) acc[q] = 0.f;
+    for (int j0 = i + g; j0 < rend; j0 += G * kUnroll) {
+      uint4 bv[kUnroll];
+      uint16_t vv[kUnroll];
 #pragma unroll
-  for (int q = 0; q < 8; ++q) acc[q] = 0.f;
-  int cur = -1;
-  for (int b = 0; b < nb; ++b) {
-    cp_async_wait_group<kRing - 1>();
-    const int j = eb + b * G + g;
-    if (j < ee) {
-      const int2 en = sent[j];
-      const int row = en.y >> 16;
-      if (row != cur) {
-        if (cur >= 0 && active) {
-          float* dst = racc + cur * kChunk + li * 8;
-#pragma unroll
-          for (int q = 0; q < 8; ++q) atomicAdd(dst + q, acc[q]);
-        }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) acc[q] = 0.f;
-        cur = row;
+      for (int u = 0; u < kUnroll; ++u) {
+        const int j = j0 + u * G;
+        const int2 en = j < rend ? sent[j] : make_int2(c_safe, 0);
+        vv[u] = (uint16_t)en.y;
+        bv[u] = __ldg(reinterpret_cast<const uint4*>(Bf + (size_t)en.x * K));
       }
-      uint4 bv;
-      asm volatile("ld.shared.v4.u32 {%0,%1,%2,%3}, [%4];\n"
-                   : "=r"(bv.x), "=r"(bv.y), "=r"(bv.z), "=r"(bv.w)
-                   : "r"(slot0 + (b % kRing) * 512));
-      fma8h(acc, (uint16_t)(en.y & 0xFFFF), bv);
-    }
-    issue(b + kRing);
-  }
-  cp_async_wait_group<0>();
-  if (cur >= 0 && active) {
-    float* dst = racc + cur * kChunk + li * 8;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) atomicAdd(dst + q, acc[q]);
+      for (int u = 0; u < kUnroll; ++u) fma8h(acc, vv[u], bv[u]);
+    }
+    for (int off = L; off < 32; off <<= 1)
+#pragma unroll
+      for (int q = 0; q < 8; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+    if (g == 0 && active) {
+      float* dst = racc + row * kChunk + li * 8;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) atomicAdd(dst + q, acc[q]);
+    }
+    i = rend;
+    while (row < kBlockRows - 1 && rp[row + 1] - e0 <= i) ++row;
   }
 }
 
@@ -154,14 +128,14 @@ __device__ __forceinline__ void accumulate_chunk(int n, const int2* sent,
 __device__ __forceinline__ void block_accumulate(const int* rp, const int32_t* __restrict__ col,
                                                  const __half* __restrict__ val,
                                                  const __half* __restrict__ B, int K, int f0,
-                                                 int fc, float* racc, int2* sent, uint8_t* ring) {
+                                                 int fc, float* racc, int2* sent) {
   const int e_begin = rp[0], e_end = rp[kBlockRows];
   for (int c0 = e_begin; c0 < e_end; c0 += kStage) {
     const int n = min(kStage, e_end - c0);
     __syncthreads();                       // previous chunk fully consumed
-    stage_chunk(rp, col, val, c0, n, sent);
+    stage_chunk(col, val, c0, n, sent);
     __syncthreads();
-    accumulate_chunk(n, sent, B, K, f0, fc, racc, ring);
+    accumulate_chunk(rp, c0, n, sent, B, K, f0, fc, racc);
   }
 }
 
@@ -181,18 +155,16 @@ template <bool F16OUT>
 __global__ void __launch_bounds__(kThreads, 4) csr_block_kernel(
     const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
     const __half* __restrict__ values, int M, const __half* __restrict__ B, int K, void* C) {
-  extern __shared__ __align__(16) uint8_t csr_smem[];
-  uint8_t* ring = csr_smem;                                            // [kWarps][kRingBytes]
-  float* racc = reinterpret_cast<float*>(ring + kWarps * kRingBytes);  // [16][kChunk]
-  int2* sent = reinterpret_cast<int2*>(racc + kBlockRows * kChunk);    // [kStage]
-  int* rp = reinterpret_cast<int*>(sent + kStage);                     // [17]
+  __shared__ __align__(16) float racc[kBlockRows * kChunk];
+  __shared__ int2 sent[kStage];
+  __shared__ int rp[kBlockRows + 1];
   const int r0 = blockIdx.x * kBlockRows;
   if (threadIdx.x <= kBlockRows) rp[threadIdx.x] = indptr[min(r0 + (int)threadIdx.x, M)];
   for (int f0 = 0; f0 < K; f0 += kChunk) {
     const int fc = min(kChunk, K - f0);
     for (int i = threadIdx.x; i < kBlockRows * kChunk; i += kThreads) racc[i] = 0.f;
     __syncthreads();
-    block_accumulate(rp, indices, values, B, K, f0, fc, racc, sent, ring);
+    block_accumulate(rp, indices, values, B, K, f0, fc, racc, sent);
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int f = (warp & 3) * 32 + lane;
@@ -206,8 +178,6 @@ __global__ void __launch_bounds__(kThreads, 4) csr_block_kernel(
     __syncthreads();
   }
 }
-
-constexpr int kSmemCsr = kWarps * kRingBytes + kBlockRows * kChunk * 4 + kStage * 8 + 128;
 
 // Any K: one thread per (row, feature).
 template <bool F16OUT>
@@ -248,7 +218,6 @@ constexpr int kTileColCap = kStage / 16;    // tiles whose columns fit the stagi
 constexpr int kSmemRouted = 1024 + 2 * kHalf * (kAOpBytes + kBOpBytes) + kBlockRows * kChunk * 4 +
                             kStage * 8 + 128;
 constexpr uint32_t kIdesc = umma_idesc_f16(128, 16, /*a MN-major*/ true, /*b MN-major*/ false);
-static_assert(kWarps * kRingBytes <= 2 * kHalf * kAOpBytes, "residual ring must fit the tile stages");
 
 template <bool F16OUT>
 __global__ void __launch_bounds__(kThreads, 3) routed_kernel(PlanView pv, const __half* __restrict__ B,
@@ -382,13 +351,11 @@ __global__ void __launch_bounds__(kThreads, 3) routed_kernel(PlanView pv, const 
       }
     }
     if (failed) break;
-    // ---- CUDA-core residual (its gather ring reuses the tile stage buffers,
-    // so the tile MMAs are drained first) --------------------------------------
-    if (nt > 0 && (!drain(0) || !drain(1))) { failed = true; break; }
+    // ---- CUDA-core residual --------------------------------------------------
     for (int i = tid; i < kBlockRows * kChunk; i += kThreads) racc[i] = 0.f;
     if (do_res)
       block_accumulate(rp, pv.res_col, reinterpret_cast<const __half*>(pv.res_val), B, K, f0, fc,
-                       racc, sent, aop);
+                       racc, sent);
     __syncthreads();
     // ---- epilogue: D^T from TMEM + residual, one store per element ------------
     float d[8];
@@ -461,14 +428,8 @@ int launch_csr(const int32_t* indptr, const int32_t* indices, const uint16_t* va
   const bool f16 = c_dtype == TR_OUT_F16;
   if (k % 8 == 0 && aligned16(b)) {
     const int blocks = (m + kBlockRows - 1) / kBlockRows;
-    static bool attr[2] = {false, false};
-    if (!attr[f16]) {
-      if (f16) TRS_CUDA(cudaFuncSetAttribute(csr_block_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCsr));
-      else TRS_CUDA(cudaFuncSetAttribute(csr_block_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemCsr));
-      attr[f16] = true;
-    }
-    if (f16) csr_block_kernel<true><<<blocks, kThreads, kSmemCsr, stream>>>(indptr, indices, vh, m, bh, k, c);
-    else csr_block_kernel<false><<<blocks, kThreads, kSmemCsr, stream>>>(indptr, indices, vh, m, bh, k, c);
+    if (f16) csr_block_kernel<true><<<blocks, kThreads, 0, stream>>>(indptr, indices, vh, m, bh, k, c);
+    else csr_block_kernel<false><<<blocks, kThreads, 0, stream>>>(indptr, indices, vh, m, bh, k, c);
   } else {
     const int64_t n = (int64_t)m * k;
     const int blocks = (int)((n + 255) / 256);
