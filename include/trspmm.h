@@ -97,6 +97,9 @@ typedef struct tr_plan_info {
   int64_t sptc_tiles;      /* 16x16 2:4 tiles from the SPTC route */
   int64_t residual_nnz;    /* CUDA-core entries */
   int64_t device_bytes;    /* plan footprint in HBM */
+  int64_t promoted_tiles;  /* 16x16 tiles holding residual columns moved onto the tensor cores */
+  int32_t row_scaled;      /* 1 if values are stored as FP16(v / row scale) */
+  int32_t reordered;       /* 1 if the plan's rows were clustered before routing */
 } tr_plan_info;
 
 /* Host route tables (pointer + element count each), in the reference's
@@ -129,6 +132,43 @@ int tr_plan_from_tables(const tr_tables* t, int32_t n_rows, int32_t n_cols, int3
 int tr_plan_from_csr(const int32_t* indptr, const int32_t* indices, const float* values,
                      int32_t n_rows, int32_t n_cols, const tr_route_params* params,
                      tr_plan** out);
+/* Options of the native plan builder (tr_plan_build).  Zero-initialised
+ * options give the same plan as tr_plan_from_csr. */
+typedef struct tr_plan_opts {
+  int32_t row_scale;       /* 1: per-row FP32 scale s_r = max|v| of the row; the
+                              plan stores FP16(v / s_r) and the epilogue
+                              multiplies by s_r (small GCN weights keep FP16
+                              precision) */
+  int32_t promote_min;     /* residual columns used by >= promote_min rows of a
+                              16-row window are gathered once and multiplied on
+                              the tensor cores (0: keep the CUDA-core residual) */
+  int32_t transpose;       /* 1: plan for A^T (the adjoint dB = A^T dC); entry
+                              indices still refer to A's CSR */
+  int32_t reorder;         /* 1: cluster rows with shared columns into the same
+                              windows before routing; results are written to the
+                              original row positions */
+} tr_plan_opts;
+
+/* Native plan builder: validate the CSR, optionally transpose and reorder it,
+ * route it (params; mode TR_ROUTE_EXACT keeps every entry) and lay it out.
+ * The plan records, for every CSR entry of A, where its value lives, so that
+ * tr_plan_set_values can re-value it on the device.  No reference counterpart:
+ * the reference re-routes on the host for every new value set. */
+int tr_plan_build(const int32_t* indptr, const int32_t* indices, const float* values,
+                  int32_t n_rows, int32_t n_cols, const tr_route_params* params,
+                  const tr_plan_opts* opts, tr_plan** out);
+/* The same builder, stopping before the upload: the host arrays of the plan
+ * (for inspection and host-side tests; no device needed).  Arrays by index:
+ * 0 win_tile, 1 win_split, 2 win_prom, 3 tile_col, 4 tile_a (FP16 bits),
+ * 5 res_ptr, 6 res_col, 7 res_val (FP16 bits), 8 win_order, 9 row_scale
+ * (FP32), 10 row_out, 11 val_slot, 12 edge_row; `count` is in elements. */
+typedef struct tr_host_plan tr_host_plan;
+int tr_plan_build_host(const int32_t* indptr, const int32_t* indices, const float* values,
+                       int32_t n_rows, int32_t n_cols, const tr_route_params* params,
+                       const tr_plan_opts* opts, tr_host_plan** out);
+int tr_host_plan_array(const tr_host_plan* h, int idx, const void** data, int64_t* count);
+int tr_host_plan_upload(const tr_host_plan* h, tr_plan** out);
+void tr_host_plan_free(tr_host_plan* h);
 int tr_plan_info_get(const tr_plan* p, tr_plan_info* info);
 void tr_plan_free(tr_plan* p);
 
@@ -144,9 +184,26 @@ int tr_spmm_csr(const int32_t* indptr, const int32_t* indices, const uint16_t* v
                 void* c, int c_dtype, void* stream);
 
 /* Routed forward: C = A_plan · B.  route_mask restricts the routes computed
- * (for per-route timing); C rows of the plan are fully overwritten. */
+ * (for per-route timing; promoted tiles count as TR_ROUTE_CUDA); C rows of
+ * the plan are fully overwritten.  For a plan built with opts.transpose this
+ * is the adjoint dB = A^T · dC. */
 int tr_spmm_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_dtype,
                    int route_mask, void* stream);
+
+/* Replace the plan's values with new FP32 values of A's CSR entries (device
+ * array of n_edges, in A's CSR order), recomputing the row scales of a
+ * row-scaled plan.  Entries a compat plan does not multiply are ignored.
+ * Used for learnable edge weights (the forward and the adjoint plan of the
+ * same A take the same array). */
+int tr_plan_set_values(tr_plan* p, const float* values, int64_t n_edges, void* stream);
+
+/* Sampled dense-dense product on A's pattern (the gradient of the values):
+ * out[e] = sum_f x[row(e), f] * y[indices[e], f] for every CSR entry e,
+ * FP16 x [m, k] and y [n_cols, k], FP32 accumulation and output.  device:
+ * indptr[m+1], indices[nnz], out[nnz]. */
+int tr_sddmm_csr(const int32_t* indptr, const int32_t* indices, int32_t m, int32_t n_cols,
+                 int64_t nnz, const uint16_t* x, const uint16_t* y, int32_t k, float* out,
+                 void* stream);
 
 /* ------------------------------------------------------------------------
  * Reference-compatible entry points (host tensors in, FP32 host out; device

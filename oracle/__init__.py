@@ -12,12 +12,16 @@ Contents
   decode_tables()    rebuilds the matrix the 29 route tables encode (TC bitmap
                      sub-blocks, SPTC groups, CUDA parts), i.e. the operand the
                      reference's routed forward multiplies.
+  decode_plan()      rebuilds the matrix a device plan multiplies from the
+                     native builder's host arrays (tiles, residual, row
+                     scales, output rows); plan_value_of_entries() reads back
+                     each CSR entry's value through the entry -> slot map.
   spmm_f64() / spmm_f16_f32() / sddmm_f64()   CSR arithmetic in C (OpenMP).
 """
 from .core import (TABLE_NAMES, route, ref_route, ref_available, decode_tables,
-                   decode_sptc_tiles, spmm_f64, spmm_f16_f32, sddmm_f64, max_threads,
-                   lib_path)
+                   decode_sptc_tiles, decode_plan, plan_value_of_entries, spmm_f64,
+                   spmm_f16_f32, sddmm_f64, max_threads, lib_path)
 
 __all__ = ["TABLE_NAMES", "route", "ref_route", "ref_available", "decode_tables",
-           "decode_sptc_tiles", "spmm_f64", "spmm_f16_f32", "sddmm_f64", "max_threads",
+           "decode_sptc_tiles", "decode_plan", "plan_value_of_entries", "spmm_f64", "spmm_f16_f32", "sddmm_f64", "max_threads",
            "lib_path"]

@@ -247,6 +247,77 @@ def decode_tables(tabs, n_rows, n_cols, window=16, sptc_from="pos"):
     return {"tc": tc, "sptc": sptc, "cuda": cuda, "all": total}
 
 
+def decode_plan(P):
+    """Rebuild the matrix a device plan multiplies, from its host arrays (the
+    dict of trspmm.host_plan; layout in tr-spmm_b200/csrc/plan.h): tile
+    element (n, k) of tile t sits at (n//8)*128 + (k//8)*64 + (n%8)*8 + k%8
+    and multiplies B[tile_col[t*16+k]] into plan row 16*w + n; residual
+    entries are CSR over plan rows; every plan row r is scaled by
+    row_scale[r] and lands in output row row_out[r].  Returns
+    {'tiles': (tc, sptc, promoted) CSR float64 matrices, 'res', 'all'} in the
+    output row space, values as the kernels see them (FP16 x FP32 scale)."""
+    n_rows, n_cols = int(P["n_rows"]), int(P["n_cols"])
+    wt, split, prom = P["win_tile"], P["win_split"], P["win_prom"]
+    W = len(wt) - 1
+    a = P["tile_a"].view(np.float16).astype(np.float64)
+    cols = P["tile_col"]
+    scale = P["row_scale"].astype(np.float64)
+    out = P["row_out"]
+    i = np.arange(256)
+    n_of = (i // 128) * 8 + (i % 64) // 8
+    k_of = ((i % 128) // 64) * 8 + (i % 8)
+    parts = {"tc": [], "sptc": [], "prom": []}
+    for w in range(W):
+        for t in range(int(wt[w]), int(wt[w + 1])):
+            key = "tc" if t < split[w] else ("sptc" if t < prom[w] else "prom")
+            vals = a[t * 256:(t + 1) * 256]
+            nz = np.nonzero(vals)[0]
+            if nz.size == 0:
+                continue
+            c = cols[t * 16 + k_of[nz]]
+            assert (c >= 0).all(), "non-zero tile element in an empty column slot"
+            prow = w * 16 + n_of[nz]
+            parts[key].append((prow, c, vals[nz]))
+
+    def to_csr(lst):
+        if not lst:
+            return sp.csr_matrix((n_rows, n_cols))
+        pr = np.concatenate([x[0] for x in lst])
+        cc = np.concatenate([x[1] for x in lst])
+        vv = np.concatenate([x[2] for x in lst]) * scale[pr]
+        orow = out[pr]
+        assert (orow >= 0).all(), "tile entry in a padding row"
+        return sp.csr_matrix((vv, (orow, cc)), shape=(n_rows, n_cols))
+
+    mats = {k: to_csr(v) for k, v in parts.items()}
+    rp = P["res_ptr"]
+    cnt = np.diff(rp)
+    pr = np.repeat(np.arange(len(cnt)), cnt)
+    rv = P["res_val"].view(np.float16).astype(np.float64) * scale[pr]
+    assert (out[pr] >= 0).all(), "residual entry in a padding row"
+    res = sp.csr_matrix((rv, (out[pr], P["res_col"])), shape=(n_rows, n_cols))
+    total = (mats["tc"] + mats["sptc"] + mats["prom"] + res).tocsr()
+    return {"tc": mats["tc"], "sptc": mats["sptc"], "prom": mats["prom"], "res": res,
+            "all": total}
+
+
+def plan_value_of_entries(P):
+    """Value the plan holds for each CSR entry of A (via val_slot), FP16 x
+    row scale, NaN where an entry has no slot."""
+    T = len(P["tile_col"]) // 16
+    slot = P["val_slot"].astype(np.int64)
+    a = P["tile_a"].view(np.float16).astype(np.float64)
+    r = P["res_val"].view(np.float16).astype(np.float64)
+    v = np.full(slot.shape, np.nan)
+    t = (slot >= 0) & (slot < T * 256)
+    v[t] = a[slot[t]]
+    q = slot >= T * 256
+    v[q] = r[slot[q] - T * 256]
+    has = slot >= 0
+    v[has] *= P["row_scale"][P["edge_row"][has]]
+    return v
+
+
 def max_threads():
     return _load().oracle_max_threads()
 

@@ -1,0 +1,167 @@
+"""The native plan builder (host side, no device): the plan a kernel reads
+encodes exactly A (or A^T), whatever the options — row scaling, promotion of
+shared residual columns to tensor-core tiles, row clustering — and its
+entry -> slot map finds every value.  Checked with the oracle's plan decoder."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+import oracle
+import trspmm
+from trspmm import graphs
+
+GRAPHS = {
+    "random_ragged": lambda: graphs.random_csr(300, 280, 0.05, seed=3, empty_rows=0.3),
+    "chung_lu": lambda: graphs.chung_lu(n=2000, avg_degree=12, seed=4),
+    "route_mix": lambda: graphs.route_mix(n=2048, target_nnz=100_000, seed=5),
+    "sbm": lambda: graphs.sbm_powerlaw(n=3000, avg_degree=24, communities=30, seed=6),
+    "batched": lambda: graphs.batched(num_graphs=10, seed=7),
+}
+OPTS = [
+    dict(),
+    dict(row_scale=True),
+    dict(promote_min=2),
+    dict(promote_min=1, row_scale=True),
+    dict(transpose=True),
+    dict(transpose=True, promote_min=2, row_scale=True),
+    dict(reorder=True),
+    dict(reorder=True, transpose=True, promote_min=2, row_scale=True),
+]
+
+
+def _expected(g, transpose, row_scale):
+    """A (or A^T) with the values the plan must hold: FP16(v / s_r) * s_r,
+    s_r = max |v| over the (transposed) row in FP32, s_r = 1 without scaling."""
+    A = sp.csr_matrix((np.asarray(g.values, np.float32), g.indices, g.indptr),
+                      shape=(g.n_rows, g.n_cols))
+    if transpose:
+        A = A.T.tocsr()
+    A.sort_indices()
+    rows = np.repeat(np.arange(A.shape[0]), np.diff(A.indptr))
+    v = A.data.astype(np.float32)
+    if row_scale:
+        s = np.zeros(A.shape[0], np.float32)
+        np.maximum.at(s, rows, np.abs(v))
+        s[s == 0] = 1
+    else:
+        s = np.ones(A.shape[0], np.float32)
+    q = (v / s[rows]).astype(np.float16).astype(np.float64) * s[rows].astype(np.float64)
+    return sp.csr_matrix((q, A.indices, A.indptr), shape=A.shape)
+
+
+@pytest.mark.parametrize("opt", range(len(OPTS)), ids=lambda i: "-".join(
+    f"{k}={v}" for k, v in OPTS[i].items()) or "default")
+@pytest.mark.parametrize("name", list(GRAPHS))
+def test_plan_encodes_matrix(name, opt):
+    g = GRAPHS[name]()
+    o = OPTS[opt]
+    P = trspmm.host_plan(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, **o)
+    D = oracle.decode_plan(P)
+    ref = _expected(g, o.get("transpose", False), o.get("row_scale", False))
+    diff = abs(D["all"] - ref)
+    assert diff.nnz == 0 or diff.max() <= 1e-12 * max(abs(ref).max(), 1)
+    # every plan row lands in a distinct output row; padding rows nowhere
+    ro = P["row_out"]
+    n_out = ref.shape[0]
+    assert np.array_equal(np.sort(ro[ro >= 0]), np.arange(n_out))
+    # the entry -> slot map reads back every entry's value (exact mode)
+    v = oracle.plan_value_of_entries(P)
+    assert not np.isnan(v).any(), "entry without a value slot"
+    w = np.asarray(g.values, np.float32)
+    # the value the plan holds for entry e: compare entry by entry through A's order
+    A = sp.csr_matrix((np.arange(1, g.nnz + 1, dtype=np.float64), g.indices, g.indptr),
+                      shape=(g.n_rows, g.n_cols))
+    if o.get("transpose"):
+        rows_t = g.indices
+        s = np.zeros(g.n_cols, np.float32)
+        if o.get("row_scale"):
+            np.maximum.at(s, rows_t, np.abs(w))
+        s[s == 0] = 1
+        srow = s[rows_t]
+    else:
+        rows = np.repeat(np.arange(g.n_rows), np.diff(g.indptr))
+        s = np.zeros(g.n_rows, np.float32)
+        if o.get("row_scale"):
+            np.maximum.at(s, rows, np.abs(w))
+        s[s == 0] = 1
+        srow = s[rows]
+    want = (w / srow).astype(np.float16).astype(np.float64) * srow
+    assert np.allclose(v, want, rtol=0, atol=0), "plan value of an entry differs"
+    del A
+
+
+def test_promotion_moves_shared_columns_only():
+    g = graphs.sbm_powerlaw(n=3000, avg_degree=24, communities=30, seed=6)
+    base = trspmm.host_plan(g.indptr, g.indices, g.values, g.n_rows, g.n_cols)
+    P = trspmm.host_plan(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, promote_min=2)
+    D = oracle.decode_plan(P)
+    assert D["prom"].nnz > 0
+    assert len(P["res_col"]) < len(base["res_col"])
+    # a promoted column slot holds >= 2 entries of its window
+    wt, prom = P["win_tile"], P["win_prom"]
+    a = P["tile_a"].view(np.float16).reshape(-1, 256)
+    i = np.arange(256)
+    k_of = ((i % 128) // 64) * 8 + (i % 8)
+    for w in range(len(wt) - 1):
+        for t in range(int(prom[w]), int(wt[w + 1])):
+            cnt = np.bincount(k_of[a[t] != 0], minlength=16)
+            used = P["tile_col"][t * 16:(t + 1) * 16] >= 0
+            assert (cnt[used] >= 2).all()
+    # promote_min = 1 empties the residual (no repeated (row, col) in this graph)
+    P1 = trspmm.host_plan(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, promote_min=1)
+    assert len(P1["res_col"]) == 0
+
+
+def test_duplicate_entries_stay_exact():
+    # repeated (row, column) entries: a tile slot holds one, the rest stay residual
+    indptr = np.array([0, 4, 6], np.int32)
+    indices = np.array([3, 3, 5, 3, 5, 5], np.int32)
+    values = np.array([1.0, 2.0, 0.5, 4.0, 1.5, -1.0], np.float32)
+    for pm in (0, 1, 2):
+        P = trspmm.host_plan(indptr, indices, values, 2, 8, promote_min=pm)
+        D = oracle.decode_plan(P)["all"].toarray()
+        want = np.zeros((2, 8))
+        np.add.at(want, (np.repeat([0, 1], [4, 2]), indices), values)
+        assert np.allclose(D, want)
+        assert not np.isnan(oracle.plan_value_of_entries(P)).any()
+
+
+def test_reorder_clusters_communities():
+    """Randomly permuted SBM: clustering rows before routing cuts the number
+    of distinct (window, column) pairs, i.e. the feature rows gathered."""
+    g = graphs.sbm_powerlaw(n=4000, avg_degree=30, communities=40, seed=11)
+
+    def gathers(P):
+        wt = P["win_tile"]
+        n_tiles_cols = int((P["tile_col"] >= 0).sum())
+        return n_tiles_cols + len(P["res_col"]), len(wt) - 1
+
+    plain = trspmm.host_plan(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, promote_min=1)
+    clus = trspmm.host_plan(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, promote_min=1,
+                            reorder=True)
+    gp, _ = gathers(plain)
+    gc, _ = gathers(clus)
+    assert gc * 1.3 < gp, (gc, gp)
+    ro = clus["row_out"]
+    assert not np.array_equal(ro[: g.n_rows], np.arange(g.n_rows))
+
+
+def test_builder_rejects_malformed_csr():
+    with pytest.raises(trspmm.TrError, match="out of range"):
+        trspmm.host_plan(np.array([0, 1], np.int32), np.array([9], np.int32),
+                         np.ones(1, np.float32), 1, 4)
+    with pytest.raises(trspmm.TrError, match="non-decreasing"):
+        trspmm.host_plan(np.array([0, 2, 1], np.int32), np.array([0, 1], np.int32),
+                         np.ones(2, np.float32), 2, 4)
+    with pytest.raises(trspmm.TrError, match="promote_min"):
+        trspmm.host_plan(np.array([0, 1], np.int32), np.array([0], np.int32),
+                         np.ones(1, np.float32), 1, 4, promote_min=-1)
+
+
+def test_empty_matrix_plan():
+    P = trspmm.host_plan(np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0, np.float32),
+                         0, 5)
+    assert len(P["win_tile"]) == 1 and len(P["val_slot"]) == 0
+    P = trspmm.host_plan(np.zeros(4, np.int32), np.zeros(0, np.int32), np.zeros(0, np.float32),
+                         3, 5, transpose=True, reorder=True)
+    assert oracle.decode_plan(P)["all"].nnz == 0

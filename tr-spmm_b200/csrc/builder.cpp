@@ -1,0 +1,266 @@
+// Native plan builder: CSR -> (transpose) -> (row clustering) -> route -> plan.
+//
+// Every step keeps, for each CSR entry it moves, the index of the entry of
+// the caller's A it came from, so the finished plan knows where the value of
+// each entry of A lives (learnable edge weights re-value the plan on the
+// device without rebuilding it).
+//
+// Row clustering (opts.reorder) is this library's counterpart of the
+// reference's optional row reorder (spmm/tr_csr_fp16/tr_tca_reorder.py:44-357,
+// MinHash-LSH Jaccard clustering, off by default at
+// spmm/tr_csr_fp16/mdataset2_online.py:73): rows that share columns are put
+// into the same 16-row windows so that a gathered feature row serves several
+// output rows.  Here it is label propagation over the bipartite row/column
+// graph (deterministic sweeps, seeded visiting order), then a stable sort of
+// rows by label.  Only rows move; B is never permuted, and the kernels write
+// every result row back to its original position.
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/trspmm.h"
+#include "common.cuh"
+#include "plan.h"
+#include "router.h"
+
+namespace trs {
+
+struct Csr {
+  int32_t n_rows = 0, n_cols = 0;
+  std::vector<int32_t> ptr, idx;
+  std::vector<float> val;
+  std::vector<int32_t> src;      // entry of the caller's A behind each entry
+};
+
+int validate_csr(const int32_t* indptr, const int32_t* indices, int32_t n_rows, int32_t n_cols,
+                 std::string& err) {
+  if (n_rows < 0 || n_cols < 0) { err = "negative matrix shape"; return TR_ERR_ARG; }
+  if (indptr[0] != 0) { err = "indptr must start at 0"; return TR_ERR_ARG; }
+  for (int32_t r = 0; r < n_rows; ++r)
+    if (indptr[r + 1] < indptr[r]) { err = "indptr must be non-decreasing"; return TR_ERR_ARG; }
+  const int64_t nnz = indptr[n_rows];
+  if (nnz > 0 && !indices) { err = "null indices"; return TR_ERR_ARG; }
+  for (int64_t e = 0; e < nnz; ++e)
+    if (indices[e] < 0 || indices[e] >= n_cols) { err = "column index out of range"; return TR_ERR_ARG; }
+  return TR_OK;
+}
+
+namespace {
+
+void transpose(const Csr& a, Csr& t) {
+  t.n_rows = a.n_cols;
+  t.n_cols = a.n_rows;
+  const int64_t nnz = (int64_t)a.idx.size();
+  t.ptr.assign((size_t)t.n_rows + 1, 0);
+  for (int32_t c : a.idx) t.ptr[c + 1]++;
+  for (int32_t r = 0; r < t.n_rows; ++r) t.ptr[r + 1] += t.ptr[r];
+  t.idx.resize(nnz);
+  t.val.resize(nnz);
+  t.src.resize(nnz);
+  std::vector<int32_t> fill(t.ptr.begin(), t.ptr.end() - 1);
+  for (int32_t r = 0; r < a.n_rows; ++r)
+    for (int32_t e = a.ptr[r]; e < a.ptr[r + 1]; ++e) {
+      const int32_t at = fill[a.idx[e]]++;
+      t.idx[at] = r;
+      t.val[at] = a.val[e];
+      t.src[at] = a.src[e];
+    }
+}
+
+inline uint32_t mix32(uint32_t x) {
+  x ^= x >> 16; x *= 0x7feb352dU;
+  x ^= x >> 15; x *= 0x846ca68bU;
+  x ^= x >> 16;
+  return x;
+}
+
+struct Vote {
+  int32_t label;
+  float w;
+};
+
+// Label with the largest summed vote among those with room (size < cap),
+// the current label winning ties; `votes` is sorted in place.
+int32_t best_label(std::vector<Vote>& votes, int32_t cur, const std::vector<int32_t>& size,
+                   int32_t cap) {
+  std::sort(votes.begin(), votes.end(), [](const Vote& x, const Vote& y) { return x.label < y.label; });
+  float cur_w = 0.f;
+  for (const Vote& v : votes)
+    if (v.label == cur) cur_w += v.w;
+  int32_t best = cur;
+  float best_w = cur_w;
+  for (size_t i = 0; i < votes.size();) {
+    size_t j = i;
+    float w = 0.f;
+    while (j < votes.size() && votes[j].label == votes[i].label) w += votes[j++].w;
+    const int32_t l = votes[i].label;
+    if (l != cur && size[l] < cap && w > best_w) {
+      best = l;
+      best_w = w;
+    }
+    i = j;
+  }
+  return best;
+}
+
+}  // namespace
+
+// Row order that clusters rows sharing columns: perm[new] = old.
+//
+// Asynchronous label propagation in a seeded visiting order.  Two changes
+// keep hubs of power-law graphs from flooding every community with their
+// label: a neighbour's vote weighs 1 / its degree (a hub is adjacent to many
+// communities, so it says little about any one), and a label takes no new
+// member once it holds `cap` rows.  Sweeps stop when fewer than 0.1% of rows
+// change.  A square matrix is taken as a graph on one node set (row i and
+// column i are the same node, in- and out-neighbours both vote); otherwise
+// rows and columns carry separate labels and vote for each other.
+void cluster_rows(const Csr& a, std::vector<int32_t>& perm, int sweeps, int32_t cap) {
+  const int32_t R = a.n_rows, C = a.n_cols;
+  perm.resize(R);
+  std::iota(perm.begin(), perm.end(), 0);
+  if (R <= 16 || a.idx.empty()) return;
+  std::vector<int32_t> cptr((size_t)C + 1, 0), crow(a.idx.size());
+  for (int32_t c : a.idx) cptr[c + 1]++;
+  for (int32_t c = 0; c < C; ++c) cptr[c + 1] += cptr[c];
+  {
+    std::vector<int32_t> fill(cptr.begin(), cptr.end() - 1);
+    for (int32_t r = 0; r < R; ++r)
+      for (int32_t e = a.ptr[r]; e < a.ptr[r + 1]; ++e) crow[fill[a.idx[e]]++] = r;
+  }
+  const bool square = R == C;
+  std::vector<float> rinv(R), cinv(C);
+  for (int32_t r = 0; r < R; ++r) {
+    const int32_t d = (a.ptr[r + 1] - a.ptr[r]) + (square ? cptr[r + 1] - cptr[r] : 0);
+    rinv[r] = d > 0 ? 1.f / (float)d : 0.f;
+  }
+  for (int32_t c = 0; c < C; ++c) {
+    const int32_t d = cptr[c + 1] - cptr[c];
+    cinv[c] = d > 0 ? 1.f / (float)d : 0.f;
+  }
+  std::vector<int32_t> rlab(R), rsize(R, 1);
+  std::iota(rlab.begin(), rlab.end(), 0);
+  std::vector<int32_t> clab;
+  if (!square) clab.assign(C, -1);
+  std::vector<int32_t> order(R);
+  std::iota(order.begin(), order.end(), 0);
+  std::sort(order.begin(), order.end(), [](int32_t x, int32_t y) {
+    const uint32_t hx = mix32((uint32_t)x * 2654435761u), hy = mix32((uint32_t)y * 2654435761u);
+    return hx != hy ? hx < hy : x < y;
+  });
+  std::vector<Vote> votes;
+  const std::vector<int32_t> no_size(R, 0);
+  for (int s = 0; s < sweeps; ++s) {
+    if (!square) {
+      for (int32_t c = 0; c < C; ++c) {
+        votes.clear();
+        for (int32_t e = cptr[c]; e < cptr[c + 1]; ++e) votes.push_back({rlab[crow[e]], rinv[crow[e]]});
+        clab[c] = votes.empty() ? -1 : best_label(votes, -1, no_size, INT32_MAX);
+      }
+    }
+    int64_t changed = 0;
+    for (int32_t r : order) {
+      votes.clear();
+      for (int32_t e = a.ptr[r]; e < a.ptr[r + 1]; ++e) {
+        const int32_t c = a.idx[e];
+        if (square) {
+          if (c != r) votes.push_back({rlab[c], rinv[c]});
+        } else if (clab[c] >= 0) {
+          votes.push_back({clab[c], cinv[c]});
+        }
+      }
+      if (square)
+        for (int32_t e = cptr[r]; e < cptr[r + 1]; ++e)
+          if (crow[e] != r) votes.push_back({rlab[crow[e]], rinv[crow[e]]});
+      const int32_t cur = rlab[r];
+      const int32_t l = best_label(votes, cur, rsize, cap);
+      if (l != cur) {
+        rsize[cur]--;
+        rsize[l]++;
+        rlab[r] = l;
+        ++changed;
+      }
+    }
+    if (changed * 1000 < R) break;
+  }
+  std::stable_sort(perm.begin(), perm.end(),
+                   [&](int32_t x, int32_t y) { return rlab[x] < rlab[y]; });
+}
+
+namespace {
+
+void permute_rows(const Csr& a, const std::vector<int32_t>& perm, Csr& p) {
+  p.n_rows = a.n_rows;
+  p.n_cols = a.n_cols;
+  p.ptr.assign((size_t)a.n_rows + 1, 0);
+  for (int32_t r = 0; r < a.n_rows; ++r) p.ptr[r + 1] = p.ptr[r] + (a.ptr[perm[r] + 1] - a.ptr[perm[r]]);
+  const size_t nnz = a.idx.size();
+  p.idx.resize(nnz);
+  p.val.resize(nnz);
+  p.src.resize(nnz);
+  for (int32_t r = 0; r < a.n_rows; ++r) {
+    const int32_t o = perm[r];
+    std::copy(a.idx.begin() + a.ptr[o], a.idx.begin() + a.ptr[o + 1], p.idx.begin() + p.ptr[r]);
+    std::copy(a.val.begin() + a.ptr[o], a.val.begin() + a.ptr[o + 1], p.val.begin() + p.ptr[r]);
+    std::copy(a.src.begin() + a.ptr[o], a.src.begin() + a.ptr[o + 1], p.src.begin() + p.ptr[r]);
+  }
+}
+
+}  // namespace
+
+int build_plan(const int32_t* indptr, const int32_t* indices, const float* values, int32_t n_rows,
+               int32_t n_cols, const tr_route_params& params, const tr_plan_opts& opts,
+               HostPlan& hp, std::string& err) {
+  int rc = validate_csr(indptr, indices, n_rows, n_cols, err);
+  if (rc) return rc;
+  if (params.window != 16) { err = "routed plans need window == 16"; return TR_ERR_UNSUPPORTED; }
+  if (opts.promote_min < 0) { err = "promote_min must be >= 0"; return TR_ERR_ARG; }
+  const int64_t nnz = indptr[n_rows];
+  if (nnz > INT32_MAX) { err = "more than 2^31 - 1 entries"; return TR_ERR_UNSUPPORTED; }
+  Csr a;
+  a.n_rows = n_rows;
+  a.n_cols = n_cols;
+  a.ptr.assign(indptr, indptr + n_rows + 1);
+  a.idx.assign(indices, indices + nnz);
+  a.val.resize(nnz);
+  for (int64_t e = 0; e < nnz; ++e) a.val[e] = values ? values[e] : 1.0f;
+  a.src.resize(nnz);
+  std::iota(a.src.begin(), a.src.end(), 0);
+  if (opts.transpose) {
+    Csr t;
+    transpose(a, t);
+    a = std::move(t);
+  }
+  std::vector<int32_t> perm;
+  if (opts.reorder) {
+    cluster_rows(a, perm, 8, 256);
+    Csr p;
+    permute_rows(a, perm, p);
+    a = std::move(p);
+  }
+  RouteTables T;
+  rc = build_route(a.ptr.data(), a.idx.data(), a.val.data(), a.n_rows, params, T, err);
+  if (rc) return rc;
+  PlanOptions po;
+  po.row_scale = opts.row_scale != 0;
+  po.promote_min = opts.promote_min;
+  rc = plan_from_route(T, a.n_rows, a.n_cols, nnz, po, hp, err);
+  if (rc) return rc;
+  // entry indices of the routed matrix -> entries of the caller's A
+  std::vector<int32_t> slot(nnz, -1), erow(nnz, -1);
+  for (int64_t e = 0; e < nnz; ++e) {
+    slot[a.src[e]] = hp.val_slot[e];
+    erow[a.src[e]] = hp.edge_row[e];
+  }
+  hp.val_slot.swap(slot);
+  hp.edge_row.swap(erow);
+  if (opts.reorder)
+    for (size_t r = 0; r < perm.size(); ++r) hp.row_out[r] = perm[r];
+  hp.reordered = opts.reorder != 0;
+  return TR_OK;
+}
+
+}  // namespace trs

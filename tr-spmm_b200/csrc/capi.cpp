@@ -136,6 +136,10 @@ struct tr_route {
   RouteTables t;
 };
 
+struct tr_host_plan {
+  HostPlan hp;
+};
+
 extern "C" {
 
 const char* tr_last_error(void) { return g_error.c_str(); }
@@ -195,46 +199,52 @@ int tr_plan_from_tables(const tr_tables* t, int32_t n_rows, int32_t n_cols, int3
 int tr_plan_from_csr(const int32_t* indptr, const int32_t* indices, const float* values,
                      int32_t n_rows, int32_t n_cols, const tr_route_params* params,
                      tr_plan** out) {
-  if (!indptr || !params || !out) return fail(TR_ERR_ARG, "null argument");
-  tr_route_params p = *params;
-  if (p.window != 16) return fail(TR_ERR_UNSUPPORTED, "routed plans need window == 16");
-  RouteTables T;
-  std::string err;
-  int rc = build_route(indptr, indices, values, n_rows, p, T, err);
-  if (rc) return fail(rc, err);
-  for (int32_t c : T.c_column) if (c >= n_cols) return fail(TR_ERR_ARG, "column index >= n_cols");
-  std::vector<uint16_t> tv(T.t_value.size()), cv(T.c_value.size()), csv(T.cs_value.size());
-  auto h = [](float f) { _Float16 x = (_Float16)f; uint16_t b; std::memcpy(&b, &x, 2); return b; };
-  for (size_t i = 0; i < tv.size(); ++i) tv[i] = h(T.t_value[i]);
-  for (size_t i = 0; i < cv.size(); ++i) cv[i] = h(T.c_value[i]);
-  for (size_t i = 0; i < csv.size(); ++i) csv[i] = h(T.cs_value[i]);
-  tr_tables tt{};
-  tt.t_row_offset = T.t_row_offset.data(); tt.n_t_row_offset = (int64_t)T.t_row_offset.size();
-  tt.t_block_offset = T.t_block_offset.data(); tt.n_t_block_offset = (int64_t)T.t_block_offset.size();
-  tt.t_column = T.t_column.data(); tt.n_t_column = (int64_t)T.t_column.size();
-  tt.t_value = tv.data(); tt.n_t_value = (int64_t)tv.size();
-  tt.t_window_row = T.t_window_row.data(); tt.n_t_window_row = (int64_t)T.t_window_row.size();
-  tt.t_binary = T.t_binary.data(); tt.n_t_binary = (int64_t)T.t_binary.size();
-  tt.c_row_offset = T.c_row_offset.data(); tt.n_c_row_offset = (int64_t)T.c_row_offset.size();
-  tt.c_row = T.c_row.data(); tt.n_c_row = (int64_t)T.c_row.size();
-  tt.c_column = T.c_column.data(); tt.n_c_column = (int64_t)T.c_column.size();
-  tt.c_value = cv.data(); tt.n_c_value = (int64_t)cv.size();
-  tt.cs_row_offset = T.cs_row_offset.data(); tt.n_cs_row_offset = (int64_t)T.cs_row_offset.size();
-  tt.cs_row = T.cs_row.data(); tt.n_cs_row = (int64_t)T.cs_row.size();
-  tt.cs_column = T.cs_column.data(); tt.n_cs_column = (int64_t)T.cs_column.size();
-  tt.cs_value = csv.data(); tt.n_cs_value = (int64_t)csv.size();
-  tt.s_tile_column = T.s_tile_column.data(); tt.n_s_tile_column = (int64_t)T.s_tile_column.size();
-  tt.s_packed_a = reinterpret_cast<const uint32_t*>(T.s_packed_a.data());
-  tt.n_s_packed_a = (int64_t)T.s_packed_a.size();
-  tt.s_packed_meta = reinterpret_cast<const uint32_t*>(T.s_packed_meta.data());
-  tt.n_s_packed_meta = (int64_t)T.s_packed_meta.size();
-  tt.s_window_tile_offset = T.s_window_tile_offset.data();
-  tt.n_s_window_tile_offset = (int64_t)T.s_window_tile_offset.size();
+  tr_plan_opts opts{};
+  return tr_plan_build(indptr, indices, values, n_rows, n_cols, params, &opts, out);
+}
+
+int tr_plan_build(const int32_t* indptr, const int32_t* indices, const float* values,
+                  int32_t n_rows, int32_t n_cols, const tr_route_params* params,
+                  const tr_plan_opts* opts, tr_plan** out) {
+  if (!indptr || !params || !opts || !out) return fail(TR_ERR_ARG, "null argument");
   HostPlan hp;
-  rc = plan_from_tables(tt, n_rows, n_cols, 16, hp, err);
+  std::string err;
+  const int rc = build_plan(indptr, indices, values, n_rows, n_cols, *params, *opts, hp, err);
   if (rc) return fail(rc, err);
   return plan_upload(hp, out);
 }
+
+int tr_plan_build_host(const int32_t* indptr, const int32_t* indices, const float* values,
+                       int32_t n_rows, int32_t n_cols, const tr_route_params* params,
+                       const tr_plan_opts* opts, tr_host_plan** out) {
+  if (!indptr || !params || !opts || !out) return fail(TR_ERR_ARG, "null argument");
+  std::unique_ptr<tr_host_plan> h(new tr_host_plan());
+  std::string err;
+  const int rc = build_plan(indptr, indices, values, n_rows, n_cols, *params, *opts, h->hp, err);
+  if (rc) return fail(rc, err);
+  *out = h.release();
+  return TR_OK;
+}
+
+int tr_host_plan_array(const tr_host_plan* h, int idx, const void** data, int64_t* count) {
+  if (!h || !data || !count) return fail(TR_ERR_ARG, "null argument");
+  const HostPlan& P = h->hp;
+#define TRS_A(i, v) case i: *data = P.v.data(); *count = (int64_t)P.v.size(); return TR_OK;
+  switch (idx) {
+    TRS_A(0, win_tile) TRS_A(1, win_split) TRS_A(2, win_prom) TRS_A(3, tile_col)
+    TRS_A(4, tile_a) TRS_A(5, res_ptr) TRS_A(6, res_col) TRS_A(7, res_val) TRS_A(8, win_order)
+    TRS_A(9, row_scale) TRS_A(10, row_out) TRS_A(11, val_slot) TRS_A(12, edge_row)
+    default: return fail(TR_ERR_ARG, "plan array index out of range");
+  }
+#undef TRS_A
+}
+
+int tr_host_plan_upload(const tr_host_plan* h, tr_plan** out) {
+  if (!h || !out) return fail(TR_ERR_ARG, "null argument");
+  return plan_upload(h->hp, out);
+}
+
+void tr_host_plan_free(tr_host_plan* h) { delete h; }
 
 int tr_plan_info_get(const tr_plan* p, tr_plan_info* info) {
   if (!p || !info) return fail(TR_ERR_ARG, "null argument");
@@ -265,6 +275,24 @@ int tr_spmm_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int 
   if (c_dtype != TR_OUT_F32 && c_dtype != TR_OUT_F16) return fail(TR_ERR_ARG, "bad output dtype");
   if (p->view.n_rows > 0 && k > 0 && (!b || !c)) return fail(TR_ERR_ARG, "null device pointer");
   return launch_routed(p, b, k, c, c_dtype, route_mask & TR_ROUTE_ALL, (cudaStream_t)stream);
+}
+
+int tr_plan_set_values(tr_plan* p, const float* values, int64_t n_edges, void* stream) {
+  if (!p) return fail(TR_ERR_ARG, "null plan");
+  if (n_edges != p->n_edges)
+    return fail(TR_ERR_ARG, "value count " + std::to_string(n_edges) + " != plan entries " +
+                                std::to_string(p->n_edges));
+  if (n_edges > 0 && !values) return fail(TR_ERR_ARG, "null device pointer");
+  return launch_set_values(p, values, (cudaStream_t)stream);
+}
+
+int tr_sddmm_csr(const int32_t* indptr, const int32_t* indices, int32_t m, int32_t n_cols,
+                 int64_t nnz, const uint16_t* x, const uint16_t* y, int32_t k, float* out,
+                 void* stream) {
+  if (m < 0 || n_cols < 0 || nnz < 0 || k < 0) return fail(TR_ERR_ARG, "negative size");
+  if (nnz > 0 && (!indptr || !indices || !out || (k > 0 && (!x || !y))))
+    return fail(TR_ERR_ARG, "null device pointer");
+  return launch_sddmm(indptr, indices, m, nnz, x, y, k, out, (cudaStream_t)stream);
 }
 
 int tr_forward_fp16_tcu_cuda_sptc_mma_parallel_online(

@@ -1,25 +1,34 @@
-// Plan construction: reference route tables -> the fused kernel's layout.
+// Plan construction: route tables -> the fused kernel's layout.
 //
 // Semantics of the tables follow the reference's kernels:
 //  * dense TC sub-blocks (16 rows x 8 columns): bit (r*8 + k) of binary_lo
 //    for rows 0-7 / binary_hi for rows 8-15, value index = rank of the bit
 //    (popcount below it, binary_hi ranks after all of binary_lo), rows from
 //    t_window_row (TR-source/SpMM/mGCNkernel_online.cu:106-204);
-//  * packed 2:4 tiles: per row group g and chunk c, one half2 word for row g
-//    and one for row g+8, positions from the 4-bit meta nibble
-//    (TR-source/Block/block_online.cpp:797-841);
+//  * 2:4 groups: per (group, local row) up to two (position, value) pairs
+//    (TR-source/Block/block_online.cpp:663-702), or the packed tiles built
+//    from them (:797-841);
 //  * CUDA parts: c_row / c_row_offset / c_column / c_value, long and short
 //    alike (TR-source/SpMM/spmm_utils/compute.h:27-88, :176-240).
 // Every index is range-checked here so the kernels can trust the plan.
+//
+// Values are carried in FP32 with the CSR entry they came from (when the
+// tables record it) until the plan is flattened: then an optional per-row
+// scale s_r = max |v| over the row is taken in FP32, FP16(v / s_r) is stored
+// and s_r is re-applied to the row in the kernel epilogue, so small GCN
+// weights keep full FP16 precision.  The entry -> slot map lets a device
+// kernel re-value the plan (learnable edge weights) without rebuilding it.
 #include "plan.h"
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <numeric>
 
 #include "common.cuh"
+#include "router.h"
 
 namespace trs {
 namespace {
@@ -32,52 +41,164 @@ inline uint16_t f2h(float f) {
   std::memcpy(&b, &h, 2);
   return b;
 }
+inline float h2f(uint16_t b) {
+  _Float16 h;
+  std::memcpy(&h, &b, 2);
+  return (float)h;
+}
 
 // Per-window staging before flattening.
 struct WinTiles {
   std::vector<int32_t> col;        // 16 per tile
-  std::vector<uint16_t> a;         // 256 per tile
+  std::vector<float> a;            // 256 per tile (kernel operand order)
+  std::vector<int32_t> edge;       // 256 per tile, -1 where no entry
   int n = 0;
   void add_empty() {
     col.insert(col.end(), 16, -1);
-    a.insert(a.end(), 256, 0);
+    a.insert(a.end(), 256, 0.f);
+    edge.insert(edge.end(), 256, -1);
     n++;
   }
 };
 
-void finish(HostPlan& hp, std::vector<WinTiles>& tc, std::vector<WinTiles>& sp,
-            const std::vector<std::vector<std::pair<int32_t, std::pair<int32_t, uint16_t>>>>& res) {
+struct ResEntry {
+  int32_t row, col;
+  float val;
+  int32_t edge;
+};
+
+struct Staging {
+  std::vector<WinTiles> tc, sp, pr;   // dense TC, 2:4, promoted residual columns
+  std::vector<ResEntry> res;
+  explicit Staging(int W) : tc(W), sp(W), pr(W) {}
+};
+
+bool in_range(int64_t v, int64_t lo, int64_t hi) { return v >= lo && v < hi; }
+
+// Window row of tile element i (inverse of a_index in n).
+inline int elem_row(int i) { return (i / 128) * 8 + (i % 64) / 8; }
+
+// Residual columns used by at least `min_rows` entries of a window move onto
+// the tensor cores: 16 such columns per tile, each (row, column) once (a
+// repeated entry stays in the residual).  Columns are taken in increasing
+// order so the result does not depend on the residual's entry order.
+void promote(Staging& st, int W, int min_rows) {
+  if (min_rows <= 0) return;
+  std::vector<std::vector<size_t>> by_win(W);
+  for (size_t i = 0; i < st.res.size(); ++i) by_win[st.res[i].row / 16].push_back(i);
+  std::vector<char> moved(st.res.size(), 0);
+  std::vector<size_t> idx;
+  for (int w = 0; w < W; ++w) {
+    idx = by_win[w];
+    std::stable_sort(idx.begin(), idx.end(),
+                     [&](size_t x, size_t y) { return st.res[x].col < st.res[y].col; });
+    WinTiles& wt = st.pr[w];
+    std::vector<char> occ;                           // (tile, element) taken
+    int slot = 16;
+    for (size_t i = 0; i < idx.size();) {
+      size_t j = i;
+      while (j < idx.size() && st.res[idx[j]].col == st.res[idx[i]].col) ++j;
+      if ((int)(j - i) >= min_rows) {
+        if (slot == 16) {
+          wt.add_empty();
+          occ.insert(occ.end(), 256, 0);
+          slot = 0;
+        }
+        const size_t cb = (size_t)(wt.n - 1) * 16, ab = (size_t)(wt.n - 1) * 256;
+        wt.col[cb + slot] = st.res[idx[i]].col;
+        for (size_t q = i; q < j; ++q) {
+          const ResEntry& e = st.res[idx[q]];
+          const size_t at = ab + a_index(e.row % 16, slot);
+          if (occ[at]) continue;                     // repeated (row, column): stays
+          occ[at] = 1;
+          wt.a[at] = e.val;
+          wt.edge[at] = e.edge;
+          moved[idx[q]] = 1;
+        }
+        ++slot;
+      }
+      i = j;
+    }
+  }
+  size_t keep = 0;
+  for (size_t i = 0; i < st.res.size(); ++i)
+    if (!moved[i]) st.res[keep++] = st.res[i];
+  st.res.resize(keep);
+}
+
+void flatten(HostPlan& hp, Staging& st, const PlanOptions& opt, int64_t n_edges) {
   const int W = hp.n_windows;
+  const int64_t rows = (int64_t)W * 16;
+  promote(st, W, opt.promote_min);
+  // ---- per-row scales ---------------------------------------------------------
+  hp.row_scale.assign(rows, 1.0f);
+  hp.row_scaled = opt.row_scale;
+  if (opt.row_scale) {
+    std::vector<float> mx(rows, 0.f);
+    for (int w = 0; w < W; ++w)
+      for (WinTiles* wt : {&st.tc[w], &st.sp[w], &st.pr[w]})
+        for (int t = 0; t < wt->n; ++t)
+          for (int i = 0; i < 256; ++i) {
+            const int64_t r = (int64_t)w * 16 + elem_row(i);
+            mx[r] = std::max(mx[r], std::fabs(wt->a[(size_t)t * 256 + i]));
+          }
+    for (auto& e : st.res) mx[e.row] = std::max(mx[e.row], std::fabs(e.val));
+    for (int64_t r = 0; r < rows; ++r) hp.row_scale[r] = mx[r] > 0.f ? mx[r] : 1.0f;
+  }
+  hp.row_out.resize(rows);
+  for (int64_t r = 0; r < rows; ++r) hp.row_out[r] = r < hp.n_rows ? (int32_t)r : -1;
+  // ---- tiles, window-major: dense TC, then 2:4, then promoted ------------------
   hp.win_tile.assign(1, 0);
   hp.win_split.resize(W);
+  hp.win_prom.resize(W);
   hp.tile_col.clear();
   hp.tile_a.clear();
+  hp.val_slot.assign(n_edges, -1);
+  hp.edge_row.assign(n_edges, -1);
+  auto put_tiles = [&](int w, WinTiles& wt) {
+    for (int t = 0; t < wt.n; ++t) {
+      const int64_t tile = (int64_t)hp.tile_col.size() / 16;
+      hp.tile_col.insert(hp.tile_col.end(), wt.col.begin() + t * 16, wt.col.begin() + t * 16 + 16);
+      for (int i = 0; i < 256; ++i) {
+        const int64_t r = (int64_t)w * 16 + elem_row(i);
+        hp.tile_a.push_back(f2h(wt.a[(size_t)t * 256 + i] / hp.row_scale[r]));
+        const int32_t e = wt.edge[(size_t)t * 256 + i];
+        if (e >= 0 && e < n_edges) {
+          hp.val_slot[e] = (int32_t)(tile * 256 + i);
+          hp.edge_row[e] = (int32_t)r;
+        }
+      }
+    }
+  };
   for (int w = 0; w < W; ++w) {
-    hp.tile_col.insert(hp.tile_col.end(), tc[w].col.begin(), tc[w].col.end());
-    hp.tile_a.insert(hp.tile_a.end(), tc[w].a.begin(), tc[w].a.end());
-    hp.win_split[w] = hp.win_tile.back() + tc[w].n;
-    hp.tile_col.insert(hp.tile_col.end(), sp[w].col.begin(), sp[w].col.end());
-    hp.tile_a.insert(hp.tile_a.end(), sp[w].a.begin(), sp[w].a.end());
-    hp.win_tile.push_back(hp.win_split[w] + sp[w].n);
-    hp.tc_tiles += tc[w].n;
-    hp.sptc_tiles += sp[w].n;
+    put_tiles(w, st.tc[w]);
+    hp.win_split[w] = hp.win_tile.back() + st.tc[w].n;
+    put_tiles(w, st.sp[w]);
+    hp.win_prom[w] = hp.win_split[w] + st.sp[w].n;
+    put_tiles(w, st.pr[w]);
+    hp.win_tile.push_back(hp.win_prom[w] + st.pr[w].n);
+    hp.tc_tiles += st.tc[w].n;
+    hp.sptc_tiles += st.sp[w].n;
+    hp.prom_tiles += st.pr[w].n;
   }
-  // residual CSR over padded rows, entries of a row in table order
-  const int64_t rows = (int64_t)W * 16;
+  const int64_t T = (int64_t)hp.tile_col.size() / 16;
+  // ---- residual CSR over padded rows, entries of a row in table order -------
   hp.res_ptr.assign(rows + 1, 0);
-  for (auto& r : res)
-    for (auto& e : r) hp.res_ptr[e.first + 1]++;
+  for (auto& e : st.res) hp.res_ptr[e.row + 1]++;
   for (int64_t i = 0; i < rows; ++i) hp.res_ptr[i + 1] += hp.res_ptr[i];
   hp.res_col.resize(hp.res_ptr[rows]);
   hp.res_val.resize(hp.res_ptr[rows]);
   std::vector<int32_t> fill(hp.res_ptr.begin(), hp.res_ptr.end() - 1);
-  for (auto& r : res)
-    for (auto& e : r) {
-      const int32_t at = fill[e.first]++;
-      hp.res_col[at] = e.second.first;
-      hp.res_val[at] = e.second.second;
+  for (auto& e : st.res) {
+    const int32_t at = fill[e.row]++;
+    hp.res_col[at] = e.col;
+    hp.res_val[at] = f2h(e.val / hp.row_scale[e.row]);
+    if (e.edge >= 0 && e.edge < n_edges) {
+      hp.val_slot[e.edge] = (int32_t)(T * 256 + at);
+      hp.edge_row[e.edge] = e.row;
     }
-  // launch order: heaviest windows first (cost ~ gathered rows)
+  }
+  // ---- launch order: heaviest windows first (cost ~ gathered rows) -----------
   std::vector<int64_t> cost(W);
   for (int w = 0; w < W; ++w)
     cost[w] = (int64_t)(hp.win_tile[w + 1] - hp.win_tile[w]) * 16 +
@@ -87,17 +208,74 @@ void finish(HostPlan& hp, std::vector<WinTiles>& tc, std::vector<WinTiles>& sp,
   std::stable_sort(hp.win_order.begin(), hp.win_order.end(),
                    [&](int a, int b) { return cost[a] > cost[b]; });
   int64_t nnz = (int64_t)hp.res_col.size();
-  for (uint16_t v : hp.tile_a) nnz += v != 0;
+  for (uint16_t v : hp.tile_a) nnz += (v & 0x7FFFu) != 0;
   hp.nnz = nnz;
 }
 
-bool in_range(int64_t v, int64_t lo, int64_t hi) { return v >= lo && v < hi; }
+// ---- dense TC sub-blocks ------------------------------------------------------
+int add_tc(const int32_t* t_row_offset, int64_t n_t_row_offset, const int32_t* t_block_offset,
+           int64_t n_t_block_offset, const int32_t* t_column, int64_t n_t_column,
+           const float* t_val32, const uint16_t* t_val16, int64_t n_t_value,
+           const int32_t* t_edge, const int32_t* t_window_row, int64_t n_t_window_row,
+           const int64_t* t_binary, int64_t n_t_binary, int32_t n_cols, int W, Staging& st,
+           std::string& err) {
+  if (n_t_row_offset <= 1) return TR_OK;
+  const int64_t parts = n_t_row_offset - 1;
+  if (n_t_window_row < parts) { err = "t_window_row shorter than the part count"; return TR_ERR_ARG; }
+  const int64_t subs = t_row_offset[parts];
+  if (t_row_offset[0] != 0 || subs < 0 || subs * 8 > n_t_column || subs * 2 > n_t_binary ||
+      n_t_block_offset < subs + 1) {
+    err = "TC tables have inconsistent sizes";
+    return TR_ERR_ARG;
+  }
+  std::vector<std::vector<int64_t>> win_subs(W);
+  for (int64_t p = 0; p < parts; ++p) {
+    const int32_t wr = t_window_row[p];
+    if (wr < 0 || wr % 16 != 0 || wr / 16 >= W) { err = "t_window_row out of range"; return TR_ERR_ARG; }
+    if (t_row_offset[p + 1] < t_row_offset[p]) { err = "t_row_offset must be non-decreasing"; return TR_ERR_ARG; }
+    for (int64_t s = t_row_offset[p]; s < t_row_offset[p + 1]; ++s) win_subs[wr / 16].push_back(s);
+  }
+  for (int w = 0; w < W; ++w) {
+    auto& L = win_subs[w];
+    for (size_t i = 0; i < L.size(); i += 2) {
+      WinTiles& wt = st.tc[w];
+      const size_t cbase = wt.col.size(), abase = wt.a.size();
+      wt.add_empty();
+      for (int half = 0; half < 2 && i + half < L.size(); ++half) {
+        const int64_t s = L[i + half];
+        const int64_t voff = t_block_offset[s], vend = t_block_offset[s + 1];
+        if (voff < 0 || vend < voff || vend > n_t_value) { err = "t_block_offset out of range"; return TR_ERR_ARG; }
+        for (int k = 0; k < 8; ++k) {
+          const int32_t c = t_column[s * 8 + k];
+          if (c < -1 || c >= n_cols) { err = "t_column out of range"; return TR_ERR_ARG; }
+          wt.col[cbase + half * 8 + k] = c;
+        }
+        const uint64_t lo = (uint64_t)t_binary[2 * s], hi = (uint64_t)t_binary[2 * s + 1];
+        int rank = 0;
+        for (int hsel = 0; hsel < 2; ++hsel) {
+          const uint64_t word = hsel ? hi : lo;
+          for (int bit = 0; bit < 64; ++bit) {
+            if (!((word >> bit) & 1u)) continue;
+            const int row = hsel * 8 + bit / 8, k = half * 8 + bit % 8;
+            if (voff + rank >= vend) { err = "TC bitmap has more bits than values"; return TR_ERR_ARG; }
+            if (wt.col[cbase + k] < 0) { err = "TC bit set in a padded column"; return TR_ERR_ARG; }
+            const int64_t vi = voff + rank;
+            wt.a[abase + a_index(row, k)] = t_val32 ? t_val32[vi] : h2f(t_val16[vi]);
+            wt.edge[abase + a_index(row, k)] = t_edge ? t_edge[vi] : -1;
+            rank++;
+          }
+        }
+      }
+    }
+  }
+  return TR_OK;
+}
 
-// Decode packed 2:4 tiles (block_online.cpp:797-841) into dense tiles.
+// ---- packed 2:4 tiles (block_online.cpp:797-841) --------------------------------
 int add_packed_tiles(const int32_t* tile_column, int64_t n_tile_column, const uint32_t* packed_a,
                      int64_t n_packed_a, const uint32_t* packed_meta, int64_t n_packed_meta,
-                     const int32_t* wto, int64_t n_wto, int32_t n_cols, int W,
-                     std::vector<WinTiles>& sp, std::string& err) {
+                     const int32_t* wto, int64_t n_wto, int32_t n_cols, int W, Staging& st,
+                     std::string& err) {
   if (n_wto == 0) return TR_OK;
   const int64_t tiles = n_tile_column / 16;
   if (n_tile_column % 16 || n_packed_a != tiles * 64 || n_packed_meta != tiles * 8) {
@@ -112,7 +290,7 @@ int add_packed_tiles(const int32_t* tile_column, int64_t n_tile_column, const ui
   for (int64_t w = 0; w + 1 < n_wto; ++w) {
     if (wto[w + 1] < wto[w]) { err = "s_window_tile_offset must be non-decreasing"; return TR_ERR_ARG; }
     for (int64_t t = wto[w]; t < wto[w + 1]; ++t) {
-      WinTiles& wt = sp[w];
+      WinTiles& wt = st.sp[w];
       const size_t cbase = wt.col.size(), abase = wt.a.size();
       wt.add_empty();
       for (int k = 0; k < 16; ++k) {
@@ -133,13 +311,77 @@ int add_packed_tiles(const int32_t* tile_column, int64_t n_tile_column, const ui
               if ((bits & 0x7FFFu) == 0) continue;     // padding (+-0)
               const int k = ch * 4 + p[s];
               if (wt.col[cbase + k] < 0) { err = "SPTC value in a padded column"; return TR_ERR_ARG; }
-              wt.a[abase + a_index(row, k)] = bits;
+              wt.a[abase + a_index(row, k)] = h2f(bits);
             }
           }
       }
     }
   }
   return TR_OK;
+}
+
+// ---- 2:4 groups (s_column / s_value / s_pos) -------------------------------------
+int add_groups(const int32_t* s_column, const float* s_value, const int8_t* s_pos,
+               const int32_t* s_edge, int64_t groups, const std::vector<int32_t>& gwin,
+               int32_t n_rows, int32_t n_cols, int W, Staging& st, std::string& err) {
+  std::vector<std::vector<int64_t>> wg(W);
+  for (int64_t g = 0; g < groups; ++g)
+    if (in_range(gwin[g], 0, W)) wg[gwin[g]].push_back(g);   // others lie beyond the matrix
+  for (int w = 0; w < W; ++w) {
+    for (size_t i = 0; i < wg[w].size(); i += 4) {
+      WinTiles& wt = st.sp[w];
+      const size_t cbase = wt.col.size(), abase = wt.a.size();
+      wt.add_empty();
+      for (int ch = 0; ch < 4 && i + ch < wg[w].size(); ++ch) {
+        const int64_t g = wg[w][i + ch];
+        for (int p = 0; p < 4; ++p) {
+          const int32_t c = s_column[g * 4 + p];
+          if (c < -1 || c >= n_cols) { err = "s_column out of range"; return TR_ERR_ARG; }
+          wt.col[cbase + ch * 4 + p] = c;
+        }
+        for (int lr = 0; lr < 16; ++lr) {
+          if ((int64_t)w * 16 + lr >= n_rows) continue;
+          for (int s = 0; s < 2; ++s) {
+            const int64_t at = (g * 16 + lr) * 2 + s;
+            const int pos = s_pos[at];
+            if (pos < 0 || pos > 3 || wt.col[cbase + ch * 4 + pos] < 0) continue;   // kernel skips
+            wt.a[abase + a_index(lr, ch * 4 + pos)] = s_value[at];
+            wt.edge[abase + a_index(lr, ch * 4 + pos)] = s_edge ? s_edge[at] : -1;
+          }
+        }
+      }
+    }
+  }
+  return TR_OK;
+}
+
+// ---- CUDA parts -----------------------------------------------------------------
+int add_parts(const int32_t* off, int64_t n_off, const int32_t* row, int64_t n_row,
+              const int32_t* col, int64_t n_col, const float* v32, const uint16_t* v16,
+              int64_t n_val, const int32_t* edge, int32_t n_rows, int32_t n_cols, Staging& st,
+              std::string& err) {
+  if (n_off <= 1) return TR_OK;
+  const int64_t parts = n_off - 1;
+  if (n_row < parts || off[0] != 0 || off[parts] > n_col || off[parts] > n_val) {
+    err = "CUDA part tables have inconsistent sizes";
+    return TR_ERR_ARG;
+  }
+  for (int64_t p = 0; p < parts; ++p) {
+    if (off[p + 1] < off[p]) { err = "c_row_offset must be non-decreasing"; return TR_ERR_ARG; }
+    if (!in_range(row[p], 0, n_rows)) { err = "c_row out of range"; return TR_ERR_ARG; }
+    for (int64_t e = off[p]; e < off[p + 1]; ++e) {
+      if (!in_range(col[e], 0, n_cols)) { err = "c_column out of range"; return TR_ERR_ARG; }
+      st.res.push_back({row[p], col[e], v32 ? v32[e] : h2f(v16[e]), edge ? edge[e] : -1});
+    }
+  }
+  return TR_OK;
+}
+
+void init(HostPlan& hp, int32_t n_rows, int32_t n_cols) {
+  hp = HostPlan();
+  hp.n_rows = n_rows;
+  hp.n_cols = n_cols;
+  hp.n_windows = (n_rows + 15) / 16;
 }
 
 }  // namespace
@@ -148,99 +390,54 @@ int plan_from_tables(const tr_tables& t, int32_t n_rows, int32_t n_cols, int32_t
                      HostPlan& hp, std::string& err) {
   if (window != 16) { err = "routed plans need window == 16"; return TR_ERR_UNSUPPORTED; }
   if (n_rows < 0 || n_cols < 0) { err = "negative matrix shape"; return TR_ERR_ARG; }
-  hp = HostPlan();
-  hp.n_rows = n_rows;
-  hp.n_cols = n_cols;
-  hp.n_windows = (n_rows + 15) / 16;
-  const int W = hp.n_windows;
-  std::vector<WinTiles> tc(W), sp(W);
-  std::vector<std::vector<std::pair<int32_t, std::pair<int32_t, uint16_t>>>> res(1);
-
-  // ---- dense TC parts -------------------------------------------------------
-  if (t.n_t_row_offset > 1) {
-    const int64_t parts = t.n_t_row_offset - 1;
-    if (t.n_t_window_row < parts) { err = "t_window_row shorter than the part count"; return TR_ERR_ARG; }
-    const int64_t subs = t.t_row_offset[parts];
-    if (t.t_row_offset[0] != 0 || subs * 8 > t.n_t_column || subs * 2 > t.n_t_binary ||
-        t.n_t_block_offset < subs + 1) {
-      err = "TC tables have inconsistent sizes";
-      return TR_ERR_ARG;
-    }
-    // collect the sub-blocks of each window in table order
-    std::vector<std::vector<int64_t>> win_subs(W);
-    for (int64_t p = 0; p < parts; ++p) {
-      const int32_t wr = t.t_window_row[p];
-      if (wr < 0 || wr % 16 != 0 || wr / 16 >= W) { err = "t_window_row out of range"; return TR_ERR_ARG; }
-      if (t.t_row_offset[p + 1] < t.t_row_offset[p]) { err = "t_row_offset must be non-decreasing"; return TR_ERR_ARG; }
-      for (int64_t s = t.t_row_offset[p]; s < t.t_row_offset[p + 1]; ++s) win_subs[wr / 16].push_back(s);
-    }
-    for (int w = 0; w < W; ++w) {
-      auto& L = win_subs[w];
-      for (size_t i = 0; i < L.size(); i += 2) {
-        WinTiles& wt = tc[w];
-        const size_t cbase = wt.col.size(), abase = wt.a.size();
-        wt.add_empty();
-        for (int half = 0; half < 2 && i + half < L.size(); ++half) {
-          const int64_t s = L[i + half];
-          const int64_t voff = t.t_block_offset[s];
-          const int64_t vend = t.t_block_offset[s + 1];
-          if (voff < 0 || vend < voff || vend > t.n_t_value) { err = "t_block_offset out of range"; return TR_ERR_ARG; }
-          for (int k = 0; k < 8; ++k) {
-            const int32_t c = t.t_column[s * 8 + k];
-            if (c < -1 || c >= n_cols) { err = "t_column out of range"; return TR_ERR_ARG; }
-            wt.col[cbase + half * 8 + k] = c;
-          }
-          const uint64_t lo = (uint64_t)t.t_binary[2 * s], hi = (uint64_t)t.t_binary[2 * s + 1];
-          int rank = 0;
-          for (int hsel = 0; hsel < 2; ++hsel) {
-            const uint64_t word = hsel ? hi : lo;
-            for (int bit = 0; bit < 64; ++bit) {
-              if (!((word >> bit) & 1u)) continue;
-              const int row = hsel * 8 + bit / 8, k = half * 8 + bit % 8;
-              if (voff + rank >= vend) { err = "TC bitmap has more bits than values"; return TR_ERR_ARG; }
-              if (wt.col[cbase + k] < 0) { err = "TC bit set in a padded column"; return TR_ERR_ARG; }
-              wt.a[abase + a_index(row, k)] = t.t_value[voff + rank];
-              rank++;
-            }
-          }
-        }
-      }
-    }
-  }
-
-  // ---- SPTC packed tiles ----------------------------------------------------
-  int rc = add_packed_tiles(t.s_tile_column, t.n_s_tile_column, t.s_packed_a, t.n_s_packed_a,
-                            t.s_packed_meta, t.n_s_packed_meta, t.s_window_tile_offset,
-                            t.n_s_window_tile_offset, n_cols, W, sp, err);
+  init(hp, n_rows, n_cols);
+  Staging st(hp.n_windows);
+  int rc = add_tc(t.t_row_offset, t.n_t_row_offset, t.t_block_offset, t.n_t_block_offset,
+                  t.t_column, t.n_t_column, nullptr, t.t_value, t.n_t_value, nullptr,
+                  t.t_window_row, t.n_t_window_row, t.t_binary, t.n_t_binary, n_cols,
+                  hp.n_windows, st, err);
   if (rc) return rc;
-
-  // ---- CUDA parts (long then short) -----------------------------------------
-  auto& R = res[0];
-  auto add_parts = [&](const int32_t* off, int64_t n_off, const int32_t* row, int64_t n_row,
-                       const int32_t* col, int64_t n_col, const uint16_t* val, int64_t n_val) -> int {
-    if (n_off <= 1) return TR_OK;
-    const int64_t parts = n_off - 1;
-    if (n_row < parts || off[0] != 0 || off[parts] > n_col || off[parts] > n_val) {
-      err = "CUDA part tables have inconsistent sizes";
-      return TR_ERR_ARG;
-    }
-    for (int64_t p = 0; p < parts; ++p) {
-      if (off[p + 1] < off[p]) { err = "c_row_offset must be non-decreasing"; return TR_ERR_ARG; }
-      if (!in_range(row[p], 0, n_rows)) { err = "c_row out of range"; return TR_ERR_ARG; }
-      for (int64_t e = off[p]; e < off[p + 1]; ++e) {
-        if (!in_range(col[e], 0, n_cols)) { err = "c_column out of range"; return TR_ERR_ARG; }
-        R.push_back({row[p], {col[e], val[e]}});
-      }
-    }
-    return TR_OK;
-  };
+  rc = add_packed_tiles(t.s_tile_column, t.n_s_tile_column, t.s_packed_a, t.n_s_packed_a,
+                        t.s_packed_meta, t.n_s_packed_meta, t.s_window_tile_offset,
+                        t.n_s_window_tile_offset, n_cols, hp.n_windows, st, err);
+  if (rc) return rc;
   rc = add_parts(t.c_row_offset, t.n_c_row_offset, t.c_row, t.n_c_row, t.c_column, t.n_c_column,
-                 t.c_value, t.n_c_value);
+                 nullptr, t.c_value, t.n_c_value, nullptr, n_rows, n_cols, st, err);
   if (rc) return rc;
   rc = add_parts(t.cs_row_offset, t.n_cs_row_offset, t.cs_row, t.n_cs_row, t.cs_column,
-                 t.n_cs_column, t.cs_value, t.n_cs_value);
+                 t.n_cs_column, nullptr, t.cs_value, t.n_cs_value, nullptr, n_rows, n_cols, st,
+                 err);
   if (rc) return rc;
-  finish(hp, tc, sp, res);
+  flatten(hp, st, PlanOptions(), 0);
+  return TR_OK;
+}
+
+int plan_from_route(const RouteTables& T, int32_t n_rows, int32_t n_cols, int64_t n_edges,
+                    const PlanOptions& opt, HostPlan& hp, std::string& err) {
+  if (T.window != 16) { err = "routed plans need window == 16"; return TR_ERR_UNSUPPORTED; }
+  init(hp, n_rows, n_cols);
+  Staging st(hp.n_windows);
+  int rc = add_tc(T.t_row_offset.data(), (int64_t)T.t_row_offset.size(), T.t_block_offset.data(),
+                  (int64_t)T.t_block_offset.size(), T.t_column.data(), (int64_t)T.t_column.size(),
+                  T.t_value.data(), nullptr, (int64_t)T.t_value.size(), T.t_edge.data(),
+                  T.t_window_row.data(), (int64_t)T.t_window_row.size(), T.t_binary.data(),
+                  (int64_t)T.t_binary.size(), n_cols, hp.n_windows, st, err);
+  if (rc) return rc;
+  const int64_t groups = (int64_t)T.s_window.size();
+  rc = add_groups(T.s_column.data(), T.s_value.data(), T.s_pos.data(), T.s_edge.data(), groups,
+                  T.s_window, n_rows, n_cols, hp.n_windows, st, err);
+  if (rc) return rc;
+  rc = add_parts(T.c_row_offset.data(), (int64_t)T.c_row_offset.size(), T.c_row.data(),
+                 (int64_t)T.c_row.size(), T.c_column.data(), (int64_t)T.c_column.size(),
+                 T.c_value.data(), nullptr, (int64_t)T.c_value.size(), T.c_edge.data(), n_rows,
+                 n_cols, st, err);
+  if (rc) return rc;
+  rc = add_parts(T.cs_row_offset.data(), (int64_t)T.cs_row_offset.size(), T.cs_row.data(),
+                 (int64_t)T.cs_row.size(), T.cs_column.data(), (int64_t)T.cs_column.size(),
+                 T.cs_value.data(), nullptr, (int64_t)T.cs_value.size(), T.cs_edge.data(), n_rows,
+                 n_cols, st, err);
+  if (rc) return rc;
+  flatten(hp, st, opt, n_edges);
   return TR_OK;
 }
 
@@ -249,11 +446,7 @@ int plan_from_groups(const int32_t* s_column, const float* s_value, const int8_t
                      int64_t n_offsets, int32_t window, int32_t n_rows, int32_t n_cols,
                      HostPlan& hp, std::string& err) {
   if (window != 16) { err = "routed plans need window == 16"; return TR_ERR_UNSUPPORTED; }
-  hp = HostPlan();
-  hp.n_rows = n_rows;
-  hp.n_cols = n_cols;
-  hp.n_windows = (n_rows + 15) / 16;
-  const int W = hp.n_windows;
+  init(hp, n_rows, n_cols);
   std::vector<int32_t> gwin(groups);
   if (s_window) {
     for (int64_t g = 0; g < groups; ++g) gwin[g] = s_window[g];
@@ -267,88 +460,84 @@ int plan_from_groups(const int32_t* s_column, const float* s_value, const int8_t
       for (int64_t g = s_offsets[w]; g < s_offsets[w + 1]; ++g) gwin[g] = (int32_t)w;
     }
   }
-  std::vector<WinTiles> tc(W), sp(W);
-  // groups of one window, four per tile, in table order
-  std::vector<std::vector<int64_t>> wg(W);
-  for (int64_t g = 0; g < groups; ++g) {
-    if (!in_range(gwin[g], 0, W)) {
-      // rows of such a group are beyond the matrix: the reference kernel
-      // skips them (global_row >= mOri), so do we
-      continue;
-    }
-    wg[gwin[g]].push_back(g);
-  }
-  for (int w = 0; w < W; ++w) {
-    for (size_t i = 0; i < wg[w].size(); i += 4) {
-      WinTiles& wt = sp[w];
-      const size_t cbase = wt.col.size(), abase = wt.a.size();
-      wt.add_empty();
-      for (int ch = 0; ch < 4 && i + ch < wg[w].size(); ++ch) {
-        const int64_t g = wg[w][i + ch];
-        for (int p = 0; p < 4; ++p) {
-          const int32_t c = s_column[g * 4 + p];
-          if (c < -1 || c >= n_cols) { err = "s_column out of range"; return TR_ERR_ARG; }
-          wt.col[cbase + ch * 4 + p] = c;
-        }
-        for (int lr = 0; lr < 16; ++lr) {
-          if ((int64_t)w * 16 + lr >= n_rows) continue;
-          for (int s = 0; s < 2; ++s) {
-            const int pos = s_pos[(g * 16 + lr) * 2 + s];
-            if (pos < 0) continue;
-            if (pos > 3 || wt.col[cbase + ch * 4 + pos] < 0) continue;  // kernel skips (col < 0)
-            wt.a[abase + a_index(lr, ch * 4 + pos)] = f2h(s_value[(g * 16 + lr) * 2 + s]);
-          }
-        }
-      }
-    }
-  }
-  std::vector<std::vector<std::pair<int32_t, std::pair<int32_t, uint16_t>>>> res(1);
-  finish(hp, tc, sp, res);
+  Staging st(hp.n_windows);
+  int rc = add_groups(s_column, s_value, s_pos, nullptr, groups, gwin, n_rows, n_cols,
+                      hp.n_windows, st, err);
+  if (rc) return rc;
+  flatten(hp, st, PlanOptions(), 0);
   return TR_OK;
 }
 
 int plan_upload(const HostPlan& hp, tr_plan** out) {
   const int W = hp.n_windows;
   const int64_t T = (int64_t)hp.tile_col.size() / 16;
-  auto al = [](int64_t b) { return (b + 255) / 256 * 256; };
-  const int64_t sz_win_tile = al((W + 1) * 4), sz_win_split = al(std::max(W, 1) * 4),
-                sz_tile_col = al(std::max<int64_t>(T, 1) * 64),
-                sz_tile_a = al(std::max<int64_t>(T, 1) * 512),
-                sz_res_ptr = al(((int64_t)W * 16 + 1) * 4),
-                sz_res_col = al(std::max<size_t>(hp.res_col.size(), 1) * 4),
-                sz_res_val = al(std::max<size_t>(hp.res_val.size(), 1) * 2),
-                sz_order = al(std::max(W, 1) * 4), sz_err = 256;
-  const int64_t total = sz_win_tile + sz_win_split + sz_tile_col + sz_tile_a + sz_res_ptr +
-                        sz_res_col + sz_res_val + sz_order + sz_err;
+  const int64_t rows = (int64_t)W * 16;
+  const int64_t n_edges = (int64_t)hp.val_slot.size();
+  auto al = [](int64_t b) { return (std::max<int64_t>(b, 1) + 255) / 256 * 256; };
+  struct Sec { const void* src; int64_t bytes; int64_t size; };
+  Sec secs[] = {
+      {hp.win_tile.data(), (W + 1) * 4, 0},
+      {hp.win_split.data(), (int64_t)W * 4, 0},
+      {hp.win_prom.data(), (int64_t)W * 4, 0},
+      {hp.tile_col.data(), T * 64, 0},
+      {hp.tile_a.data(), T * 512, 0},
+      {hp.res_ptr.data(), (rows + 1) * 4, 0},
+      {hp.res_col.data(), (int64_t)hp.res_col.size() * 4, 0},
+      {hp.res_val.data(), (int64_t)hp.res_val.size() * 2, 0},
+      {hp.win_order.data(), (int64_t)W * 4, 0},
+      {hp.row_scale.data(), rows * 4, 0},
+      {hp.row_out.data(), rows * 4, 0},
+      {hp.val_slot.data(), n_edges * 4, 0},
+      {hp.edge_row.data(), n_edges * 4, 0},
+      {nullptr, 0, 256},                       // error words
+  };
+  constexpr int kSecs = sizeof(secs) / sizeof(secs[0]);
+  int64_t total = 0;
+  for (auto& s : secs) {
+    if (s.size == 0) s.size = al(s.bytes);
+    total += s.size;
+  }
   tr_plan* p = new tr_plan();
   cudaGetDevice(&p->device);
   cudaError_t e = cudaMalloc(&p->block, total);
   if (e != cudaSuccess) { delete p; return cuda_fail(e, "cudaMalloc(plan)"); }
   p->bytes = total;
   char* base = (char*)p->block;
+  char* at[kSecs];
   int64_t off = 0;
-  auto put = [&](const void* src, int64_t nbytes, int64_t sz) -> char* {
-    char* dst = base + off;
-    off += sz;
-    if (nbytes > 0) cudaMemcpy(dst, src, nbytes, cudaMemcpyHostToDevice);
-    return dst;
-  };
+  for (int i = 0; i < kSecs; ++i) {
+    at[i] = base + off;
+    if (secs[i].bytes > 0) e = cudaMemcpy(at[i], secs[i].src, secs[i].bytes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) break;
+    off += secs[i].size;
+  }
+  if (e == cudaSuccess) e = cudaMemset(at[kSecs - 1], 0, 256);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) { cudaFree(p->block); delete p; return cuda_fail(e, "plan upload"); }
   PlanView& v = p->view;
   v.n_rows = hp.n_rows;
   v.n_cols = hp.n_cols;
   v.n_windows = W;
-  v.win_tile = (int32_t*)put(hp.win_tile.data(), (W + 1) * 4, sz_win_tile);
-  v.win_split = (int32_t*)put(hp.win_split.data(), W * 4, sz_win_split);
-  v.tile_col = (int32_t*)put(hp.tile_col.data(), T * 64, sz_tile_col);
-  v.tile_a = (uint16_t*)put(hp.tile_a.data(), T * 512, sz_tile_a);
-  v.res_ptr = (int32_t*)put(hp.res_ptr.data(), ((int64_t)W * 16 + 1) * 4, sz_res_ptr);
-  v.res_col = (int32_t*)put(hp.res_col.data(), hp.res_col.size() * 4, sz_res_col);
-  v.res_val = (uint16_t*)put(hp.res_val.data(), hp.res_val.size() * 2, sz_res_val);
-  v.win_order = (int32_t*)put(hp.win_order.data(), W * 4, sz_order);
-  v.err = (int*)(base + off);
-  cudaMemset(v.err, 0, sz_err);
-  e = cudaDeviceSynchronize();
-  if (e != cudaSuccess) { cudaFree(p->block); delete p; return cuda_fail(e, "plan upload"); }
+  v.win_tile = (const int32_t*)at[0];
+  v.win_split = (const int32_t*)at[1];
+  v.win_prom = (const int32_t*)at[2];
+  v.tile_col = (const int32_t*)at[3];
+  v.tile_a = (const uint16_t*)at[4];
+  v.res_ptr = (const int32_t*)at[5];
+  v.res_col = (const int32_t*)at[6];
+  v.res_val = (const uint16_t*)at[7];
+  v.win_order = (const int32_t*)at[8];
+  v.row_scale = (const float*)at[9];
+  v.row_out = (const int32_t*)at[10];
+  v.err = (int*)at[13];
+  p->tile_a = (uint16_t*)at[4];
+  p->res_val = (uint16_t*)at[7];
+  p->row_scale = (float*)at[9];
+  p->val_slot = (int32_t*)at[11];
+  p->edge_row = (int32_t*)at[12];
+  p->n_edges = n_edges;
+  p->n_tile_vals = T * 256;
+  p->row_scaled = hp.row_scaled;
   p->info.n_rows = hp.n_rows;
   p->info.n_cols = hp.n_cols;
   p->info.n_windows = W;
@@ -357,6 +546,9 @@ int plan_upload(const HostPlan& hp, tr_plan** out) {
   p->info.sptc_tiles = hp.sptc_tiles;
   p->info.residual_nnz = (int64_t)hp.res_col.size();
   p->info.device_bytes = total;
+  p->info.promoted_tiles = hp.prom_tiles;
+  p->info.row_scaled = hp.row_scaled ? 1 : 0;
+  p->info.reordered = hp.reordered ? 1 : 0;
   *out = p;
   return TR_OK;
 }

@@ -1,9 +1,12 @@
-// Routed operand laid out for the fused sm_100a kernel.
+// Routed operand laid out for the sm_100a kernels.
 //
 // HBM layout (one allocation, window-major, 256-byte aligned sections):
 //   win_tile[W+1]    tensor-core tiles of window w: [win_tile[w], win_tile[w+1])
 //   win_split[W]     first 2:4 tile of window w; tiles before it come from the
-//                    dense TC route, tiles from it on from the SPTC route
+//                    dense TC route
+//   win_prom[W]      first promoted tile of window w: tiles from it on hold
+//                    residual columns that the plan moved onto the tensor
+//                    cores (columns gathered once, used by several rows)
 //   tile_col[T*16]   column of B gathered for each K slot of a tile (-1: none)
 //   tile_a[T*256]    16x16 FP16 A tile, stored in the tcgen05 K-major,
 //                    no-swizzle core-matrix order (N = window row, K = slot):
@@ -11,6 +14,14 @@
 //   res_ptr[W*16+1]  CUDA-core residual as CSR over the padded rows
 //   res_col[R], res_val[R] (FP16)
 //   win_order[W]     windows in decreasing cost order (launch order)
+//   row_scale[W*16]  FP32 factor re-applied to each plan row in the epilogue
+//                    (values are stored as FP16(v / row_scale))
+//   row_out[W*16]    output row of each plan row (-1: padding); the identity
+//                    unless the plan was built on reordered rows
+//   val_slot[E]      for each CSR entry of the source matrix, its value slot:
+//                    tile_a index (< T*256) or T*256 + residual index; -1 if
+//                    the entry is not multiplied (compat-mode truncation)
+//   edge_row[E]      plan row of each CSR entry (row scale of learnable values)
 //   err[4]           device error flags (bounded-wait timeouts)
 #pragma once
 #include <cstdint>
@@ -25,23 +36,30 @@ struct PlanView {
   int32_t n_rows, n_cols, n_windows;
   const int32_t* win_tile;
   const int32_t* win_split;
+  const int32_t* win_prom;
   const int32_t* tile_col;
   const uint16_t* tile_a;
   const int32_t* res_ptr;
   const int32_t* res_col;
   const uint16_t* res_val;
   const int32_t* win_order;
+  const float* row_scale;
+  const int32_t* row_out;
   int* err;
 };
 
 struct HostPlan {
   int32_t n_rows = 0, n_cols = 0, n_windows = 0;
-  std::vector<int32_t> win_tile{0}, win_split, tile_col;
+  std::vector<int32_t> win_tile{0}, win_split, win_prom, tile_col;
   std::vector<uint16_t> tile_a;
   std::vector<int32_t> res_ptr, res_col;
   std::vector<uint16_t> res_val;
   std::vector<int32_t> win_order;
-  int64_t tc_tiles = 0, sptc_tiles = 0, nnz = 0;
+  std::vector<float> row_scale;
+  std::vector<int32_t> row_out;
+  std::vector<int32_t> val_slot, edge_row;
+  bool row_scaled = false, reordered = false;
+  int64_t tc_tiles = 0, sptc_tiles = 0, prom_tiles = 0, nnz = 0;
 };
 
 }  // namespace trs
@@ -51,14 +69,35 @@ struct tr_plan {
   void* block = nullptr;        // the single device allocation
   int64_t bytes = 0;
   int device = 0;
+  int64_t n_edges = 0;          // entries of the source CSR (val_slot / edge_row length)
+  int32_t* val_slot = nullptr;
+  int32_t* edge_row = nullptr;
+  float* row_scale = nullptr;   // writable alias of view.row_scale
+  uint16_t* tile_a = nullptr;   // writable aliases for re-valuing
+  uint16_t* res_val = nullptr;
+  int64_t n_tile_vals = 0;      // T*256
+  bool row_scaled = false;
   tr_plan_info info{};
 };
 
 namespace trs {
 
+struct RouteTables;
+
+// Plan-shaping options of the native builder.
+struct PlanOptions {
+  bool row_scale = false;       // per-row FP32 scale, FP16(v / scale) stored
+  int promote_min = 0;          // residual columns used by >= this many rows of a
+                                // window become tensor-core tiles (0: never)
+};
+
 // Host construction from the reference's tables (validates every index).
 int plan_from_tables(const tr_tables& t, int32_t n_rows, int32_t n_cols, int32_t window,
                      HostPlan& hp, std::string& err);
+// Construction from this library's route tables, which record the CSR entry
+// behind every value; fills val_slot / edge_row over n_edges entries.
+int plan_from_route(const RouteTables& T, int32_t n_rows, int32_t n_cols, int64_t n_edges,
+                    const PlanOptions& opt, HostPlan& hp, std::string& err);
 // SPTC-only plans from the unpacked group tables (s_column/s_value/s_pos),
 // windows given either per group (s_window) or as offsets (s_offsets).
 int plan_from_groups(const int32_t* s_column, const float* s_value, const int8_t* s_pos,
@@ -66,5 +105,11 @@ int plan_from_groups(const int32_t* s_column, const float* s_value, const int8_t
                      int64_t n_offsets, int32_t window, int32_t n_rows, int32_t n_cols,
                      HostPlan& hp, std::string& err);
 int plan_upload(const HostPlan& hp, tr_plan** out);
+// Native builder (builder.cpp): validate, transpose / reorder as asked, route, lay out.
+int validate_csr(const int32_t* indptr, const int32_t* indices, int32_t n_rows, int32_t n_cols,
+                 std::string& err);
+int build_plan(const int32_t* indptr, const int32_t* indices, const float* values, int32_t n_rows,
+               int32_t n_cols, const tr_route_params& params, const tr_plan_opts& opts,
+               HostPlan& hp, std::string& err);
 
 }  // namespace trs

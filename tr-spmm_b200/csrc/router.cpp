@@ -83,6 +83,7 @@ struct Chunk {
   std::vector<int8_t> s_pos;
   std::vector<int32_t> s_tile_window, s_tile_group_local, s_tile_column, s_packed_a,
       s_packed_meta, s_tiles_per_window;
+  std::vector<int32_t> t_edge, s_edge, c_edge, cs_edge;
   int64_t lost = 0;
 };
 
@@ -101,6 +102,7 @@ struct Scratch {
   std::vector<std::array<int, 4>> groups;   // profile indices, -1 padded
   std::vector<int> rc;                      // residual columns of one row
   std::vector<float> rv;
+  std::vector<int> re;                      // their CSR entry ids
 };
 
 // Candidate order of block_online.cpp:226-230 / :285-289 (count desc, column
@@ -118,7 +120,7 @@ void order_by_count(const std::vector<ColProfile>& prof, std::vector<int>& idx,
 
 void split_residual_row(int row, int base_atomic, int part, int shortsz,
                         const std::vector<int>& cols, const std::vector<float>& vals,
-                        Chunk& ck) {
+                        const std::vector<int>& edges, Chunk& ck) {
   const int n = (int)cols.size();
   auto emit = [&](int atomic, int off, int cnt, bool small) {
     auto& counts = small ? ck.cs_counts : ck.c_counts;
@@ -126,11 +128,13 @@ void split_residual_row(int row, int base_atomic, int part, int shortsz,
     auto& ats = small ? ck.cs_atomic : ck.c_atomic;
     auto& cc = small ? ck.cs_column : ck.c_column;
     auto& vv = small ? ck.cs_value : ck.c_value;
+    auto& ee = small ? ck.cs_edge : ck.c_edge;
     counts.push_back(cnt);
     rows.push_back(row);
     ats.push_back(atomic);
     cc.insert(cc.end(), cols.begin() + off, cols.begin() + off + cnt);
     vv.insert(vv.end(), vals.begin() + off, vals.begin() + off + cnt);
+    ee.insert(ee.end(), edges.begin() + off, edges.begin() + off + cnt);
   };
   if (n <= 0) return;
   if (n <= shortsz) { emit(base_atomic, 0, n, true); return; }
@@ -348,6 +352,7 @@ void route_window(const int32_t* indptr, const int32_t* indices, const float* va
       int slots = 0;
       float v[2] = {0.f, 0.f};
       int8_t ps[2] = {-1, -1};
+      int32_t ed[2] = {-1, -1};
       for (int k = 0; k < 4 && g[k] >= 0; ++k) {
         const int le = lr < 16 ? prof[g[k]].first_edge[lr] : -1;
         if (le < 0) continue;
@@ -355,6 +360,7 @@ void route_window(const int32_t* indptr, const int32_t* indices, const float* va
         if (slots < 2) {
           v[slots] = values[e0 + le];
           ps[slots] = (int8_t)k;
+          ed[slots] = e0 + le;
           S.edge_route[le] = 2;
         } else {
           ck.lost++;                                   // dropped by the reference
@@ -364,6 +370,7 @@ void route_window(const int32_t* indptr, const int32_t* indices, const float* va
       ck.s_mask.push_back(mask);
       ck.s_value.push_back(v[0]); ck.s_value.push_back(v[1]);
       ck.s_pos.push_back(ps[0]); ck.s_pos.push_back(ps[1]);
+      ck.s_edge.push_back(ed[0]); ck.s_edge.push_back(ed[1]);
     }
   }
   ck.s_groups_per_window.push_back(ng);
@@ -395,6 +402,7 @@ void route_window(const int32_t* indptr, const int32_t* indices, const float* va
     const size_t val_base = ck.t_value.size();
     std::vector<uint64_t> lo(nsub, 0), hi(nsub, 0);
     std::vector<std::vector<float>> sv(nsub);
+    std::vector<std::vector<int32_t>> se(nsub);
     for (int r = r0; r < r1; ++r) {
       const int lr = r - r0;
       for (int e = indptr[r]; e < indptr[r + 1]; ++e) {
@@ -405,6 +413,7 @@ void route_window(const int32_t* indptr, const int32_t* indices, const float* va
         if (lr >= 8) hi[s] |= 1ull << ((lr - 8) * 8 + k);
         else lo[s] |= 1ull << (lr * 8 + k);
         sv[s].push_back(values[e]);
+        se[s].push_back(e);
       }
     }
     (void)val_base;
@@ -416,6 +425,7 @@ void route_window(const int32_t* indptr, const int32_t* indices, const float* va
       ck.t_binary.push_back((int64_t)lo[s]);
       ck.t_binary.push_back((int64_t)hi[s]);
       ck.t_value.insert(ck.t_value.end(), sv[s].begin(), sv[s].end());
+      ck.t_edge.insert(ck.t_edge.end(), se[s].begin(), se[s].end());
     }
     auto part = [&](int first, int cnt, int atomic) {
       ck.t_parts.push_back(cnt);
@@ -435,13 +445,14 @@ void route_window(const int32_t* indptr, const int32_t* indices, const float* va
   // ---- CUDA residual (block_online.cpp:721-731) ---------------------------
   const int base_atomic = tc_groups.empty() ? 0 : 1;
   for (int r = r0; r < r1; ++r) {
-    S.rc.clear(); S.rv.clear();
+    S.rc.clear(); S.rv.clear(); S.re.clear();
     for (int e = indptr[r]; e < indptr[r + 1]; ++e) {
       if (S.edge_route[e - e0] != 0) continue;
       S.rc.push_back(indices[e]);
       S.rv.push_back(values[e]);
+      S.re.push_back(e);
     }
-    split_residual_row(r, base_atomic, p.partsize_c, p.shortsize, S.rc, S.rv, ck);
+    split_residual_row(r, base_atomic, p.partsize_c, p.shortsize, S.rc, S.rv, S.re, ck);
   }
 
   // ---- mma.sp tile packing (block_online.cpp:797-841) ---------------------
@@ -573,6 +584,9 @@ int build_route(const int32_t* indptr, const int32_t* indices, const float* valu
     append(T.t_window_row, ck.t_window_row);
     append(T.t_atomic, ck.t_atomic);
     append(T.t_binary, ck.t_binary);
+    append(T.t_edge, ck.t_edge);
+    append(T.c_edge, ck.c_edge);
+    append(T.s_edge, ck.s_edge);
     prefix_append(T.c_row_offset, ck.c_counts);
     append(T.c_row, ck.c_row);
     append(T.c_atomic, ck.c_atomic);
@@ -600,6 +614,7 @@ int build_route(const int32_t* indptr, const int32_t* indices, const float* valu
     append(T.cs_atomic, ck.cs_atomic);
     append(T.cs_column, ck.cs_column);
     append(T.cs_value, ck.cs_value);
+    append(T.cs_edge, ck.cs_edge);
   }
   if (p.mode == TR_ROUTE_EXACT) T.dropped = 0;
   T.seconds = std::chrono::duration<double>(std::chrono::high_resolution_clock::now() - t0).count();

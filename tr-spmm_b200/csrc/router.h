@@ -26,6 +26,9 @@ struct RouteTables {
   std::vector<int32_t> s_window, s_offsets{0};
   std::vector<int32_t> s_tile_window, s_tile_group, s_tile_column, s_packed_a, s_packed_meta;
   std::vector<int32_t> s_window_tile_offset{0};
+  // Provenance of every table value: the CSR entry it came from (-1: padding).
+  // Parallel to t_value, s_value, c_value and cs_value.
+  std::vector<int32_t> t_edge, s_edge, c_edge, cs_edge;
   int window = 16;
   int64_t dropped = 0;     // entries the compat tables leave out
   double seconds = 0.0;

@@ -18,6 +18,8 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "plan.h"
 #include "spmm.h"
@@ -194,6 +196,20 @@ __global__ void csr_generic_kernel(const int32_t* __restrict__ indptr,
   store_row_feature<F16OUT>(C, K, r, f, acc);
 }
 
+// Tile ranges of window w that route_mask selects: [a0, a1) dense TC tiles,
+// [b0, b1) 2:4 tiles and/or promoted residual columns (which follow the 2:4
+// tiles and belong to the CUDA-core route).
+__device__ __forceinline__ void route_ranges(const PlanView& pv, int w, int mask, int& a0, int& a1,
+                                             int& b0, int& b1) {
+  const int t0 = pv.win_tile[w], split = pv.win_split[w], prom = pv.win_prom[w],
+            t1 = pv.win_tile[w + 1];
+  a0 = t0;
+  a1 = (mask & TR_ROUTE_TC) ? split : t0;
+  b0 = (mask & TR_ROUTE_SPTC) ? split : prom;
+  b1 = (mask & TR_ROUTE_CUDA) ? t1 : prom;
+  if (b1 < b0) b1 = b0;
+}
+
 // ---------------------------------------------------------------------------
 // Fused routed forward
 // ---------------------------------------------------------------------------
@@ -239,11 +255,10 @@ __global__ void __launch_bounds__(kThreads, 3) routed_kernel(PlanView pv, const 
   const int r0 = w * kBlockRows;
   const int M = pv.n_rows;
 
-  // tiles of the selected routes: [ta0, ta1) dense TC, [tb0, tb1) 2:4
-  int ta0 = pv.win_tile[w], ta1 = pv.win_split[w];
-  int tb0 = ta1, tb1 = pv.win_tile[w + 1];
-  if (!(route_mask & TR_ROUTE_TC)) ta1 = ta0;
-  if (!(route_mask & TR_ROUTE_SPTC)) tb1 = tb0;
+  // tiles of the selected routes: [ta0, ta1) dense TC, [tb0, tb1) 2:4 and/or
+  // promoted residual columns (2:4 tiles precede the promoted ones)
+  int ta0, ta1, tb0, tb1;
+  route_ranges(pv, w, route_mask, ta0, ta1, tb0, tb1);
   const int n_tc = ta1 - ta0;
   const int nt = n_tc + (tb1 - tb0);
   const bool do_res = (route_mask & TR_ROUTE_CUDA) != 0;
@@ -372,8 +387,10 @@ __global__ void __launch_bounds__(kThreads, 3) routed_kernel(PlanView pv, const 
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
         const int r = (warp >> 2) * 8 + i;
-        if (r0 + r < M)
-          store_row_feature<F16OUT>(C, K, (int64_t)r0 + r, f0 + f, d[i] + racc[r * kChunk + f]);
+        const int out = r0 + r < M ? pv.row_out[r0 + r] : -1;
+        if (out >= 0)
+          store_row_feature<F16OUT>(C, K, out, f0 + f,
+                                    (d[i] + racc[r * kChunk + f]) * pv.row_scale[r0 + r]);
       }
     }
     tc_fence_before();
@@ -397,10 +414,10 @@ __global__ void routed_generic_kernel(PlanView pv, const __half* __restrict__ B,
   const int row = (int)(idx / K), f = (int)(idx % K);
   const int w = row / kBlockRows, n = row % kBlockRows;
   float acc = 0.f;
-  const int tsplit = pv.win_split[w];
-  for (int t = pv.win_tile[w]; t < pv.win_tile[w + 1]; ++t) {
-    if (t < tsplit && !(route_mask & TR_ROUTE_TC)) continue;
-    if (t >= tsplit && !(route_mask & TR_ROUTE_SPTC)) continue;
+  int ta0, ta1, tb0, tb1;
+  route_ranges(pv, w, route_mask, ta0, ta1, tb0, tb1);
+  for (int t = ta0; t < tb1; ++t) {
+    if (t >= ta1 && t < tb0) continue;
     for (int k = 0; k < 16; ++k) {
       const int c = pv.tile_col[(int64_t)t * 16 + k];
       if (c < 0) continue;
@@ -413,7 +430,102 @@ __global__ void routed_generic_kernel(PlanView pv, const __half* __restrict__ B,
       acc = fmaf(__half2float(__ushort_as_half(pv.res_val[e])),
                  __half2float(B[(int64_t)pv.res_col[e] * K + f]), acc);
   }
-  store_row_feature<F16OUT>(C, K, row, f, acc);
+  const int out = pv.row_out[row];
+  if (out >= 0) store_row_feature<F16OUT>(C, K, out, f, acc * pv.row_scale[row]);
+}
+
+// ---------------------------------------------------------------------------
+// Re-valuing a plan (learnable edge weights)
+// ---------------------------------------------------------------------------
+// Row scales of a row-scaled plan: s_r = max |v| over the row's entries.  The
+// scale words start at 0; |v| >= 0 compares like its IEEE bit pattern, so an
+// integer atomicMax on the bits takes the maximum.
+__global__ void row_absmax_kernel(const float* __restrict__ v, const int32_t* __restrict__ erow,
+                                  int64_t n, float* scale) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int r = erow[e];
+    if (r >= 0) atomicMax(reinterpret_cast<int*>(scale + r), __float_as_int(fabsf(v[e])));
+  }
+}
+
+__global__ void scatter_values_kernel(const float* __restrict__ v, const int32_t* __restrict__ slot,
+                                      const int32_t* __restrict__ erow,
+                                      const float* __restrict__ scale, int64_t n,
+                                      int64_t n_tile_vals, __half* tile_a, __half* res_val) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int s = slot[e];
+    if (s < 0) continue;
+    float x = v[e];
+    if (scale) {
+      const float sr = scale[erow[e]];
+      x = sr > 0.f ? x / sr : x;
+    }
+    if (s < n_tile_vals) tile_a[s] = __float2half_rn(x);
+    else res_val[s - n_tile_vals] = __float2half_rn(x);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// SDDMM on A's pattern: out[e] = <x[row(e)], y[col(e)]>
+// ---------------------------------------------------------------------------
+// One warp per row (grid-stride); lane groups of L lanes take one entry each
+// and walk the feature dimension in 16-byte chunks; the row of x is re-read
+// from L1 per entry.  FP16 operands, FP32 products and sums.
+__device__ __forceinline__ float dot8h(const uint4& a, const uint4& b) {
+  const uint32_t x[4] = {a.x, a.y, a.z, a.w}, y[4] = {b.x, b.y, b.z, b.w};
+  float acc = 0.f;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint16_t xl = (uint16_t)(x[i] & 0xFFFFu), xh = (uint16_t)(x[i] >> 16);
+    const uint16_t yl = (uint16_t)(y[i] & 0xFFFFu), yh = (uint16_t)(y[i] >> 16);
+    asm("fma.rn.f32.f16 %0, %1, %2, %0;" : "+f"(acc) : "h"(xl), "h"(yl));
+    asm("fma.rn.f32.f16 %0, %1, %2, %0;" : "+f"(acc) : "h"(xh), "h"(yh));
+  }
+  return acc;
+}
+
+__global__ void __launch_bounds__(256) sddmm_kernel(const int32_t* __restrict__ indptr,
+                                                    const int32_t* __restrict__ indices, int M,
+                                                    const __half* __restrict__ X,
+                                                    const __half* __restrict__ Y, int K,
+                                                    float* __restrict__ out) {
+  const int lane = threadIdx.x & 31;
+  const int nchunk = K / 8;
+  int L = 1;
+  while (L < nchunk && L < 32) L <<= 1;
+  const int G = 32 / L, g = lane / L, li = lane % L;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < M; r += warps) {
+    const uint4* xr = reinterpret_cast<const uint4*>(X + (int64_t)r * K);
+    const int e0 = indptr[r], e1 = indptr[r + 1];
+    for (int eb = e0; eb < e1; eb += G) {
+      const int e = eb + g;
+      float acc = 0.f;
+      if (e < e1) {
+        const uint4* yr = reinterpret_cast<const uint4*>(Y + (int64_t)__ldg(indices + e) * K);
+        for (int c = li; c < nchunk; c += L) acc += dot8h(__ldg(xr + c), __ldg(yr + c));
+      }
+      for (int off = 1; off < L; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+      if (li == 0 && e < e1) out[e] = acc;
+    }
+  }
+}
+
+// Any K: one thread per entry.
+__global__ void sddmm_generic_kernel(const int32_t* __restrict__ indptr,
+                                     const int32_t* __restrict__ indices, int M,
+                                     const __half* __restrict__ X, const __half* __restrict__ Y,
+                                     int K, float* __restrict__ out) {
+  for (int r = blockIdx.x; r < M; r += gridDim.x)
+    for (int e = indptr[r] + threadIdx.x; e < indptr[r + 1]; e += blockDim.x) {
+      const int64_t c = indices[e];
+      float acc = 0.f;
+      for (int f = 0; f < K; ++f)
+        acc = fmaf(__half2float(X[(int64_t)r * K + f]), __half2float(Y[c * K + f]), acc);
+      out[e] = acc;
+    }
 }
 
 bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
@@ -460,6 +572,44 @@ int launch_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c
     const int blocks = (int)((n + 255) / 256);
     if (f16) routed_generic_kernel<true><<<blocks, 256, 0, stream>>>(v, bh, k, c, route_mask);
     else routed_generic_kernel<false><<<blocks, 256, 0, stream>>>(v, bh, k, c, route_mask);
+  }
+  TRS_CUDA(cudaGetLastError());
+  return TR_OK;
+}
+
+int launch_set_values(tr_plan* p, const float* values, cudaStream_t stream) {
+  const int64_t n = p->n_edges;
+  if (n == 0) return TR_OK;
+  const int threads = 256;
+  const int blocks = (int)std::min<int64_t>((n + threads - 1) / threads, 148 * 32);
+  if (p->row_scaled) {
+    TRS_CUDA(cudaMemsetAsync(p->row_scale, 0, (size_t)p->view.n_windows * kBlockRows * 4, stream));
+    row_absmax_kernel<<<blocks, threads, 0, stream>>>(values, p->edge_row, n, p->row_scale);
+    TRS_CUDA(cudaGetLastError());
+  }
+  scatter_values_kernel<<<blocks, threads, 0, stream>>>(
+      values, p->val_slot, p->edge_row, p->row_scaled ? p->row_scale : nullptr, n, p->n_tile_vals,
+      reinterpret_cast<__half*>(p->tile_a), reinterpret_cast<__half*>(p->res_val));
+  TRS_CUDA(cudaGetLastError());
+  return TR_OK;
+}
+
+int launch_sddmm(const int32_t* indptr, const int32_t* indices, int32_t m, int64_t nnz,
+                 const uint16_t* x, const uint16_t* y, int32_t k, float* out,
+                 cudaStream_t stream) {
+  if (m == 0 || nnz == 0) return TR_OK;
+  const __half* xh = reinterpret_cast<const __half*>(x);
+  const __half* yh = reinterpret_cast<const __half*>(y);
+  if (k == 0) {
+    TRS_CUDA(cudaMemsetAsync(out, 0, (size_t)nnz * 4, stream));
+    return TR_OK;
+  }
+  if (k % 8 == 0 && aligned16(x) && aligned16(y)) {
+    const int blocks = (int)std::min<int64_t>(((int64_t)m + 7) / 8, 148 * 16);
+    sddmm_kernel<<<blocks, 256, 0, stream>>>(indptr, indices, m, xh, yh, k, out);
+  } else {
+    const int blocks = (int)std::min<int64_t>(m, 148 * 32);
+    sddmm_generic_kernel<<<blocks, 128, 0, stream>>>(indptr, indices, m, xh, yh, k, out);
   }
   TRS_CUDA(cudaGetLastError());
   return TR_OK;

@@ -20,8 +20,9 @@ TR_ROUTE_COMPAT, TR_ROUTE_EXACT = 0, 1
 EXPORTED = [
     "tr_last_error", "tr_version", "tr_device_info",
     "tr_route_build", "tr_route_table", "tr_route_seconds", "tr_route_free",
-    "tr_plan_from_tables", "tr_plan_from_csr", "tr_plan_info_get", "tr_plan_free",
-    "tr_spmm_csr", "tr_spmm_routed",
+    "tr_plan_from_tables", "tr_plan_from_csr", "tr_plan_build", "tr_plan_build_host",
+    "tr_host_plan_array", "tr_host_plan_upload", "tr_host_plan_free", "tr_plan_info_get",
+    "tr_plan_free", "tr_spmm_csr", "tr_spmm_routed", "tr_plan_set_values", "tr_sddmm_csr",
     "tr_forward_fp16_tcu_cuda_sptc_mma_parallel_online", "tr_forward_fp16_sptc_online",
     "tr_forward_fp16_sptc_mma_online", "tr_forward_fp16_sptc_mma_packed_online",
 ]
@@ -47,7 +48,14 @@ class PlanInfo(ctypes.Structure):
     _fields_ = [("n_rows", ctypes.c_int32), ("n_cols", ctypes.c_int32),
                 ("n_windows", ctypes.c_int32), ("nnz", ctypes.c_int64),
                 ("tc_tiles", ctypes.c_int64), ("sptc_tiles", ctypes.c_int64),
-                ("residual_nnz", ctypes.c_int64), ("device_bytes", ctypes.c_int64)]
+                ("residual_nnz", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
+                ("promoted_tiles", ctypes.c_int64), ("row_scaled", ctypes.c_int32),
+                ("reordered", ctypes.c_int32)]
+
+
+class PlanOpts(ctypes.Structure):
+    _fields_ = [("row_scale", ctypes.c_int32), ("promote_min", ctypes.c_int32),
+                ("transpose", ctypes.c_int32), ("reorder", ctypes.c_int32)]
 
 
 _TABLE_FIELDS = ["t_row_offset", "t_block_offset", "t_column", "t_value", "t_window_row",
@@ -82,6 +90,15 @@ def lib():
     L.tr_route_free.argtypes = [P]
     L.tr_plan_from_tables.argtypes = [ctypes.POINTER(Tables), I32, I32, I32, P]
     L.tr_plan_from_csr.argtypes = [P, P, P, I32, I32, ctypes.POINTER(RouteParams), P]
+    L.tr_plan_build.argtypes = [P, P, P, I32, I32, ctypes.POINTER(RouteParams),
+                                ctypes.POINTER(PlanOpts), P]
+    L.tr_plan_build_host.argtypes = [P, P, P, I32, I32, ctypes.POINTER(RouteParams),
+                                     ctypes.POINTER(PlanOpts), P]
+    L.tr_host_plan_array.argtypes = [P, ctypes.c_int, ctypes.POINTER(P), ctypes.POINTER(I64)]
+    L.tr_host_plan_upload.argtypes = [P, P]
+    L.tr_host_plan_free.argtypes = [P]
+    L.tr_plan_set_values.argtypes = [P, P, I64, P]
+    L.tr_sddmm_csr.argtypes = [P, P, I32, I32, I64, P, P, I32, P, P]
     L.tr_plan_info_get.argtypes = [P, ctypes.POINTER(PlanInfo)]
     L.tr_plan_free.argtypes = [P]
     L.tr_spmm_csr.argtypes = [P, P, P, I32, I32, I64, P, I32, P, ctypes.c_int, P]
@@ -95,8 +112,9 @@ def lib():
     del pairs29
     for name in EXPORTED:
         if name not in ("tr_last_error", "tr_route_seconds"):
-            getattr(L, name).restype = ctypes.c_int if name != "tr_route_free" else None
+            getattr(L, name).restype = ctypes.c_int
     L.tr_plan_free.restype = None
+    L.tr_host_plan_free.restype = None
     L.tr_route_free.restype = None
     _lib = L
     return L

@@ -1,0 +1,107 @@
+"""Differentiable routed SpMM: C = A(w) . B with a hand-written adjoint.
+
+``RoutedAdjacency`` holds one sparse matrix A (CSR pattern on the device plus
+two routed plans built once: A for the forward, A^T for the adjoint).
+``routed_spmm(adj, b, w)`` is the ``torch.autograd.Function`` front end:
+
+  forward    C  = A(w) . B                         (routed kernel, plan of A)
+  backward   dB = A(w)^T . dC                      (routed kernel, plan of A^T)
+             dw[e] = <dC[row(e)], B[col(e)]>       (SDDMM on A's pattern)
+
+The reference has no backward at all; this is the differentiation path a GNN
+built on the reference's operator would need.  Operands are FP16 on the
+tensor cores with FP32 accumulation; FP32 inputs and gradients are scaled by
+their largest magnitude before the FP16 cast (and the results scaled back),
+so their FP16 copies use the full exponent range.  When the values ``w`` are
+learnable, both plans are re-valued on the device (tr_plan_set_values)
+whenever a forward or backward runs, so the pattern is routed only once.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .core import Plan, sddmm_csr
+
+
+class RoutedAdjacency:
+    """Sparse A (n_rows x n_cols, CSR) with its forward and adjoint plans."""
+
+    def __init__(self, indptr, indices, values, n_rows, n_cols, device="cuda",
+                 row_scale=True, promote_min=2, reorder=False, **route_kw):
+        indptr = np.ascontiguousarray(indptr, dtype=np.int32)
+        indices = np.ascontiguousarray(indices, dtype=np.int32)
+        values = np.ascontiguousarray(values, dtype=np.float32)
+        self.n_rows, self.n_cols = int(n_rows), int(n_cols)
+        self.nnz = int(indices.size)
+        kw = dict(row_scale=row_scale, promote_min=promote_min, reorder=reorder, **route_kw)
+        self.fwd = Plan.build(indptr, indices, values, n_rows, n_cols, transpose=False, **kw)
+        self.adj = Plan.build(indptr, indices, values, n_rows, n_cols, transpose=True, **kw)
+        self.device = torch.device(device)
+        self.indptr = torch.from_numpy(indptr).to(self.device)
+        self.indices = torch.from_numpy(indices).to(self.device)
+        self.values = torch.from_numpy(values).to(self.device)
+
+    def set_values(self, w):
+        """Re-value both plans from FP32 entry values (CUDA tensor [nnz])."""
+        w = w.detach().to(torch.float32).contiguous()
+        if w.numel() != self.nnz:
+            raise RuntimeError(f"expected {self.nnz} values, got {w.numel()}")
+        self.fwd.set_values(w)
+        self.adj.set_values(w)
+
+
+def _to_half_scaled(x):
+    """(FP16 copy of x / s, s) with s = max |x| (1 for FP16 input or all zeros)."""
+    if x.dtype == torch.float16:
+        return x.contiguous(), None
+    s = x.detach().abs().amax()
+    s = torch.where(s > 0, s, torch.ones_like(s)).to(torch.float32)
+    return (x / s).to(torch.float16).contiguous(), s
+
+
+class RoutedSpMMFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, w, b, adj):
+        if w is not None:
+            adj.set_values(w)
+        b16, sb = _to_half_scaled(b)
+        out = adj.fwd.spmm(b16, out_dtype=torch.float32)
+        if sb is not None:
+            out = out * sb
+        ctx.adj = adj
+        ctx.has_w = w is not None
+        ctx.b_dtype = b.dtype
+        ctx.save_for_backward(w if w is not None else torch.empty(0, device=b.device), b16,
+                              sb if sb is not None else torch.empty(0, device=b.device))
+        return out
+
+    @staticmethod
+    def backward(ctx, dc):
+        w, b16, sb = ctx.saved_tensors
+        adj = ctx.adj
+        if ctx.has_w:
+            adj.set_values(w)
+        dc16, sc = _to_half_scaled(dc.contiguous())
+        db = dw = None
+        if ctx.needs_input_grad[1]:
+            db = adj.adj.spmm(dc16, out_dtype=torch.float32)
+            if sc is not None:
+                db = db * sc
+            db = db.to(ctx.b_dtype)
+        if ctx.has_w and ctx.needs_input_grad[0]:
+            dw = sddmm_csr(adj.indptr, adj.indices, dc16, b16)
+            scale = None
+            if sc is not None:
+                scale = sc
+            if sb.numel():
+                scale = sb if scale is None else scale * sb
+            if scale is not None:
+                dw = dw * scale
+        return dw, db, None
+
+
+def routed_spmm(adj, b, w=None):
+    """C = A . B (FP32 out).  With w (FP32 [nnz], may require grad) the values
+    of A are w; without, the values A was built with."""
+    return RoutedSpMMFunction.apply(w, b, adj)

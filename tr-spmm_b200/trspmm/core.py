@@ -3,8 +3,13 @@
   route(...)              the three-stage router -> the reference's 30 tables
   Plan.from_tables(...)   device plan from route tables (reference layout)
   Plan.from_csr(...)      route with this library's router and build the plan
+  Plan.build(...)         native builder: row scaling, promotion of shared
+                          residual columns to tensor-core tiles, adjoint
+                          (transposed) plans, row clustering
   Plan.spmm(B)            routed forward C = A_plan . B on the GPU
+  Plan.set_values(w)      re-value a plan from FP32 per-entry values (device)
   spmm_csr(...)           the plain single-route CSR kernel
+  sddmm_csr(...)          out[e] = <X[row e], Y[col e]> on a CSR pattern
 """
 from __future__ import annotations
 
@@ -15,7 +20,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (TR_OUT_F16, TR_OUT_F32, TR_ROUTE_ALL, TR_ROUTE_COMPAT, TR_ROUTE_EXACT,
-                   PlanInfo, RouteParams, Tables, check, lib)
+                   PlanInfo, PlanOpts, RouteParams, Tables, check, lib)
 
 TABLE_NAMES = [
     "t_row_offset", "t_block_offset", "t_column", "t_value", "t_window_row", "t_atomic",
@@ -168,6 +173,33 @@ class Plan:
                                      ctypes.byref(prm), ctypes.byref(h)))
         return cls(h)
 
+    @classmethod
+    def build(cls, indptr, indices, values, n_rows, n_cols, row_scale=False, promote_min=0,
+              transpose=False, reorder=False, mode="exact", **route_kw):
+        """Native builder (tr_plan_build): route A (or A^T when transpose) and
+        lay it out; the plan keeps, for every CSR entry of A, where its value
+        lives (set_values).  For a transposed plan n_rows/n_cols are A's."""
+        rp = np.ascontiguousarray(indptr, dtype=np.int32)
+        ci = np.ascontiguousarray(indices, dtype=np.int32)
+        vv = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
+        prm = _params(mode=mode, **route_kw)
+        opts = PlanOpts(int(bool(row_scale)), int(promote_min), int(bool(transpose)),
+                        int(bool(reorder)))
+        h = ctypes.c_void_p()
+        check(lib().tr_plan_build(_vp(rp), _vp(ci), _vp(vv), int(n_rows), int(n_cols),
+                                  ctypes.byref(prm), ctypes.byref(opts), ctypes.byref(h)))
+        return cls(h)
+
+    def set_values(self, values, stream=None):
+        """Re-value the plan from a CUDA float32 tensor of A's CSR entries."""
+        import torch
+        if not (values.is_cuda and values.dtype == torch.float32 and values.is_contiguous()
+                and values.dim() == 1):
+            raise RuntimeError("values must be a contiguous 1-D float32 CUDA tensor")
+        s = stream if stream is not None else torch.cuda.current_stream(values.device).cuda_stream
+        check(lib().tr_plan_set_values(self._h, ctypes.c_void_p(values.data_ptr()),
+                                       int(values.numel()), ctypes.c_void_p(s)))
+
     def spmm(self, b, out=None, out_dtype=None, route_mask=TR_ROUTE_ALL, stream=None):
         """C = A_plan . B for a CUDA FP16 tensor B [n_cols, K]."""
         import torch
@@ -233,4 +265,69 @@ def spmm_csr(indptr, indices, values, b, n_rows, out=None, out_dtype=None, strea
                             ctypes.c_void_p(values.data_ptr()), int(n_rows), int(b.shape[0]),
                             int(indices.numel()), ctypes.c_void_p(b.data_ptr()), int(k),
                             ctypes.c_void_p(out.data_ptr()), _odt(out), ctypes.c_void_p(s)))
+    return out
+
+
+HOST_PLAN_ARRAYS = [("win_tile", np.int32), ("win_split", np.int32), ("win_prom", np.int32),
+                    ("tile_col", np.int32), ("tile_a", np.uint16), ("res_ptr", np.int32),
+                    ("res_col", np.int32), ("res_val", np.uint16), ("win_order", np.int32),
+                    ("row_scale", np.float32), ("row_out", np.int32), ("val_slot", np.int32),
+                    ("edge_row", np.int32)]
+
+
+def host_plan(indptr, indices, values, n_rows, n_cols, row_scale=False, promote_min=0,
+              transpose=False, reorder=False, mode="exact", **route_kw):
+    """The native builder's plan as host arrays (tr_plan_build_host), without
+    a device: a dict name -> numpy array (layout in csrc/plan.h)."""
+    rp = np.ascontiguousarray(indptr, dtype=np.int32)
+    ci = np.ascontiguousarray(indices, dtype=np.int32)
+    vv = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
+    prm = _params(mode=mode, **route_kw)
+    opts = PlanOpts(int(bool(row_scale)), int(promote_min), int(bool(transpose)),
+                    int(bool(reorder)))
+    L = lib()
+    h = ctypes.c_void_p()
+    check(L.tr_plan_build_host(_vp(rp), _vp(ci), _vp(vv), int(n_rows), int(n_cols),
+                               ctypes.byref(prm), ctypes.byref(opts), ctypes.byref(h)))
+    try:
+        out = {}
+        for i, (name, dt) in enumerate(HOST_PLAN_ARRAYS):
+            data = ctypes.c_void_p()
+            n = ctypes.c_int64()
+            check(L.tr_host_plan_array(h, i, ctypes.byref(data), ctypes.byref(n)))
+            if n.value == 0:
+                out[name] = np.zeros(0, dtype=dt)
+            else:
+                nbytes = n.value * np.dtype(dt).itemsize
+                buf = (ctypes.c_char * nbytes).from_address(data.value)
+                out[name] = np.frombuffer(buf, dtype=dt, count=n.value).copy()
+    finally:
+        L.tr_host_plan_free(h)
+    out["n_rows"], out["n_cols"] = (n_cols, n_rows) if transpose else (n_rows, n_cols)
+    return out
+
+
+def sddmm_csr(indptr, indices, x, y, out=None, stream=None):
+    """out[e] = <x[row(e)], y[indices[e]]> (FP16 x [m, K], y [n, K], FP32 out)
+    for every entry of the CSR pattern (int32 CUDA indptr/indices)."""
+    import torch
+    m = indptr.numel() - 1
+    for t in (x, y):
+        if not (t.is_cuda and t.dtype == torch.float16 and t.dim() == 2 and t.is_contiguous()):
+            raise RuntimeError("x and y must be contiguous 2-D float16 CUDA tensors")
+    if x.shape[0] != m or x.shape[1] != y.shape[1]:
+        raise RuntimeError("x must be [rows, K] and y [cols, K] with the same K")
+    for t in (indptr, indices):
+        if not (t.is_cuda and t.dtype == torch.int32 and t.is_contiguous()):
+            raise RuntimeError("indptr/indices must be contiguous int32 CUDA tensors")
+    nnz = indices.numel()
+    if out is None:
+        out = torch.empty(nnz, dtype=torch.float32, device=x.device)
+    if not (out.is_cuda and out.dtype == torch.float32 and out.numel() == nnz and out.is_contiguous()):
+        raise RuntimeError("out must be a contiguous float32 CUDA tensor with one item per entry")
+    s = stream if stream is not None else torch.cuda.current_stream(x.device).cuda_stream
+    check(lib().tr_sddmm_csr(ctypes.c_void_p(indptr.data_ptr()), ctypes.c_void_p(indices.data_ptr()),
+                             int(m), int(y.shape[0]), int(nnz), ctypes.c_void_p(x.data_ptr()),
+                             ctypes.c_void_p(y.data_ptr()), int(x.shape[1]),
+                             ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(s)))
     return out

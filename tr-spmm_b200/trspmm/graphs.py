@@ -219,6 +219,46 @@ def batched(num_graphs=512, nodes=(20, 500), degree=(4, 32), exponent=2.1, seed=
                  offsets=offsets, meta={"num_graphs": num_graphs})
 
 
+def subgraph(g, n_nodes, seed=0):
+    """Induced subgraph on n_nodes nodes of a square graph: whole communities
+    (``meta['block']``) in random order when the graph has them, else a
+    breadth-first region; nodes renumbered in their original order, GCN
+    values recomputed on the subgraph's pattern."""
+    rng = np.random.default_rng(seed)
+    n = g.n_rows
+    if "block" in g.meta:
+        block = np.asarray(g.meta["block"])
+        picked = []
+        for b in rng.permutation(block.max() + 1):
+            picked.append(np.nonzero(block == b)[0])
+            if sum(x.size for x in picked) >= n_nodes:
+                break
+        nodes = np.concatenate(picked)[:n_nodes]
+    else:
+        seen = np.zeros(n, bool)
+        order = []
+        frontier = [int(rng.integers(n))]
+        while len(order) < n_nodes and frontier:
+            nxt = []
+            for u in frontier:
+                if seen[u]:
+                    continue
+                seen[u] = True
+                order.append(u)
+                nxt.extend(g.indices[g.indptr[u]:g.indptr[u + 1]].tolist())
+            frontier = nxt
+        nodes = np.array(order[:n_nodes])
+    nodes = np.sort(nodes)
+    new = np.full(n, -1, np.int64)
+    new[nodes] = np.arange(nodes.size)
+    rows = np.repeat(np.arange(n), np.diff(g.indptr))
+    keep = (new[rows] >= 0) & (new[g.indices] >= 0)
+    m = nodes.size
+    indptr, indices, _ = _csr_from_edges(new[rows[keep]], new[g.indices[keep]], m, m)
+    vals = gcn_normalise(indptr, indices, m)
+    return Graph(indptr, indices, vals, m, m, g.name + "_sub", seed)
+
+
 def random_csr(n_rows, n_cols, density, seed=0, dup=False, empty_rows=0.0):
     """Small uniform random CSR for edge-case tests (optionally with empty rows)."""
     rng = np.random.default_rng(seed)
