@@ -36,8 +36,14 @@ enum {
 
 enum { TR_OUT_F32 = 0, TR_OUT_F16 = 1 };
 
-/* Route-mask bits for tr_spmm_routed (all set = full product). */
-enum { TR_ROUTE_TC = 1, TR_ROUTE_SPTC = 2, TR_ROUTE_CUDA = 4, TR_ROUTE_ALL = 7 };
+/* Route-mask bits for tr_spmm_routed (all set = full product).  By default
+ * the one-CTA-per-window fused kernel runs (TR_ROUTE_PER_WINDOW names it
+ * explicitly).  TR_ROUTE_PIPELINED added to TR_ROUTE_ALL selects the
+ * persistent warp-specialised kernel (TMA gathers, double-buffered TMEM
+ * accumulators) where it applies: K % 64 == 0, K <= 256, at most 512 windows
+ * per SM; elsewhere the fused kernel runs. */
+enum { TR_ROUTE_TC = 1, TR_ROUTE_SPTC = 2, TR_ROUTE_CUDA = 4, TR_ROUTE_ALL = 7,
+       TR_ROUTE_PER_WINDOW = 8, TR_ROUTE_PIPELINED = 16 };
 
 const char* tr_last_error(void);
 int tr_version(void);

@@ -274,7 +274,9 @@ int tr_spmm_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int 
   if (k < 0) return fail(TR_ERR_ARG, "negative K");
   if (c_dtype != TR_OUT_F32 && c_dtype != TR_OUT_F16) return fail(TR_ERR_ARG, "bad output dtype");
   if (p->view.n_rows > 0 && k > 0 && (!b || !c)) return fail(TR_ERR_ARG, "null device pointer");
-  return launch_routed(p, b, k, c, c_dtype, route_mask & TR_ROUTE_ALL, (cudaStream_t)stream);
+  return launch_routed(p, b, k, c, c_dtype,
+                       route_mask & (TR_ROUTE_ALL | TR_ROUTE_PER_WINDOW | TR_ROUTE_PIPELINED),
+                       (cudaStream_t)stream);
 }
 
 int tr_plan_set_values(tr_plan* p, const float* values, int64_t n_edges, void* stream) {

@@ -558,6 +558,11 @@ int launch_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c
   if (v.n_rows == 0 || k == 0) return TR_OK;
   const __half* bh = reinterpret_cast<const __half*>(b);
   const bool f16 = c_dtype == TR_OUT_F16;
+  const int sel = route_mask & (TR_ROUTE_PER_WINDOW | TR_ROUTE_PIPELINED);
+  route_mask &= TR_ROUTE_ALL;
+  if (route_mask == TR_ROUTE_ALL && sel == TR_ROUTE_PIPELINED && pipe_supported(k, b) &&
+      pipe_fits(p))
+    return launch_pipe(p, b, k, c, c_dtype, stream);
   if (k % 8 == 0 && aligned16(b)) {
     static bool attr[2] = {false, false};
     if (!attr[f16]) {

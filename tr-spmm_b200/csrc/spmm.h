@@ -13,6 +13,10 @@ int launch_csr(const int32_t* indptr, const int32_t* indices, const uint16_t* va
 int launch_set_values(tr_plan* p, const float* values, cudaStream_t stream);
 int launch_sddmm(const int32_t* indptr, const int32_t* indices, int32_t m, int64_t nnz,
                  const uint16_t* x, const uint16_t* y, int32_t k, float* out, cudaStream_t stream);
+bool pipe_supported(int32_t k, const void* b);
+bool pipe_fits(const tr_plan* p);
+int launch_pipe(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_dtype,
+                cudaStream_t stream);
 int launch_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_dtype,
                   int route_mask, cudaStream_t stream);
 
