@@ -153,6 +153,9 @@ typedef struct tr_plan_opts {
   int32_t reorder;         /* 1: cluster rows with shared columns into the same
                               windows before routing; results are written to the
                               original row positions */
+  int32_t demote_below;    /* 2:4 tile columns holding fewer than demote_below
+                              entries of their window go to the CUDA-core
+                              residual (0 or 1: keep the router's 2:4 tiles) */
 } tr_plan_opts;
 
 /* Native plan builder: validate the CSR, optionally transpose and reorder it,

@@ -26,6 +26,8 @@ OPTS = [
     dict(transpose=True, promote_min=2, row_scale=True),
     dict(reorder=True),
     dict(reorder=True, transpose=True, promote_min=2, row_scale=True),
+    dict(demote_below=3),
+    dict(demote_below=4, promote_min=4, reorder=True, row_scale=True),
 ]
 
 
@@ -110,6 +112,24 @@ def test_promotion_moves_shared_columns_only():
     # promote_min = 1 empties the residual (no repeated (row, col) in this graph)
     P1 = trspmm.host_plan(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, promote_min=1)
     assert len(P1["res_col"]) == 0
+
+
+def test_demotion_moves_thin_sptc_columns_only():
+    g = graphs.route_mix(n=2048, target_nnz=100_000, seed=5)
+    base = trspmm.host_plan(g.indptr, g.indices, g.values, g.n_rows, g.n_cols)
+    P = trspmm.host_plan(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, demote_below=4)
+    assert len(P["res_col"]) > len(base["res_col"])
+    Db, D = oracle.decode_plan(base), oracle.decode_plan(P)
+    assert D["sptc"].nnz < Db["sptc"].nnz and D["tc"].nnz == Db["tc"].nnz
+    wt, split, prom = P["win_tile"], P["win_split"], P["win_prom"]
+    a = P["tile_a"].view(np.float16).reshape(-1, 256)
+    i = np.arange(256)
+    k_of = ((i % 128) // 64) * 8 + (i % 8)
+    for w in range(len(wt) - 1):
+        for t in range(int(split[w]), int(prom[w])):
+            cnt = np.bincount(k_of[a[t] != 0], minlength=16)
+            used = P["tile_col"][t * 16:(t + 1) * 16] >= 0
+            assert used.any() and (cnt[used] >= 4).all()
 
 
 def test_duplicate_entries_stay_exact():

@@ -218,6 +218,7 @@ int build_plan(const int32_t* indptr, const int32_t* indices, const float* value
   if (rc) return rc;
   if (params.window != 16) { err = "routed plans need window == 16"; return TR_ERR_UNSUPPORTED; }
   if (opts.promote_min < 0) { err = "promote_min must be >= 0"; return TR_ERR_ARG; }
+  if (opts.demote_below < 0) { err = "demote_below must be >= 0"; return TR_ERR_ARG; }
   const int64_t nnz = indptr[n_rows];
   if (nnz > INT32_MAX) { err = "more than 2^31 - 1 entries"; return TR_ERR_UNSUPPORTED; }
   Csr a;
@@ -247,6 +248,7 @@ int build_plan(const int32_t* indptr, const int32_t* indices, const float* value
   PlanOptions po;
   po.row_scale = opts.row_scale != 0;
   po.promote_min = opts.promote_min;
+  po.demote_below = opts.demote_below;
   rc = plan_from_route(T, a.n_rows, a.n_cols, nnz, po, hp, err);
   if (rc) return rc;
   // entry indices of the routed matrix -> entries of the caller's A

@@ -18,14 +18,19 @@
 //       (M = 128 features, N = 16 window rows, K = 16 columns) into the
 //       window's accumulator, commit to the slot's empty barrier; after a
 //       window's last stage commit to the accumulator's full barrier;
-//       accumulators are double-buffered in TMEM so the next window's MMAs
-//       overlap the previous window's epilogue;
+//       accumulators rotate through kAcc TMEM buffers so later windows'
+//       MMAs overlap earlier windows' epilogues;
 //   epilogue warps 0-3 (thread t <-> TMEM lane t <-> feature t of a chunk)
 //       per window: wait for the accumulator, tcgen05.ld its 16 columns,
 //       add the window's CUDA-core residual entries (if the plan kept any),
 //       apply the row scale and store each output element once, to the
 //       row's original position; release the accumulator.  Row metadata is
-//       prefetched one window ahead.
+//       prefetched one window ahead.  In accumulate mode (ACC) the residual
+//       has already been written by the CUDA-core kernel: the epilogue reads
+//       those values before it waits for the accumulator (all loads ahead of
+//       all stores), adds the tiles' product and leaves windows without
+//       tiles alone.  kAcc accumulators let the MMAs run up to kAcc windows
+//       ahead of the epilogue.
 //
 // Every wait is bounded (about a second of %globaltimer); a wait that runs
 // out raises a CTA-wide abort flag, every role leaves its loop, in-flight
@@ -55,6 +60,7 @@ constexpr int kPipeThreads = (kEpiWarps + 1 + kProd) * 32;
 constexpr int kTileAop = 4096;            // 16 columns x 128 features, FP16
 constexpr int kTileBop = 512;             // 16 x 16 A block, FP16
 constexpr int kMaxWin = 512;              // windows per CTA held in shared memory
+constexpr int kAcc = 8;                   // TMEM accumulators (windows in flight)
 
 template <int NCH, int TPS>
 struct PipeCfg {
@@ -62,11 +68,11 @@ struct PipeCfg {
   static constexpr int kSlotBop = TPS * kTileBop;
   static constexpr int kSlotBytes = kSlotAop + kSlotBop;   // a multiple of 1024
   static constexpr int kBarOff = kSlots * kSlotBytes;
-  // full[S], empty[S], acc_full[2], acc_empty[2], done, tmem slot, abort flag
-  static constexpr int kWinOff = kBarOff + (2 * kSlots + 5) * 8 + 16;
+  // full[S], empty[S], acc_full[kAcc], acc_empty[kAcc], done, tmem slot, abort flag
+  static constexpr int kWinOff = kBarOff + (2 * kSlots + 2 * kAcc + 1) * 8 + 16;
   // per window of this CTA: id, first tile, end tile
   static constexpr int kSmem = 1024 + kWinOff + 3 * kMaxWin * 4;
-  static constexpr uint32_t kTmemCols = (2 * NCH * 16) <= 32 ? 32 : (2 * NCH * 16);
+  static constexpr uint32_t kTmemCols = kAcc * NCH * 16;   // 128 or 256 columns
   static_assert(kSlotBytes % 1024 == 0, "stage slots must keep 1024-byte alignment");
   static_assert(kSmem <= 227 * 1024, "shared memory budget");
   static_assert(TPS * 4 * 2 * NCH <= 32, "one gather per lane per stage");
@@ -152,20 +158,21 @@ __device__ __forceinline__ void store_out(void* C, int K, int64_t row, int f, fl
     __stcs(reinterpret_cast<float*>(C) + row * K + f, v);
 }
 
-template <bool F16OUT, int NCH, int TPS>
+template <bool F16OUT, int NCH, int TPS, bool ACC>
 __global__ void __launch_bounds__(kPipeThreads, 1)
     pipe_kernel(PlanView pv, const __grid_constant__ CUtensorMap tmap_b,
                 const __half* __restrict__ B, int K, void* C) {
   using Cfg = PipeCfg<NCH, TPS>;
   extern __shared__ uint8_t smem_raw[];
-  uint8_t* smem = reinterpret_cast<uint8_t*>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  // 1024-byte aligned base, derived by offsetting the __shared__ array so the
+  // compiler keeps it in the shared address space (LDS/STS/ATOMS, not generic)
+  uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::kBarOff);
   uint64_t* full = bars;
   uint64_t* empty = bars + kSlots;
   uint64_t* acc_full = bars + 2 * kSlots;
-  uint64_t* acc_empty = acc_full + 2;
-  uint64_t* done = acc_empty + 2;
+  uint64_t* acc_empty = acc_full + kAcc;
+  uint64_t* done = acc_empty + kAcc;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
@@ -181,7 +188,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
       mbar_init(smem_u32(&full[s]), 1);
       mbar_init(smem_u32(&empty[s]), 1);
     }
-    for (int a = 0; a < 2; ++a) {
+    for (int a = 0; a < kAcc; ++a) {
       mbar_init(smem_u32(&acc_full[a]), 1);
       mbar_init(smem_u32(&acc_empty[a]), kEpiWarps);
     }
@@ -275,7 +282,7 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
       for (int i = 0; i < nwin && ok; ++i) {
         const int t0 = s_t0[i], t1 = s_t1[i];
         if (t1 == t0) continue;
-        const int a = nacc & 1, u = nacc >> 1;
+        const int a = nacc % kAcc, u = nacc / kAcc;
         if (!wait_bar(smem_u32(&acc_empty[a]), (u & 1) ^ 1, abort_flag)) { ok = false; break; }
         tc_fence_after();
         const uint32_t dcol = tmem + (uint32_t)(a * NCH * 16);
@@ -330,9 +337,26 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
       const float scl = nsc;
       load_rows(i + 1, nro, nsc, nrp0, nrp1);
       const bool has = s_t1[i] > s_t0[i];
+      if (ACC && !has) continue;
+      // accumulate mode: C already holds the residual (written by an earlier
+      // kernel on the stream), so its values are read before the wait
+      float prev[NCH][16];
+      if (ACC) {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+          const int out = __shfl_sync(0xffffffffu, ro, r);
+#pragma unroll
+          for (int c = 0; c < NCH; ++c) {
+            const int f = c * 128 + e * 32 + lane;
+            const int64_t at = (int64_t)(out < 0 ? 0 : out) * K + (f < K ? f : 0);
+            prev[c][r] = F16OUT ? __half2float(reinterpret_cast<const __half*>(C)[at])
+                                : reinterpret_cast<const float*>(C)[at];
+          }
+        }
+      }
       float d[NCH][16];
       if (has) {
-        const int a = nacc & 1, u = nacc >> 1;
+        const int a = nacc % kAcc, u = nacc / kAcc;
         if (!wait_bar(smem_u32(&acc_full[a]), u & 1, abort_flag)) break;
         tc_fence_after();
 #pragma unroll
@@ -347,6 +371,20 @@ __global__ void __launch_bounds__(kPipeThreads, 1)
         for (int c = 0; c < NCH; ++c)
 #pragma unroll
           for (int r = 0; r < 16; ++r) d[c][r] = 0.f;
+      }
+      if (ACC) {
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+          const int out = __shfl_sync(0xffffffffu, ro, r);
+          const float sc = __shfl_sync(0xffffffffu, scl, r);
+          if (out < 0) continue;
+#pragma unroll
+          for (int c = 0; c < NCH; ++c) {
+            const int f = c * 128 + e * 32 + lane;
+            if (f < K) store_out<F16OUT>(C, K, out, f, prev[c][r] + d[c][r] * sc);
+          }
+        }
+        continue;
       }
 #pragma unroll
       for (int r = 0; r < 16; ++r) {
@@ -401,12 +439,12 @@ int make_b_map(CUtensorMap* map, const void* b, int32_t n_cols, int32_t k) {
   return TR_OK;
 }
 
-template <bool F16OUT, int NCH, int TPS>
+template <bool F16OUT, int NCH, int TPS, bool ACC>
 int launch_pipe_t(const tr_plan* p, const __half* b, int32_t k, void* c, cudaStream_t stream) {
   using Cfg = PipeCfg<NCH, TPS>;
   static bool attr = false;
   if (!attr) {
-    TRS_CUDA(cudaFuncSetAttribute(pipe_kernel<F16OUT, NCH, TPS>,
+    TRS_CUDA(cudaFuncSetAttribute(pipe_kernel<F16OUT, NCH, TPS, ACC>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::kSmem));
     attr = true;
   }
@@ -414,7 +452,7 @@ int launch_pipe_t(const tr_plan* p, const __half* b, int32_t k, void* c, cudaStr
   int rc = make_b_map(&map, b, p->view.n_cols, k);
   if (rc) return rc;
   const int grid = std::max(1, std::min(sm_count(), p->view.n_windows));
-  pipe_kernel<F16OUT, NCH, TPS><<<grid, kPipeThreads, Cfg::kSmem, stream>>>(p->view, map, b, k, c);
+  pipe_kernel<F16OUT, NCH, TPS, ACC><<<grid, kPipeThreads, Cfg::kSmem, stream>>>(p->view, map, b, k, c);
   TRS_CUDA(cudaGetLastError());
   return TR_OK;
 }
@@ -432,18 +470,25 @@ bool pipe_fits(const tr_plan* p) {
 }
 
 int launch_pipe(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_dtype,
-                cudaStream_t stream) {
+                bool accumulate, cudaStream_t stream) {
   if (p->view.n_rows == 0 || k == 0) return TR_OK;
   if (!pipe_supported(k, b) || !pipe_fits(p))
     return fail(TR_ERR_UNSUPPORTED,
                 "pipelined kernel needs K % 64 == 0, K <= 256 and at most 512 windows per SM");
   const __half* bh = reinterpret_cast<const __half*>(b);
   const bool f16 = c_dtype == TR_OUT_F16;
+  if (accumulate) {
+    if (k <= 128)
+      return f16 ? launch_pipe_t<true, 1, 4, true>(p, bh, k, c, stream)
+                 : launch_pipe_t<false, 1, 4, true>(p, bh, k, c, stream);
+    return f16 ? launch_pipe_t<true, 2, 2, true>(p, bh, k, c, stream)
+               : launch_pipe_t<false, 2, 2, true>(p, bh, k, c, stream);
+  }
   if (k <= 128)
-    return f16 ? launch_pipe_t<true, 1, 4>(p, bh, k, c, stream)
-               : launch_pipe_t<false, 1, 4>(p, bh, k, c, stream);
-  return f16 ? launch_pipe_t<true, 2, 2>(p, bh, k, c, stream)
-             : launch_pipe_t<false, 2, 2>(p, bh, k, c, stream);
+    return f16 ? launch_pipe_t<true, 1, 4, false>(p, bh, k, c, stream)
+               : launch_pipe_t<false, 1, 4, false>(p, bh, k, c, stream);
+  return f16 ? launch_pipe_t<true, 2, 2, false>(p, bh, k, c, stream)
+             : launch_pipe_t<false, 2, 2, false>(p, bh, k, c, stream);
 }
 
 }  // namespace trs

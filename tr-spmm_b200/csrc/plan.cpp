@@ -82,6 +82,43 @@ inline int elem_row(int i) { return (i / 128) * 8 + (i % 64) / 8; }
 // the tensor cores: 16 such columns per tile, each (row, column) once (a
 // repeated entry stays in the residual).  Columns are taken in increasing
 // order so the result does not depend on the residual's entry order.
+// 2:4 tile columns holding fewer than `min_rows` entries of their window go
+// back to the CUDA-core residual (a gathered feature row that serves one or
+// two rows costs the tensor core more than the CUDA cores); tiles left empty
+// are dropped.
+void demote(Staging& st, int W, int min_rows) {
+  if (min_rows <= 1) return;
+  for (int w = 0; w < W; ++w) {
+    WinTiles& wt = st.sp[w];
+    WinTiles kept;
+    for (int t = 0; t < wt.n; ++t) {
+      const size_t cb = (size_t)t * 16, ab = (size_t)t * 256;
+      int cnt[16] = {0};
+      for (int i = 0; i < 256; ++i)
+        if (wt.a[ab + i] != 0.f || wt.edge[ab + i] >= 0) cnt[((i % 128) / 64) * 8 + (i % 8)]++;
+      bool any = false;
+      for (int k = 0; k < 16; ++k) {
+        if (wt.col[cb + k] < 0) continue;
+        if (cnt[k] >= min_rows) { any = true; continue; }
+        for (int i = 0; i < 256; ++i) {
+          if (((i % 128) / 64) * 8 + (i % 8) != k) continue;
+          if (wt.a[ab + i] == 0.f && wt.edge[ab + i] < 0) continue;
+          st.res.push_back({w * 16 + elem_row(i), wt.col[cb + k], wt.a[ab + i], wt.edge[ab + i]});
+          wt.a[ab + i] = 0.f;
+          wt.edge[ab + i] = -1;
+        }
+        wt.col[cb + k] = -1;
+      }
+      if (!any) continue;
+      kept.col.insert(kept.col.end(), wt.col.begin() + cb, wt.col.begin() + cb + 16);
+      kept.a.insert(kept.a.end(), wt.a.begin() + ab, wt.a.begin() + ab + 256);
+      kept.edge.insert(kept.edge.end(), wt.edge.begin() + ab, wt.edge.begin() + ab + 256);
+      kept.n++;
+    }
+    wt = std::move(kept);
+  }
+}
+
 void promote(Staging& st, int W, int min_rows) {
   if (min_rows <= 0) return;
   std::vector<std::vector<size_t>> by_win(W);
@@ -129,6 +166,7 @@ void promote(Staging& st, int W, int min_rows) {
 void flatten(HostPlan& hp, Staging& st, const PlanOptions& opt, int64_t n_edges) {
   const int W = hp.n_windows;
   const int64_t rows = (int64_t)W * 16;
+  demote(st, W, opt.demote_below);
   promote(st, W, opt.promote_min);
   // ---- per-row scales ---------------------------------------------------------
   hp.row_scale.assign(rows, 1.0f);

@@ -89,6 +89,8 @@ struct PlanOptions {
   bool row_scale = false;       // per-row FP32 scale, FP16(v / scale) stored
   int promote_min = 0;          // residual columns used by >= this many rows of a
                                 // window become tensor-core tiles (0: never)
+  int demote_below = 0;         // 2:4 tile columns with fewer entries than this
+                                // go to the CUDA-core residual (0, 1: never)
 };
 
 // Host construction from the reference's tables (validates every index).

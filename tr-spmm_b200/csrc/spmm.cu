@@ -153,15 +153,25 @@ __device__ __forceinline__ void store_row_feature(void* C, int K, int64_t row, i
 // ---------------------------------------------------------------------------
 // Plain CSR (single route)
 // ---------------------------------------------------------------------------
-template <bool F16OUT>
+// With PLAN, the rows are a plan's rows (its CUDA-core residual as CSR) and
+// each result row r is scaled by row_scale[r] and stored to row row_out[r]
+// (skipped when negative).
+template <bool F16OUT, bool PLAN = false>
 __global__ void __launch_bounds__(kThreads, 4) csr_block_kernel(
     const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
-    const __half* __restrict__ values, int M, const __half* __restrict__ B, int K, void* C) {
+    const __half* __restrict__ values, int M, const __half* __restrict__ B, int K, void* C,
+    const int32_t* __restrict__ row_out = nullptr, const float* __restrict__ row_scale = nullptr) {
   __shared__ __align__(16) float racc[kBlockRows * kChunk];
   __shared__ int2 sent[kStage];
   __shared__ int rp[kBlockRows + 1];
+  __shared__ int s_out[kBlockRows];
+  __shared__ float s_scale[kBlockRows];
   const int r0 = blockIdx.x * kBlockRows;
   if (threadIdx.x <= kBlockRows) rp[threadIdx.x] = indptr[min(r0 + (int)threadIdx.x, M)];
+  if (PLAN && threadIdx.x < kBlockRows) {
+    s_out[threadIdx.x] = r0 + (int)threadIdx.x < M ? row_out[r0 + threadIdx.x] : -1;
+    s_scale[threadIdx.x] = r0 + (int)threadIdx.x < M ? row_scale[r0 + threadIdx.x] : 0.f;
+  }
   for (int f0 = 0; f0 < K; f0 += kChunk) {
     const int fc = min(kChunk, K - f0);
     for (int i = threadIdx.x; i < kBlockRows * kChunk; i += kThreads) racc[i] = 0.f;
@@ -174,7 +184,12 @@ __global__ void __launch_bounds__(kThreads, 4) csr_block_kernel(
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
         const int r = (warp >> 2) * 8 + i;
-        if (r0 + r < M) store_row_feature<F16OUT>(C, K, r0 + r, f0 + f, racc[r * kChunk + f]);
+        if (PLAN) {
+          if (s_out[r] >= 0)
+            store_row_feature<F16OUT>(C, K, s_out[r], f0 + f, racc[r * kChunk + f] * s_scale[r]);
+        } else if (r0 + r < M) {
+          store_row_feature<F16OUT>(C, K, r0 + r, f0 + f, racc[r * kChunk + f]);
+        }
       }
     }
     __syncthreads();
@@ -195,6 +210,10 @@ __global__ void csr_generic_kernel(const int32_t* __restrict__ indptr,
     acc = fmaf(__half2float(values[e]), __half2float(B[(int64_t)indices[e] * K + f]), acc);
   store_row_feature<F16OUT>(C, K, r, f, acc);
 }
+
+// Kernel-internal route-mask bit: every tile of the selected routes, none of
+// the CUDA-core residual entries (they were computed by another kernel).
+constexpr int kTilesOnly = 64;
 
 // Tile ranges of window w that route_mask selects: [a0, a1) dense TC tiles,
 // [b0, b1) 2:4 tiles and/or promoted residual columns (which follow the 2:4
@@ -232,15 +251,16 @@ constexpr int kAOpBytes = 4096;
 constexpr int kBOpBytes = 512;
 constexpr int kTileColCap = kStage / 16;    // tiles whose columns fit the staging buffer
 constexpr int kSmemRouted = 1024 + 2 * kHalf * (kAOpBytes + kBOpBytes) + kBlockRows * kChunk * 4 +
-                            kStage * 8 + 128;
+                            kStage * 8 + 128 + 2 * kBlockRows * 4;
 constexpr uint32_t kIdesc = umma_idesc_f16(128, 16, /*a MN-major*/ true, /*b MN-major*/ false);
 
-template <bool F16OUT>
+template <bool F16OUT, bool ACC = false>
 __global__ void __launch_bounds__(kThreads, 3) routed_kernel(PlanView pv, const __half* __restrict__ B,
                                                           int K, void* C, int route_mask) {
   extern __shared__ uint8_t smem_raw[];
-  uint8_t* smem = reinterpret_cast<uint8_t*>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  // 1024-byte aligned base, derived by offsetting the __shared__ array so the
+  // compiler keeps it in the shared address space (LDS/STS/ATOMS, not generic)
+  uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   uint8_t* aop = smem;
   uint8_t* bop = smem + 2 * kHalf * kAOpBytes;
   float* racc = reinterpret_cast<float*>(bop + 2 * kHalf * kBOpBytes);
@@ -248,6 +268,10 @@ __global__ void __launch_bounds__(kThreads, 3) routed_kernel(PlanView pv, const 
   int* scol = reinterpret_cast<int*>(sent);          // tile columns while gathering tiles
   int* rp = reinterpret_cast<int*>(sent + kStage);
   uint64_t* mbar = reinterpret_cast<uint64_t*>(rp + 18);
+  // the window's output rows and row scales, read once at the start so the
+  // epilogue's stores wait on shared memory only
+  int* s_out = reinterpret_cast<int*>(mbar + 2) + 4;
+  float* s_scale = reinterpret_cast<float*>(s_out + kBlockRows);
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -261,11 +285,15 @@ __global__ void __launch_bounds__(kThreads, 3) routed_kernel(PlanView pv, const 
   route_ranges(pv, w, route_mask, ta0, ta1, tb0, tb1);
   const int n_tc = ta1 - ta0;
   const int nt = n_tc + (tb1 - tb0);
-  const bool do_res = (route_mask & TR_ROUTE_CUDA) != 0;
+  const bool do_res = (route_mask & TR_ROUTE_CUDA) != 0 && !(route_mask & kTilesOnly);
 
   if (tid <= kBlockRows) {
     const int64_t rr = (int64_t)w * kBlockRows + tid;
     rp[tid] = do_res ? pv.res_ptr[rr] : 0;
+    if (tid < kBlockRows) {
+      s_out[tid] = r0 + tid < M ? pv.row_out[rr] : -1;
+      s_scale[tid] = pv.row_scale[rr];
+    }
   }
   uint32_t tmem = 0;
   if (nt > 0) {
@@ -384,13 +412,24 @@ __global__ void __launch_bounds__(kThreads, 3) routed_kernel(PlanView pv, const 
     }
     const int f = (warp & 3) * 32 + lane;
     if (f < fc) {
+      float prev[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {             // loads before any store (same pointer)
+        prev[i] = 0.f;
+        const int out = s_out[(warp >> 2) * 8 + i];
+        if (ACC && out >= 0) {
+          const int64_t at = (int64_t)out * K + f0 + f;
+          prev[i] = F16OUT ? __half2float(reinterpret_cast<const __half*>(C)[at])
+                           : reinterpret_cast<const float*>(C)[at];
+        }
+      }
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
         const int r = (warp >> 2) * 8 + i;
-        const int out = r0 + r < M ? pv.row_out[r0 + r] : -1;
+        const int out = s_out[r];
         if (out >= 0)
           store_row_feature<F16OUT>(C, K, out, f0 + f,
-                                    (d[i] + racc[r * kChunk + f]) * pv.row_scale[r0 + r]);
+                                    prev[i] + (d[i] + racc[r * kChunk + f]) * s_scale[r]);
       }
     }
     tc_fence_before();
@@ -552,6 +591,51 @@ int launch_csr(const int32_t* indptr, const int32_t* indices, const uint16_t* va
   return TR_OK;
 }
 
+namespace {
+
+// The plan's CUDA-core residual as a plain CSR over plan rows, each result
+// row scaled and stored to its output row (every output row is written).
+int launch_residual(const PlanView& v, const __half* bh, int32_t k, void* c, bool f16,
+                    cudaStream_t stream) {
+  const int rows = v.n_windows * kBlockRows;
+  const __half* rv = reinterpret_cast<const __half*>(v.res_val);
+  if (f16)
+    csr_block_kernel<true, true><<<v.n_windows, kThreads, 0, stream>>>(v.res_ptr, v.res_col, rv, rows,
+                                                                       bh, k, c, v.row_out, v.row_scale);
+  else
+    csr_block_kernel<false, true><<<v.n_windows, kThreads, 0, stream>>>(v.res_ptr, v.res_col, rv, rows,
+                                                                        bh, k, c, v.row_out, v.row_scale);
+  TRS_CUDA(cudaGetLastError());
+  return TR_OK;
+}
+
+// One CTA per window (tiles on tcgen05, residual on CUDA cores, in one
+// kernel); with ACC the result is added to C.
+template <bool ACC>
+int launch_per_window(const PlanView& v, const __half* bh, int32_t k, void* c, bool f16,
+                      int route_mask, cudaStream_t stream) {
+  static bool attr[2] = {false, false};
+  if (!attr[f16]) {
+    if (f16) TRS_CUDA(cudaFuncSetAttribute(routed_kernel<true, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemRouted));
+    else TRS_CUDA(cudaFuncSetAttribute(routed_kernel<false, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemRouted));
+    attr[f16] = true;
+  }
+  if (f16) routed_kernel<true, ACC><<<v.n_windows, kThreads, kSmemRouted, stream>>>(v, bh, k, c, route_mask);
+  else routed_kernel<false, ACC><<<v.n_windows, kThreads, kSmemRouted, stream>>>(v, bh, k, c, route_mask);
+  TRS_CUDA(cudaGetLastError());
+  return TR_OK;
+}
+
+}  // namespace
+
+// Full product (route_mask == TR_ROUTE_ALL, K % 8 == 0): the CUDA-core
+// residual runs as its own kernel over every window and writes C, then the
+// tensor-core tiles are added to C, by the pipelined kernel where K allows
+// (K % 64 == 0, K <= 256) or by the per-window kernel in accumulate mode.
+// A plan without residual entries needs only the tile kernel; a plan
+// without tiles only the residual kernel.  TR_ROUTE_PER_WINDOW runs the
+// single fused per-window kernel instead; TR_ROUTE_PIPELINED the single
+// pipelined kernel (its epilogue adding any residual).
 int launch_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_dtype,
                   int route_mask, cudaStream_t stream) {
   const PlanView& v = p->view;
@@ -560,24 +644,25 @@ int launch_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c
   const bool f16 = c_dtype == TR_OUT_F16;
   const int sel = route_mask & (TR_ROUTE_PER_WINDOW | TR_ROUTE_PIPELINED);
   route_mask &= TR_ROUTE_ALL;
-  if (route_mask == TR_ROUTE_ALL && sel == TR_ROUTE_PIPELINED && pipe_supported(k, b) &&
-      pipe_fits(p))
-    return launch_pipe(p, b, k, c, c_dtype, stream);
-  if (k % 8 == 0 && aligned16(b)) {
-    static bool attr[2] = {false, false};
-    if (!attr[f16]) {
-      if (f16) TRS_CUDA(cudaFuncSetAttribute(routed_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemRouted));
-      else TRS_CUDA(cudaFuncSetAttribute(routed_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemRouted));
-      attr[f16] = true;
-    }
-    if (f16) routed_kernel<true><<<v.n_windows, kThreads, kSmemRouted, stream>>>(v, bh, k, c, route_mask);
-    else routed_kernel<false><<<v.n_windows, kThreads, kSmemRouted, stream>>>(v, bh, k, c, route_mask);
-  } else {
-    const int64_t n = (int64_t)v.n_rows * k;
-    const int blocks = (int)((n + 255) / 256);
-    if (f16) routed_generic_kernel<true><<<blocks, 256, 0, stream>>>(v, bh, k, c, route_mask);
-    else routed_generic_kernel<false><<<blocks, 256, 0, stream>>>(v, bh, k, c, route_mask);
+  const bool vec = k % 8 == 0 && aligned16(b);
+  const bool pipe_ok = pipe_supported(k, b) && pipe_fits(p);
+  if (route_mask == TR_ROUTE_ALL && vec && sel == 0) {
+    const bool tiles = p->info.tc_tiles + p->info.sptc_tiles + p->info.promoted_tiles > 0;
+    const bool res = p->info.residual_nnz > 0;
+    if (!tiles) return launch_residual(v, bh, k, c, f16, stream);
+    if (!res && pipe_ok) return launch_pipe(p, b, k, c, c_dtype, false, stream);
+    int rc = launch_residual(v, bh, k, c, f16, stream);
+    if (rc) return rc;
+    if (pipe_ok) return launch_pipe(p, b, k, c, c_dtype, true, stream);
+    return launch_per_window<true>(v, bh, k, c, f16, TR_ROUTE_ALL | kTilesOnly, stream);
   }
+  if (route_mask == TR_ROUTE_ALL && sel == TR_ROUTE_PIPELINED && pipe_ok)
+    return launch_pipe(p, b, k, c, c_dtype, false, stream);
+  if (vec) return launch_per_window<false>(v, bh, k, c, f16, route_mask, stream);
+  const int64_t n = (int64_t)v.n_rows * k;
+  const int blocks = (int)((n + 255) / 256);
+  if (f16) routed_generic_kernel<true><<<blocks, 256, 0, stream>>>(v, bh, k, c, route_mask);
+  else routed_generic_kernel<false><<<blocks, 256, 0, stream>>>(v, bh, k, c, route_mask);
   TRS_CUDA(cudaGetLastError());
   return TR_OK;
 }

@@ -16,7 +16,7 @@ int launch_sddmm(const int32_t* indptr, const int32_t* indices, int32_t m, int64
 bool pipe_supported(int32_t k, const void* b);
 bool pipe_fits(const tr_plan* p);
 int launch_pipe(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_dtype,
-                cudaStream_t stream);
+                bool accumulate, cudaStream_t stream);
 int launch_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_dtype,
                   int route_mask, cudaStream_t stream);
 

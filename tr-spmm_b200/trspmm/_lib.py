@@ -56,7 +56,8 @@ class PlanInfo(ctypes.Structure):
 
 class PlanOpts(ctypes.Structure):
     _fields_ = [("row_scale", ctypes.c_int32), ("promote_min", ctypes.c_int32),
-                ("transpose", ctypes.c_int32), ("reorder", ctypes.c_int32)]
+                ("transpose", ctypes.c_int32), ("reorder", ctypes.c_int32),
+                ("demote_below", ctypes.c_int32)]
 
 
 _TABLE_FIELDS = ["t_row_offset", "t_block_offset", "t_column", "t_value", "t_window_row",

@@ -175,7 +175,7 @@ class Plan:
 
     @classmethod
     def build(cls, indptr, indices, values, n_rows, n_cols, row_scale=False, promote_min=0,
-              transpose=False, reorder=False, mode="exact", **route_kw):
+              transpose=False, reorder=False, demote_below=0, mode="exact", **route_kw):
         """Native builder (tr_plan_build): route A (or A^T when transpose) and
         lay it out; the plan keeps, for every CSR entry of A, where its value
         lives (set_values).  For a transposed plan n_rows/n_cols are A's."""
@@ -184,7 +184,7 @@ class Plan:
         vv = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
         prm = _params(mode=mode, **route_kw)
         opts = PlanOpts(int(bool(row_scale)), int(promote_min), int(bool(transpose)),
-                        int(bool(reorder)))
+                        int(bool(reorder)), int(demote_below))
         h = ctypes.c_void_p()
         check(lib().tr_plan_build(_vp(rp), _vp(ci), _vp(vv), int(n_rows), int(n_cols),
                                   ctypes.byref(prm), ctypes.byref(opts), ctypes.byref(h)))
@@ -276,7 +276,7 @@ HOST_PLAN_ARRAYS = [("win_tile", np.int32), ("win_split", np.int32), ("win_prom"
 
 
 def host_plan(indptr, indices, values, n_rows, n_cols, row_scale=False, promote_min=0,
-              transpose=False, reorder=False, mode="exact", **route_kw):
+              transpose=False, reorder=False, demote_below=0, mode="exact", **route_kw):
     """The native builder's plan as host arrays (tr_plan_build_host), without
     a device: a dict name -> numpy array (layout in csrc/plan.h)."""
     rp = np.ascontiguousarray(indptr, dtype=np.int32)
@@ -284,7 +284,7 @@ def host_plan(indptr, indices, values, n_rows, n_cols, row_scale=False, promote_
     vv = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
     prm = _params(mode=mode, **route_kw)
     opts = PlanOpts(int(bool(row_scale)), int(promote_min), int(bool(transpose)),
-                    int(bool(reorder)))
+                    int(bool(reorder)), int(demote_below))
     L = lib()
     h = ctypes.c_void_p()
     check(L.tr_plan_build_host(_vp(rp), _vp(ci), _vp(vv), int(n_rows), int(n_cols),
