@@ -3,22 +3,32 @@
 Workload: the large routed SpMM — SBM graph, N = 200,000 nodes, mean degree
 50 (~10.2 M nnz with self loops), 2,000 communities of ~100 nodes, 70 % of
 edges inside a community, power-law degrees, nodes randomly permuted, GCN
-values in FP16; B = 200,000 x 128 FP16 ~ N(0,1).  Seeded synthetic data: the
+values; B = 200,000 x 128 FP16 ~ N(0,1).  Seeded synthetic data: the
 reference ships no datasets.
 
-A step = one routed forward C = A . B (FP16 in, FP32 accumulate, FP32 out,
-the reference's output type) over the whole matrix with the device plan
-resident in HBM.  Between timed steps a 256 MiB buffer is written to flush
-L2 (126 MB); each step is timed alone with CUDA events on its stream.
+A step = one routed forward + adjoint, as a GNN layer's training step runs
+it: C = A . B (routed forward plan), dB = A^T . dC (routed adjoint plan,
+built once), dval = SDDMM(dC, B) on A's pattern (the edge-weight gradient);
+FP16 operands, FP32 accumulation and outputs, dC a fixed synthetic FP16
+gradient.  Plans are built once, outside the timed region, with the plan
+options the autotuner (trspmm.autotune) finds fastest for this graph.
+Between timed steps a 256 MiB buffer is written to flush L2 (126 MB); each
+step is timed alone with CUDA events on its stream.
 
-  value       SpMM TFLOP/s = 2 * nnz * K / t, summed over ranks (replicas)
-  e2e         same metric through the public API with host buffers: per step
-              the H2D copy of B from pinned memory, the routed kernel and the
-              D2H copy of C into pinned memory
-  roofline    routed kernel vs measured HBM copy bandwidth, algorithmic bytes
-              nnz*(4+2) + (M+1)*4 + N*K*2 + M*K*4 per launch
-  cpu_baseline / --impl reference: the oracle's C restatement of the SpMM
-              (FP16 operands, FP32 accumulation, OpenMP on all host cores)
+  value       TFLOP/s = 3 * 2 * nnz * K / t (forward, adjoint, SDDMM), summed
+              over ranks (replicas)
+  e2e         same metric through the public API with host buffers: per
+              step B and dC copied from pinned memory, the autograd forward and
+              backward of trspmm.autograd.routed_spmm, and C, dB and dval copied
+              back to pinned memory
+  roofline    the dominant kernel (the forward's CUDA-core residual pass)
+              against the measured HBM copy bandwidth; algorithmic bytes per
+              launch = res_nnz*(4+2) + (M+1)*4 + N*K*2 + M*K*4
+  cpu_baseline / --impl reference: the oracle's C restatement of the same
+              step (FP16 operands, FP32 accumulation, OpenMP on all host cores)
+  extra       the same step with the plain single-route CSR kernel (forward on
+              A, adjoint on a CSR of A^T, same SDDMM), per-pass times and the
+              autotuner's table
 
 Multi-GPU: the path does not shard (replicas only); under torchrun every rank
 runs the full workload independently and rank 0 reports max-over-ranks time.
@@ -55,9 +65,10 @@ def _peaks():
 
 
 def _profile_traffic():
-    """Per-launch DRAM bytes of the routed kernel from the committed ncu
-    summary (profiles/routed_kernel_large_routed.txt, line 'traffic_bytes_per_launch: N')."""
-    path = os.path.join(ROOT, "profiles", "routed_kernel_large_routed.txt")
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
+    summary (profiles/csr_residual_pass_large_routed.txt, line
+    'traffic_bytes_per_launch: N'); None when that summary is absent."""
+    path = os.path.join(ROOT, "profiles", "csr_residual_pass_large_routed.txt")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -130,24 +141,50 @@ def algorithmic_bytes(nnz, m, n_cols, k, out_bytes=4):
     return nnz * (4 + 2) + (m + 1) * 4 + n_cols * k * 2 + m * k * out_bytes
 
 
-def cpu_baseline(g, b, budget_s=12.0):
-    """Oracle C SpMM (FP16 operands, FP32 accumulation) on all host cores,
-    repeated for ~budget_s seconds; TFLOP/s."""
-    import oracle
-    vals = g.values.astype(np.float16)
-    out = np.empty((g.n_rows, b.shape[1]), dtype=np.float32)
-    threads = oracle.max_threads()
-    oracle.spmm_f16_f32(g.indptr, g.indices, vals, b, threads=threads, out=out)   # warm-up
-    reps, t0 = 0, time.perf_counter()
-    while True:
-        oracle.spmm_f16_f32(g.indptr, g.indices, vals, b, threads=threads, out=out)
-        reps += 1
-        el = time.perf_counter() - t0
-        if el >= budget_s or reps >= 50:
-            break
-    tflops = 2.0 * g.nnz * b.shape[1] * reps / el / 1e12
-    return {"value": tflops, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"full workload ({g.nnz} nnz x K={b.shape[1]}), {reps} passes in {el:.1f} s"}
+def step_bytes(nnz, m, n, k):
+    """Forward + adjoint + SDDMM algorithmic bytes (FP32 outputs)."""
+    sddmm = nnz * 4 + m * k * 2 + n * k * 2 + nnz * 4
+    return algorithmic_bytes(nnz, m, n, k) + algorithmic_bytes(nnz, n, m, k) + sddmm
+
+
+def transpose_csr(indptr, indices, values, n_rows, n_cols):
+    import scipy.sparse as sp
+    a = sp.csr_matrix((values, indices, indptr), shape=(n_rows, n_cols)).T.tocsr()
+    a.sort_indices()
+    return a.indptr.astype(np.int32), a.indices.astype(np.int32), a.data.astype(np.float32)
+
+
+class CpuStep:
+    """The step on the host cores with the oracle's C arithmetic (FP16
+    operands, FP32 accumulation, OpenMP on every host thread)."""
+
+    def __init__(self, g, gt, b, dc):
+        import oracle
+        self.oracle = oracle
+        self.threads = oracle.max_threads()
+        self.g, self.gt, self.b, self.dc = g, gt, b, dc
+        self.v16, self.vt16 = g.values.astype(np.float16), gt[2].astype(np.float16)
+        k = b.shape[1]
+        self.c = np.empty((g.n_rows, k), dtype=np.float32)
+        self.db = np.empty((g.n_cols, k), dtype=np.float32)
+        self.dv = np.empty(g.nnz, dtype=np.float32)
+
+    def __call__(self):
+        o, g, gt, t = self.oracle, self.g, self.gt, self.threads
+        o.spmm_f16_f32(g.indptr, g.indices, self.v16, self.b, threads=t, out=self.c)
+        o.spmm_f16_f32(gt[0], gt[1], self.vt16, self.dc, threads=t, out=self.db)
+        o.sddmm_f16_f32(g.indptr, g.indices, self.dc, self.b, threads=t, out=self.dv)
+
+    def time(self, budget_s=12.0, max_steps=50):
+        """(seconds per step, steps timed) over about budget_s seconds."""
+        self()
+        reps, t0 = 0, time.perf_counter()
+        while True:
+            self()
+            reps += 1
+            el = time.perf_counter() - t0
+            if el >= budget_s or reps >= max_steps:
+                return el / reps, reps
 
 
 def dist_setup():
@@ -157,45 +194,53 @@ def dist_setup():
     return world, rank, local
 
 
+def workload():
+    from trspmm import graphs
+    g, b = graphs.make_workload(WORKLOAD)
+    dc = graphs.dense_features(g.n_rows, b.shape[1], "normal", seed=g.seed + 101)
+    return g, b, dc
+
+
 def run_reference(args):
     world, rank, _ = dist_setup()
     if rank != 0:
         return
-    from trspmm import graphs
-    g, b = graphs.make_workload(WORKLOAD)
-    import oracle
-    vals = g.values.astype(np.float16)
-    out = np.empty((g.n_rows, b.shape[1]), dtype=np.float32)
-    threads = oracle.max_threads()
-    for _ in range(max(1, args.warmup)):
-        oracle.spmm_f16_f32(g.indptr, g.indices, vals, b, threads=threads, out=out)
-    steps = max(1, min(args.steps, 20))      # a CPU pass takes ~0.1-1 s; bounded sample
+    g, b, dc = workload()
+    gt = transpose_csr(g.indptr, g.indices, g.values, g.n_rows, g.n_cols)
+    k = int(b.shape[1])
+    step = CpuStep(g, gt, b, dc)
+    for _ in range(max(1, min(args.warmup, 3))):
+        step()
+    steps = max(1, min(args.steps, 10))      # a CPU step takes ~1 s; bounded sample
     t0 = time.perf_counter()
     for _ in range(steps):
-        oracle.spmm_f16_f32(g.indptr, g.indices, vals, b, threads=threads, out=out)
+        step()
     el = time.perf_counter() - t0
-    v = 2.0 * g.nnz * b.shape[1] * steps / el / 1e12
+    v = 3 * 2.0 * g.nnz * k * steps / el / 1e12
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
             "steps": steps, "warmup": args.warmup, "ms_per_step": el / steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_nodes": g.n_rows, "nnz": g.nnz, "k": int(b.shape[1]),
-                       "out": "f32"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"full workload, {steps} passes"},
+            "config": {"workload": WORKLOAD, "n_nodes": g.n_rows, "nnz": g.nnz, "k": k,
+                       "step": "forward + adjoint + SDDMM", "out": "f32"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": step.threads, "kind": "port",
+                             "sample": f"full workload, {steps} steps"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "note": "the reference has no CPU SpMM; its GPU operator's semantics are run by the "
-                    "oracle's C restatement (C = A.B over the routed operand) on all host cores"}
+            "note": "the reference has no CPU SpMM and no backward; its operator's semantics "
+                    "(C = A.B over the routed operand) and the adjoint are run by the oracle's C "
+                    "restatement on all host cores"}
     print(json.dumps(line), flush=True)
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=2000)
-    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the autotuner and use the reference's routing (exact mode)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -203,7 +248,8 @@ def main():
     import torch
     import torch.distributed as dist
     import trspmm
-    from trspmm import graphs
+    from trspmm import autotune
+    from trspmm.autograd import RoutedAdjacency, routed_spmm
 
     world, rank, local = dist_setup()
     if world > 1:
@@ -213,17 +259,34 @@ def main():
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
 
-    g, b = graphs.make_workload(WORKLOAD)
+    g, b, dc = workload()
     k = int(b.shape[1])
+    gt = transpose_csr(g.indptr, g.indices, g.values, g.n_rows, g.n_cols)
+
+    # ---- plan options: the autotuner's choice for the forward plan ------------
     t0 = time.perf_counter()
-    plan = trspmm.Plan.from_csr(g.indptr, g.indices, g.values, g.n_rows, g.n_cols)
+    if args.no_tune:
+        opts, tune_report = {}, {"results": []}
+    else:
+        opts, tune_report = autotune.tune(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, k,
+                                          device=dev, row_scale=True, reps=5)
+    tune_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    adj = RoutedAdjacency(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, device=dev,
+                          row_scale=True, **{"promote_min": 0, **opts})
     plan_s = time.perf_counter() - t0
+    pf, pa = adj.fwd, adj.adj
+
     bd = torch.from_numpy(b).to(dev)
+    dcd = torch.from_numpy(dc).to(dev)
     cd = torch.empty((g.n_rows, k), dtype=torch.float32, device=dev)
-    ip = torch.from_numpy(g.indptr).to(dev)
-    ix = torch.from_numpy(g.indices).to(dev)
+    dbd = torch.empty((g.n_cols, k), dtype=torch.float32, device=dev)
+    dvd = torch.empty(g.nnz, dtype=torch.float32, device=dev)
+    ip, ix = adj.indptr, adj.indices
     iv = torch.from_numpy(g.values.astype(np.float16)).to(dev)
-    c2 = torch.empty_like(cd)
+    ipt, ixt = torch.from_numpy(gt[0]).to(dev), torch.from_numpy(gt[1]).to(dev)
+    ivt = torch.from_numpy(gt[2].astype(np.float16)).to(dev)
+    c2, db2, dv2 = torch.empty_like(cd), torch.empty_like(dbd), torch.empty_like(dvd)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
 
@@ -233,22 +296,30 @@ def main():
         torch.cuda.synchronize()
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(steps)]
-        for s, e in ev:
+        for s_, e_ in ev:
             flush.fill_(1.0)
-            s.record(stream)
+            s_.record(stream)
             fn()
-            e.record(stream)
+            e_.record(stream)
         torch.cuda.synchronize()
-        return [s.elapsed_time(e) for s, e in ev]
+        return [s_.elapsed_time(e_) for s_, e_ in ev]
 
-    routed = lambda: plan.spmm(bd, out=cd)
-    plain = lambda: trspmm.spmm_csr(ip, ix, iv, bd, g.n_rows, out=c2)
+    def routed_step():
+        pf.spmm(bd, out=cd)
+        pa.spmm(dcd, out=dbd)
+        trspmm.sddmm_csr(ip, ix, dcd, bd, out=dvd)
 
+    def plain_step():
+        trspmm.spmm_csr(ip, ix, iv, bd, g.n_rows, out=c2)
+        trspmm.spmm_csr(ipt, ixt, ivt, dcd, g.n_cols, out=db2)
+        trspmm.sddmm_csr(ip, ix, dcd, bd, out=dv2)
+
+    warm = max(3, args.warmup)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(torch.cuda.current_device()) as clk:
-        times = timed(routed, args.steps, max(3, args.warmup))
+        times = timed(routed_step, args.steps, warm)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -257,23 +328,47 @@ def main():
     if world > 1:
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
     ms_max = float(ms_t.item())
-    flops = 2.0 * g.nnz * k
+    flops = 3 * 2.0 * g.nnz * k
     value = flops * world / (ms_max * 1e-3) / 1e12
 
-    plain_times = timed(plain, min(args.steps, 500), 5)
-    plain_ms = float(np.mean(plain_times))
-    err_vs_plain = float((cd - c2).abs().max().item() / max(c2.abs().max().item(), 1e-30))
+    # per-pass times and the plain single-route comparison (outside the timed region)
+    n_side = min(args.steps, 100)
+    fwd_ms = float(np.mean(timed(lambda: pf.spmm(bd, out=cd), n_side, 3)))
+    adj_ms = float(np.mean(timed(lambda: pa.spmm(dcd, out=dbd), n_side, 3)))
+    sddmm_ms = float(np.mean(timed(lambda: trspmm.sddmm_csr(ip, ix, dcd, bd, out=dvd), n_side, 3)))
+    res_mask = trspmm.TR_ROUTE_ALL | trspmm.TR_ROUTE_RESIDUAL_PASS
+    res_ms = float(np.mean(timed(lambda: pf.spmm(bd, out=c2, route_mask=res_mask), n_side, 3)))
+    plain_ms = float(np.mean(timed(plain_step, n_side, 3)))
+    plain_fwd_ms = float(np.mean(timed(lambda: trspmm.spmm_csr(ip, ix, iv, bd, g.n_rows, out=c2),
+                                       n_side, 3)))
+    routed_step()
+    plain_step()
+    torch.cuda.synchronize()
+    rel = lambda a_, b_: float((a_ - b_).abs().max().item() / max(b_.abs().max().item(), 1e-30))
+    err = {"C": rel(cd, c2), "dB": rel(dbd, db2), "dval": rel(dvd, dv2)}
 
-    # end to end through the public API with host buffers
+    # ---- end to end through the public API with host buffers -------------------
     b_host = torch.from_numpy(b).pin_memory()
+    dc_host = torch.from_numpy(dc).pin_memory()
+    w_dev = torch.from_numpy(g.values.astype(np.float32)).to(dev)
     c_host = torch.empty((g.n_rows, k), dtype=torch.float32).pin_memory()
+    db_host = torch.empty((g.n_cols, k), dtype=torch.float16).pin_memory()
+    dw_host = torch.empty(g.nnz, dtype=torch.float32).pin_memory()
+    b_in = torch.empty((g.n_cols, k), dtype=torch.float16, device=dev)
+    dc_in = torch.empty((g.n_rows, k), dtype=torch.float16, device=dev)
 
     def e2e_step():
-        bd.copy_(b_host, non_blocking=True)
-        plan.spmm(bd, out=cd)
-        c_host.copy_(cd, non_blocking=True)
+        b_in.copy_(b_host, non_blocking=True)
+        dc_in.copy_(dc_host, non_blocking=True)
+        bb = b_in.detach().requires_grad_(True)
+        w = w_dev.detach().requires_grad_(True)
+        c = routed_spmm(adj, bb, w)
+        c.backward(dc_in)
+        c_host.copy_(c.detach(), non_blocking=True)
+        db_host.copy_(bb.grad, non_blocking=True)
+        dw_host.copy_(w.grad, non_blocking=True)
 
-    e2e_steps = max(3, min(args.steps, 50))
+    e2e_steps = max(3, min(args.steps, 30))
     for _ in range(3):
         e2e_step()
     torch.cuda.synchronize()
@@ -290,34 +385,57 @@ def main():
     e2e_val = flops * world / (float(e2e_t.item()) * 1e-3) / 1e12
 
     peak, peak_kind = _peaks()
-    abytes = algorithmic_bytes(g.nnz, g.n_rows, g.n_cols, k, 4)
-    achieved = abytes / (ms * 1e-3) / 1e9
+    res_nnz = int(pf.info["residual_nnz"])
+    abytes = algorithmic_bytes(res_nnz, g.n_rows, g.n_cols, k, 4)
+    achieved = abytes / (res_ms * 1e-3) / 1e9
+    sbytes = step_bytes(g.nnz, g.n_rows, g.n_cols, k)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(g, b)
+        cs = CpuStep(g, gt, b, dc)
+        sec, reps = cs.time(budget_s=12.0)
+        cpu = {"value": flops / sec / 1e12, "unit": UNIT, "cores": cs.threads, "kind": "port",
+               "sample": f"full workload, the whole step (forward, adjoint, SDDMM), "
+                         f"{reps} steps in {sec * reps:.1f} s"}
     clocks = clk.summary()
+
+    def launches(p):
+        info = p.info
+        tiles = info["tc_tiles"] + info["sptc_tiles"] + info["promoted_tiles"] > 0
+        return (1 if (info["residual_nnz"] > 0 or not tiles) else 0) + (1 if tiles else 0)
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms_max,
+            "steps": args.steps, "warmup": warm, "ms_per_step": ms_max,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16",
             "data": "synthetic",
             "config": {"workload": WORKLOAD, "n_nodes": g.n_rows, "nnz": g.nnz, "k": k,
-                       "out": "f32", "l2": "flushed between steps (256 MiB write)",
-                       "parallelism": f"replicas{world}", "plan": "exact routing, built once"},
+                       "step": "forward + adjoint + SDDMM", "out": "f32",
+                       "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": f"replicas{world}", "plan_options": opts},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": _profile_traffic(),
-                         "peak_kind": peak_kind, "algorithmic_bytes": abytes},
+                         "peak_kind": peak_kind, "algorithmic_bytes": abytes,
+                         "kernel": "csr_block_kernel (forward residual pass)"},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(b.nbytes),
-                    "d2h_bytes_per_step": int(g.n_rows * k * 4)},
-            "gpu_launches": args.steps,
+            "e2e": {"value": e2e_val, "unit": UNIT,
+                    "h2d_bytes_per_step": int(b.nbytes + dc.nbytes),
+                    "d2h_bytes_per_step": int(g.n_rows * k * 4 + g.n_cols * k * 2 + g.nnz * 4)},
+            "gpu_launches": args.steps * (launches(pf) + launches(pa) + 1),
             "clocks": clocks,
-            "extra": {"plain_csr_ms": plain_ms,
-                      "plain_csr_tflops": flops / (plain_ms * 1e-3) / 1e12,
-                      "routed_vs_plain_csr": plain_ms / ms,
-                      "routed_vs_plain_max_rel_diff": err_vs_plain,
-                      "plan_build_s": plan_s, "plan": plan.info,
+            "extra": {"forward_ms": fwd_ms, "adjoint_ms": adj_ms, "sddmm_ms": sddmm_ms,
+                      "forward_residual_pass_ms": res_ms,
+                      "plain_csr_step_ms": plain_ms, "plain_csr_forward_ms": plain_fwd_ms,
+                      "routed_vs_plain_step": plain_ms / ms,
+                      "routed_vs_plain_forward": plain_fwd_ms / fwd_ms,
+                      "max_rel_diff_vs_plain": err,
+                      "step_algorithmic_bytes": sbytes,
+                      "step_hbm_gbs": sbytes / (ms * 1e-3) / 1e9,
+                      "step_hbm_frac": sbytes / (ms * 1e-3) / 1e9 / peak,
+                      "plan_build_s": plan_s, "tune_s": tune_s,
+                      "autotune": [{"options": r["options"], "ms": r["ms"]}
+                                   for r in tune_report.get("results", [])],
+                      "plan_forward": pf.info, "plan_adjoint": pa.info,
                       "e2e_ms_per_step": float(e2e_t.item())},
         }
         print(json.dumps(line), flush=True)

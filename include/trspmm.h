@@ -36,14 +36,18 @@ enum {
 
 enum { TR_OUT_F32 = 0, TR_OUT_F16 = 1 };
 
-/* Route-mask bits for tr_spmm_routed (all set = full product).  By default
- * the one-CTA-per-window fused kernel runs (TR_ROUTE_PER_WINDOW names it
- * explicitly).  TR_ROUTE_PIPELINED added to TR_ROUTE_ALL selects the
- * persistent warp-specialised kernel (TMA gathers, double-buffered TMEM
- * accumulators) where it applies: K % 64 == 0, K <= 256, at most 512 windows
- * per SM; elsewhere the fused kernel runs. */
+/* Route-mask bits for tr_spmm_routed (all set = full product).
+ * The full product (K % 8 == 0) runs the CUDA-core residual as one kernel
+ * over every window, then adds the tensor-core tiles (the persistent
+ * pipelined kernel where K % 64 == 0, K <= 256 and at most 512 windows per
+ * SM, else the per-window kernel in accumulate mode).  A partial mask, or
+ * TR_ROUTE_PER_WINDOW, runs the single fused one-CTA-per-window kernel (per-
+ * route timing).  TR_ROUTE_PIPELINED with TR_ROUTE_ALL runs the single
+ * pipelined kernel (residual added in its epilogue).  TR_ROUTE_RESIDUAL_PASS
+ * with TR_ROUTE_ALL runs only the first launch of the full product (C = the
+ * residual part), for timing and profiling that kernel alone. */
 enum { TR_ROUTE_TC = 1, TR_ROUTE_SPTC = 2, TR_ROUTE_CUDA = 4, TR_ROUTE_ALL = 7,
-       TR_ROUTE_PER_WINDOW = 8, TR_ROUTE_PIPELINED = 16 };
+       TR_ROUTE_PER_WINDOW = 8, TR_ROUTE_PIPELINED = 16, TR_ROUTE_RESIDUAL_PASS = 32 };
 
 const char* tr_last_error(void);
 int tr_version(void);

@@ -20,8 +20,8 @@ Contents
 """
 from .core import (TABLE_NAMES, route, ref_route, ref_available, decode_tables,
                    decode_sptc_tiles, decode_plan, plan_value_of_entries, spmm_f64,
-                   spmm_f16_f32, sddmm_f64, max_threads, lib_path)
+                   spmm_f16_f32, sddmm_f64, sddmm_f16_f32, max_threads, lib_path)
 
 __all__ = ["TABLE_NAMES", "route", "ref_route", "ref_available", "decode_tables",
-           "decode_sptc_tiles", "decode_plan", "plan_value_of_entries", "spmm_f64", "spmm_f16_f32", "sddmm_f64", "max_threads",
+           "decode_sptc_tiles", "decode_plan", "plan_value_of_entries", "spmm_f64", "spmm_f16_f32", "sddmm_f64", "sddmm_f16_f32", "max_threads",
            "lib_path"]

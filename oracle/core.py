@@ -50,6 +50,7 @@ def _load():
         L.oracle_spmm_f64.argtypes = [P, P, P, ctypes.c_int, P, ctypes.c_int, P]
         L.oracle_spmm_f16_f32.argtypes = [P, P, P, ctypes.c_int, P, ctypes.c_int, P, ctypes.c_int]
         L.oracle_sddmm_f64.argtypes = [P, P, ctypes.c_int, P, P, ctypes.c_int, P]
+        L.oracle_sddmm_f16_f32.argtypes = [P, P, ctypes.c_int, P, P, ctypes.c_int, P, ctypes.c_int]
         L.oracle_max_threads.restype = ctypes.c_int
         _lib = L
     return _lib
@@ -346,6 +347,19 @@ def spmm_f16_f32(indptr, indices, values_f16, b_f16, threads=0, out=None):
     c = out if out is not None else np.empty((m, k), dtype=np.float32)
     L.oracle_spmm_f16_f32(_ptr(rp), _ptr(ci), _ptr(vv), m, _ptr(bb), k, _ptr(c), int(threads))
     return c
+
+
+def sddmm_f16_f32(indptr, indices, dc_f16, b_f16, threads=0, out=None):
+    """dval[e] = <dC[row(e)], B[col(e)]> with FP16 operands, FP32 sums (OpenMP)."""
+    L = _load()
+    rp = np.ascontiguousarray(indptr, dtype=np.int32)
+    ci = np.ascontiguousarray(indices, dtype=np.int32)
+    g = np.ascontiguousarray(dc_f16, dtype=np.float16)
+    bb = np.ascontiguousarray(b_f16, dtype=np.float16)
+    o = out if out is not None else np.empty(ci.shape[0], dtype=np.float32)
+    L.oracle_sddmm_f16_f32(_ptr(rp), _ptr(ci), rp.shape[0] - 1, _ptr(g), _ptr(bb), g.shape[1],
+                           _ptr(o), int(threads))
+    return o
 
 
 def sddmm_f64(indptr, indices, dc, b):

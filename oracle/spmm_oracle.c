@@ -11,7 +11,9 @@
  *     the same arithmetic as the GPU path, multi-threaded, timed as the CPU
  *     baseline of bench.py.
  * Plus the adjoint pieces used by the gradient checks:
- *   - oracle_sddmm_f64:    dval[e] = <dC[row(e),:], B[col(e),:]>.
+ *   - oracle_sddmm_f64:    dval[e] = <dC[row(e),:], B[col(e),:]>;
+ *   - oracle_sddmm_f16_f32: the same with FP16 operands and FP32 sums, the
+ *     arithmetic of the GPU SDDMM (timed in bench.py's CPU baseline).
  */
 #include <stdint.h>
 #include <string.h>
@@ -69,6 +71,21 @@ void oracle_sddmm_f64(const int* rowptr, const int* col, int m, const double* dc
       const double* br = b + (int64_t)col[e] * k;
       double s = 0.0;
       for (int j = 0; j < k; ++j) s += g[j] * br[j];
+      dval[e] = s;
+    }
+  }
+}
+
+void oracle_sddmm_f16_f32(const int* rowptr, const int* col, int m, const uint16_t* dc,
+                          const uint16_t* b, int k, float* dval, int threads) {
+  if (threads > 0) omp_set_num_threads(threads);
+  #pragma omp parallel for schedule(dynamic, 64)
+  for (int r = 0; r < m; ++r) {
+    const uint16_t* g = dc + (int64_t)r * k;
+    for (int e = rowptr[r]; e < rowptr[r + 1]; ++e) {
+      const uint16_t* br = b + (int64_t)col[e] * k;
+      float s = 0.f;
+      for (int j = 0; j < k; ++j) s += h2f(g[j]) * h2f(br[j]);
       dval[e] = s;
     }
   }

@@ -275,7 +275,8 @@ int tr_spmm_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int 
   if (c_dtype != TR_OUT_F32 && c_dtype != TR_OUT_F16) return fail(TR_ERR_ARG, "bad output dtype");
   if (p->view.n_rows > 0 && k > 0 && (!b || !c)) return fail(TR_ERR_ARG, "null device pointer");
   return launch_routed(p, b, k, c, c_dtype,
-                       route_mask & (TR_ROUTE_ALL | TR_ROUTE_PER_WINDOW | TR_ROUTE_PIPELINED),
+                       route_mask & (TR_ROUTE_ALL | TR_ROUTE_PER_WINDOW | TR_ROUTE_PIPELINED |
+                                     TR_ROUTE_RESIDUAL_PASS),
                        (cudaStream_t)stream);
 }
 

@@ -552,6 +552,72 @@ __global__ void __launch_bounds__(256) sddmm_kernel(const int32_t* __restrict__ 
   }
 }
 
+// K = 8 * L with L in {8, 16, 32}: groups of L lanes, one row per group, the
+// lane's 16-byte chunk of the row of x held in a register.  A group takes
+// the row's entries U at a time: every lane loads its chunk of the U rows of
+// y (coalesced: the group reads whole rows), forms U partial dot products,
+// and the group finishes them with a reduce-scatter over its lanes (each
+// step halves the values a lane holds and the lanes that share them), after
+// which lane i holds entry i's sum: L - 1 shuffles per U entries instead of
+// log2(L) per entry, and U loads in flight per lane.  Groups of one warp
+// step through their rows' batches together (warp-uniform trip count, idle
+// groups predicated), so every shuffle sees the whole warp.
+template <int L>
+__global__ void __launch_bounds__(256) sddmm_group_kernel(const int32_t* __restrict__ indptr,
+                                                          const int32_t* __restrict__ indices,
+                                                          int M, const __half* __restrict__ X,
+                                                          const __half* __restrict__ Y,
+                                                          float* __restrict__ out) {
+  constexpr int K = L * 8, G = 32 / L, U = L > 16 ? 16 : L;
+  const int lane = threadIdx.x & 31, grp = lane / L, li = lane % L;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  const int warp_id = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  for (int rb = warp_id * G; rb < M; rb += warps * G) {
+    const int r = rb + grp;
+    const bool has_row = r < M;
+    const int e0 = has_row ? __ldg(indptr + r) : 0, e1 = has_row ? __ldg(indptr + r + 1) : 0;
+    const uint4 xv = has_row ? __ldg(reinterpret_cast<const uint4*>(X + (int64_t)r * K) + li)
+                             : make_uint4(0, 0, 0, 0);
+    int nb = (e1 - e0 + U - 1) / U;
+#pragma unroll
+    for (int off = L; off < 32; off <<= 1) nb = max(nb, __shfl_xor_sync(0xffffffffu, nb, off));
+    for (int bi = 0; bi < nb; ++bi) {
+      const int eb = e0 + bi * U;
+      // the batch's column ids: one coalesced load (lane li < U takes entry
+      // eb + li), then broadcast; every row load is issued before any use,
+      // slots past the row's end reading row 0 and being dropped
+      const int my_c = (li < U && eb + li < e1) ? __ldg(indices + eb + li) : 0;
+      uint4 yv[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int c = __shfl_sync(0xffffffffu, my_c, grp * L + u);
+        yv[u] = __ldg(reinterpret_cast<const uint4*>(Y + (int64_t)c * K) + li);
+      }
+      float v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) v[u] = eb + u < e1 ? dot8h(xv, yv[u]) : 0.f;
+      if (L > U) {                                // K = 256: first fold the two half-groups
+#pragma unroll
+        for (int u = 0; u < U; ++u) v[u] += __shfl_xor_sync(0xffffffffu, v[u], 16);
+      }
+      // reduce-scatter over U lanes (lane bits li % U): value index bits follow lane bits
+#pragma unroll
+      for (int c = U; c > 1; c >>= 1) {
+        const int m = c >> 1;
+        const bool upper = (li & m) != 0;
+#pragma unroll
+        for (int i = 0; i < m; ++i) {
+          const float send = upper ? v[i] : v[i + m];
+          const float keep = upper ? v[i + m] : v[i];
+          v[i] = keep + __shfl_xor_sync(0xffffffffu, send, m);
+        }
+      }
+      const int e = eb + (li % U);
+      if (li < U && e < e1) out[e] = v[0];
+    }
+  }
+}
+
 // Any K: one thread per entry.
 __global__ void sddmm_generic_kernel(const int32_t* __restrict__ indptr,
                                      const int32_t* __restrict__ indices, int M,
@@ -643,8 +709,11 @@ int launch_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c
   const __half* bh = reinterpret_cast<const __half*>(b);
   const bool f16 = c_dtype == TR_OUT_F16;
   const int sel = route_mask & (TR_ROUTE_PER_WINDOW | TR_ROUTE_PIPELINED);
+  const bool residual_pass = (route_mask & TR_ROUTE_RESIDUAL_PASS) != 0;
   route_mask &= TR_ROUTE_ALL;
   const bool vec = k % 8 == 0 && aligned16(b);
+  if (residual_pass && route_mask == TR_ROUTE_ALL && vec)
+    return launch_residual(v, bh, k, c, f16, stream);
   const bool pipe_ok = pipe_supported(k, b) && pipe_fits(p);
   if (route_mask == TR_ROUTE_ALL && vec && sel == 0) {
     const bool tiles = p->info.tc_tiles + p->info.sptc_tiles + p->info.promoted_tiles > 0;
@@ -694,7 +763,13 @@ int launch_sddmm(const int32_t* indptr, const int32_t* indices, int32_t m, int64
     TRS_CUDA(cudaMemsetAsync(out, 0, (size_t)nnz * 4, stream));
     return TR_OK;
   }
-  if (k % 8 == 0 && aligned16(x) && aligned16(y)) {
+  const bool vec = k % 8 == 0 && aligned16(x) && aligned16(y);
+  if (vec && (k == 64 || k == 128 || k == 256)) {
+    const int blocks = (int)std::min<int64_t>(((int64_t)m + 7) / 8, 148 * 16);
+    if (k == 64) sddmm_group_kernel<8><<<blocks, 256, 0, stream>>>(indptr, indices, m, xh, yh, out);
+    else if (k == 128) sddmm_group_kernel<16><<<blocks, 256, 0, stream>>>(indptr, indices, m, xh, yh, out);
+    else sddmm_group_kernel<32><<<blocks, 256, 0, stream>>>(indptr, indices, m, xh, yh, out);
+  } else if (vec) {
     const int blocks = (int)std::min<int64_t>(((int64_t)m + 7) / 8, 148 * 16);
     sddmm_kernel<<<blocks, 256, 0, stream>>>(indptr, indices, m, xh, yh, k, out);
   } else {

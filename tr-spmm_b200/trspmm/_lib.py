@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libtrspmm.so")
 TR_OK, TR_ERR_ARG, TR_ERR_CUDA, TR_ERR_TIMEOUT, TR_ERR_NOMEM, TR_ERR_UNSUPPORTED = range(6)
 TR_OUT_F32, TR_OUT_F16 = 0, 1
 TR_ROUTE_TC, TR_ROUTE_SPTC, TR_ROUTE_CUDA, TR_ROUTE_ALL = 1, 2, 4, 7
-TR_ROUTE_PER_WINDOW, TR_ROUTE_PIPELINED = 8, 16
+TR_ROUTE_PER_WINDOW, TR_ROUTE_PIPELINED, TR_ROUTE_RESIDUAL_PASS = 8, 16, 32
 TR_ROUTE_COMPAT, TR_ROUTE_EXACT = 0, 1
 
 # Every symbol declared in include/trspmm.h.
