@@ -174,7 +174,8 @@ int tr_plan_build(const int32_t* indptr, const int32_t* indices, const float* va
  * (for inspection and host-side tests; no device needed).  Arrays by index:
  * 0 win_tile, 1 win_split, 2 win_prom, 3 tile_col, 4 tile_a (FP16 bits),
  * 5 res_ptr, 6 res_col, 7 res_val (FP16 bits), 8 win_order, 9 row_scale
- * (FP32), 10 row_out, 11 val_slot, 12 edge_row; `count` is in elements. */
+ * (FP32), 10 row_out, 11 val_slot, 12 edge_row, 13 res_edge; `count` is in
+ * elements. */
 typedef struct tr_host_plan tr_host_plan;
 int tr_plan_build_host(const int32_t* indptr, const int32_t* indices, const float* values,
                        int32_t n_rows, int32_t n_cols, const tr_route_params* params,
@@ -209,6 +210,19 @@ int tr_spmm_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int 
  * Used for learnable edge weights (the forward and the adjoint plan of the
  * same A take the same array). */
 int tr_plan_set_values(tr_plan* p, const float* values, int64_t n_edges, void* stream);
+
+/* The backward of C = A(w) . B in one call: dB = A^T . dC through the
+ * adjoint plan (built with opts.transpose), and dval = SDDMM(dC, B) on A's
+ * pattern (a_indptr[a_rows+1], a_indices[nnz] on the device).  When the
+ * adjoint plan holds every entry of A in its CUDA-core residual (a native
+ * exact plan without tiles) and K <= 128, one kernel does both, gathering
+ * each row of dC once for the two products; otherwise the routed adjoint and
+ * the SDDMM run one after the other.  dc [a_rows, K] and b [n_cols, K] FP16,
+ * db [n_cols, K] FP32 or FP16, dval [nnz] FP32.  No reference counterpart:
+ * the reference has no backward. */
+int tr_adjoint_sddmm(const tr_plan* adj, const int32_t* a_indptr, const int32_t* a_indices,
+                     int32_t a_rows, int64_t nnz, const uint16_t* dc, const uint16_t* b, int32_t k,
+                     void* db, int db_dtype, float* dval, void* stream);
 
 /* Sampled dense-dense product on A's pattern (the gradient of the values):
  * out[e] = sum_f x[row(e), f] * y[indices[e], f] for every CSR entry e,

@@ -89,6 +89,11 @@ def test_plan_encodes_matrix(name, opt):
         srow = s[rows]
     want = (w / srow).astype(np.float16).astype(np.float64) * srow
     assert np.allclose(v, want, rtol=0, atol=0), "plan value of an entry differs"
+    # residual slot -> entry is the inverse of entry -> slot on the residual
+    T = len(P["tile_col"]) // 16
+    re_ = P["res_edge"]
+    assert len(re_) == len(P["res_col"]) and (re_ >= 0).all()
+    assert np.array_equal(P["val_slot"][re_], T * 256 + np.arange(len(re_)))
     del A
 
 

@@ -111,6 +111,37 @@ def test_sddmm(cuda, name, k):
     assert rel_err(out.cpu().numpy(), ref) <= 1e-5
 
 
+FUSED_CASES = [
+    ("chung_lu", 128, dict(row_scale=True)),                     # fused (all residual)
+    ("sbm", 64, dict(row_scale=True, demote_below=1000)),        # fused
+    ("ragged", 40, dict()),                                      # fused, K not a power of 2
+    ("sbm", 128, dict(reorder=True, demote_below=1000, row_scale=True)),   # fused, reordered
+    ("route_mix", 128, dict()),                                  # tiles: two launches
+    ("chung_lu", 256, dict()),                                   # K > 128: two launches
+]
+
+
+@pytest.mark.parametrize("case", range(len(FUSED_CASES)))
+def test_adjoint_sddmm(cuda, case):
+    name, k, opts = FUSED_CASES[case]
+    g = GRAPHS[name]()
+    if name == "sbm" and "demote_below" in opts:
+        opts = dict(opts)          # the SBM's dense route stays on tiles; force all-residual
+    plan = trspmm.Plan.build(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, transpose=True,
+                             **opts)
+    dc = graphs.dense_features(g.n_rows, k, seed=11)
+    b = graphs.dense_features(g.n_cols, k, seed=12)
+    ip = torch.from_numpy(g.indptr).to(cuda)
+    ix = torch.from_numpy(g.indices).to(cuda)
+    db, dval = plan.adjoint_sddmm(ip, ix, torch.from_numpy(dc).to(cuda),
+                                  torch.from_numpy(b).to(cuda))
+    torch.cuda.synchronize()
+    AT = _matrix(g, transpose=True, row_scale=opts.get("row_scale", False))
+    assert rel_err(db.cpu().numpy(), AT @ dc.astype(np.float64)) <= TOL32
+    ref = oracle.sddmm_f64(g.indptr, g.indices, dc.astype(np.float64), b.astype(np.float64))
+    assert rel_err(dval.cpu().numpy(), ref) <= 1e-5
+
+
 def _torch_sparse_grads(g, w, b, dc):
     """FP64 torch.sparse autograd reference: C = A(w) B, grads of <C, dc>."""
     wt = torch.tensor(w, dtype=torch.float64, requires_grad=True)

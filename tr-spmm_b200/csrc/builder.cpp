@@ -259,6 +259,8 @@ int build_plan(const int32_t* indptr, const int32_t* indices, const float* value
   }
   hp.val_slot.swap(slot);
   hp.edge_row.swap(erow);
+  for (int32_t& e : hp.res_edge)
+    if (e >= 0) e = a.src[e];
   if (opts.reorder)
     for (size_t r = 0; r < perm.size(); ++r) hp.row_out[r] = perm[r];
   hp.reordered = opts.reorder != 0;

@@ -234,6 +234,7 @@ int tr_host_plan_array(const tr_host_plan* h, int idx, const void** data, int64_
     TRS_A(0, win_tile) TRS_A(1, win_split) TRS_A(2, win_prom) TRS_A(3, tile_col)
     TRS_A(4, tile_a) TRS_A(5, res_ptr) TRS_A(6, res_col) TRS_A(7, res_val) TRS_A(8, win_order)
     TRS_A(9, row_scale) TRS_A(10, row_out) TRS_A(11, val_slot) TRS_A(12, edge_row)
+    TRS_A(13, res_edge)
     default: return fail(TR_ERR_ARG, "plan array index out of range");
   }
 #undef TRS_A
@@ -287,6 +288,19 @@ int tr_plan_set_values(tr_plan* p, const float* values, int64_t n_edges, void* s
                                 std::to_string(p->n_edges));
   if (n_edges > 0 && !values) return fail(TR_ERR_ARG, "null device pointer");
   return launch_set_values(p, values, (cudaStream_t)stream);
+}
+
+int tr_adjoint_sddmm(const tr_plan* adj, const int32_t* a_indptr, const int32_t* a_indices,
+                     int32_t a_rows, int64_t nnz, const uint16_t* dc, const uint16_t* b, int32_t k,
+                     void* db, int db_dtype, float* dval, void* stream) {
+  if (!adj) return fail(TR_ERR_ARG, "null plan");
+  if (a_rows < 0 || nnz < 0 || k < 0) return fail(TR_ERR_ARG, "negative size");
+  if (db_dtype != TR_OUT_F32 && db_dtype != TR_OUT_F16) return fail(TR_ERR_ARG, "bad output dtype");
+  if (a_rows != adj->view.n_cols) return fail(TR_ERR_ARG, "a_rows must equal the adjoint plan's column count");
+  if (k > 0 && (!dc || !b || !db || (nnz > 0 && (!a_indptr || !a_indices || !dval))))
+    return fail(TR_ERR_ARG, "null device pointer");
+  return launch_adjoint_sddmm(adj, a_indptr, a_indices, a_rows, nnz, dc, b, k, db, db_dtype, dval,
+                              (cudaStream_t)stream);
 }
 
 int tr_sddmm_csr(const int32_t* indptr, const int32_t* indices, int32_t m, int32_t n_cols,

@@ -226,12 +226,14 @@ void flatten(HostPlan& hp, Staging& st, const PlanOptions& opt, int64_t n_edges)
   for (int64_t i = 0; i < rows; ++i) hp.res_ptr[i + 1] += hp.res_ptr[i];
   hp.res_col.resize(hp.res_ptr[rows]);
   hp.res_val.resize(hp.res_ptr[rows]);
+  hp.res_edge.assign(hp.res_ptr[rows], -1);
   std::vector<int32_t> fill(hp.res_ptr.begin(), hp.res_ptr.end() - 1);
   for (auto& e : st.res) {
     const int32_t at = fill[e.row]++;
     hp.res_col[at] = e.col;
     hp.res_val[at] = f2h(e.val / hp.row_scale[e.row]);
     if (e.edge >= 0 && e.edge < n_edges) {
+      hp.res_edge[at] = e.edge;
       hp.val_slot[e.edge] = (int32_t)(T * 256 + at);
       hp.edge_row[e.edge] = e.row;
     }
@@ -527,6 +529,7 @@ int plan_upload(const HostPlan& hp, tr_plan** out) {
       {hp.row_out.data(), rows * 4, 0},
       {hp.val_slot.data(), n_edges * 4, 0},
       {hp.edge_row.data(), n_edges * 4, 0},
+      {hp.res_edge.data(), (int64_t)hp.res_edge.size() * 4, 0},
       {nullptr, 0, 256},                       // error words
   };
   constexpr int kSecs = sizeof(secs) / sizeof(secs[0]);
@@ -567,7 +570,8 @@ int plan_upload(const HostPlan& hp, tr_plan** out) {
   v.win_order = (const int32_t*)at[8];
   v.row_scale = (const float*)at[9];
   v.row_out = (const int32_t*)at[10];
-  v.err = (int*)at[13];
+  v.res_edge = (const int32_t*)at[13];
+  v.err = (int*)at[14];
   p->tile_a = (uint16_t*)at[4];
   p->res_val = (uint16_t*)at[7];
   p->row_scale = (float*)at[9];

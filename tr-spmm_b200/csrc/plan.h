@@ -13,6 +13,8 @@
 //                    element (n, k) at (n/8)*128 + (k/8)*64 + (n%8)*8 + k%8
 //   res_ptr[W*16+1]  CUDA-core residual as CSR over the padded rows
 //   res_col[R], res_val[R] (FP16)
+//   res_edge[R]      CSR entry of the source matrix behind each residual
+//                    entry (-1: unknown), for the fused adjoint + SDDMM
 //   win_order[W]     windows in decreasing cost order (launch order)
 //   row_scale[W*16]  FP32 factor re-applied to each plan row in the epilogue
 //                    (values are stored as FP16(v / row_scale))
@@ -42,6 +44,7 @@ struct PlanView {
   const int32_t* res_ptr;
   const int32_t* res_col;
   const uint16_t* res_val;
+  const int32_t* res_edge;
   const int32_t* win_order;
   const float* row_scale;
   const int32_t* row_out;
@@ -54,6 +57,7 @@ struct HostPlan {
   std::vector<uint16_t> tile_a;
   std::vector<int32_t> res_ptr, res_col;
   std::vector<uint16_t> res_val;
+  std::vector<int32_t> res_edge;
   std::vector<int32_t> win_order;
   std::vector<float> row_scale;
   std::vector<int32_t> row_out;

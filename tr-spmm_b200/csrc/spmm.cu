@@ -618,6 +618,147 @@ __global__ void __launch_bounds__(256) sddmm_group_kernel(const int32_t* __restr
   }
 }
 
+// ---------------------------------------------------------------------------
+// Fused adjoint + SDDMM (the backward of C = A(w) . B)
+// ---------------------------------------------------------------------------
+// One CTA per 16 rows of the adjoint plan (rows of A^T, i.e. rows of B),
+// K <= 128.  For every residual entry (row j of A^T, column i, value a, A's
+// entry e) a lane group gathers 16-byte chunks of dC[i] once and uses them
+// twice: dB[j] += a * dC[i] (the CUDA-core engine's row-run accumulation)
+// and dval[e] = <dC[i], B[j]> (a dot product with row j of B, held in
+// registers for the run, reduced over the group with shuffles).  The
+// separate SDDMM would gather every dC row a second time.
+constexpr int kUnrollSD = 8;        // entries per lane group and batch in the fused pass
+
+// Sums 8 per-lane values over a group of L lanes (L = 8 or 16) so that lane
+// (li & 7) ends up with the total of value (li & 7): for L = 16 the two
+// halves are folded first, then each reduce-scatter step halves the values a
+// lane keeps (15 shuffles for 8 sums instead of 8 * log2(L)).
+template <int L>
+__device__ __forceinline__ float group_reduce_scatter8(float (&d)[8], int li) {
+  if (L == 16) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) d[u] += __shfl_xor_sync(0xffffffffu, d[u], 8);
+  }
+#pragma unroll
+  for (int c = 8; c > 1; c >>= 1) {
+    const int m = c >> 1;
+    const bool upper = (li & m) != 0;
+#pragma unroll
+    for (int i = 0; i < m; ++i) {
+      const float send = upper ? d[i] : d[i + m];
+      const float keep = upper ? d[i + m] : d[i];
+      d[i] = keep + __shfl_xor_sync(0xffffffffu, send, m);
+    }
+  }
+  return d[0];
+}
+
+template <int L>
+__device__ __forceinline__ void adjoint_sddmm_chunk(const int* rp, int e0, int n, const int4* sent,
+                                                    const int* s_out, const __half* __restrict__ G,
+                                                    const __half* __restrict__ H, int K,
+                                                    float* racc, float* __restrict__ dval) {
+  constexpr int Gn = 32 / L;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int g = lane / L, li = lane % L;
+  const bool active = li * 8 < K;
+  const int per = (n + kWarps - 1) / kWarps;
+  const int eb = warp * per;
+  const int ee = min(n, eb + per);
+  if (eb >= ee) return;
+  const __half* Gf = G + (active ? li * 8 : 0);
+  int row = 0;
+  while (rp[row + 1] - e0 <= eb) ++row;            // warp-uniform
+  const int c_safe = sent[eb].x;
+  for (int i = eb; i < ee;) {
+    const int rend = min(ee, rp[row + 1] - e0);
+    const int orow = s_out[row];
+    const uint4 hv = (active && orow >= 0)
+                         ? __ldg(reinterpret_cast<const uint4*>(H + (int64_t)orow * K + li * 8))
+                         : make_uint4(0, 0, 0, 0);
+    float acc[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc[q] = 0.f;
+    // warp-uniform trip count (the dot products are reduced with full-warp
+    // shuffles inside the loop); entries past the run are predicated off
+    for (int jb = i; jb < rend; jb += Gn * kUnrollSD) {
+      const int j0 = jb + g;
+      uint4 bv[kUnrollSD];
+#pragma unroll
+      for (int u = 0; u < kUnrollSD; ++u) {       // all gathers first
+        const int j = j0 + u * Gn;
+        const int c = j < rend ? sent[j].x : c_safe;
+        bv[u] = __ldg(reinterpret_cast<const uint4*>(Gf + (size_t)c * K));
+      }
+      float d[kUnrollSD];
+      int my_ed = -1;
+#pragma unroll
+      for (int u = 0; u < kUnrollSD; ++u) {       // values and entry ids re-read from shared
+        const int j = j0 + u * Gn;
+        const int4 en = j < rend ? sent[j] : make_int4(0, 0, -1, 0);
+        fma8h(acc, (uint16_t)en.y, bv[u]);
+        d[u] = active ? dot8h(hv, bv[u]) : 0.f;
+        if ((li & 7) == u) my_ed = en.z;
+      }
+      const float tot = group_reduce_scatter8<L>(d, li);
+      if (li < 8 && my_ed >= 0) dval[my_ed] = tot;
+    }
+    for (int off = L; off < 32; off <<= 1)
+#pragma unroll
+      for (int q = 0; q < 8; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+    if (g == 0 && active) {
+      float* dst = racc + row * kChunk + li * 8;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) atomicAdd(dst + q, acc[q]);
+    }
+    i = rend;
+    while (row < kBlockRows - 1 && rp[row + 1] - e0 <= i) ++row;
+  }
+}
+
+template <bool F16OUT, int L>
+__global__ void __launch_bounds__(kThreads, 3) adjoint_sddmm_kernel(
+    const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+    const __half* __restrict__ values, const int32_t* __restrict__ edges, int M,
+    const __half* __restrict__ G, int K, void* C, const int32_t* __restrict__ row_out,
+    const float* __restrict__ row_scale, const __half* __restrict__ H, float* __restrict__ dval) {
+  __shared__ __align__(16) float racc[kBlockRows * kChunk];
+  __shared__ int4 sent[kStage];
+  __shared__ int rp[kBlockRows + 1];
+  __shared__ int s_out[kBlockRows];
+  __shared__ float s_scale[kBlockRows];
+  const int r0 = blockIdx.x * kBlockRows;
+  if (threadIdx.x <= kBlockRows) rp[threadIdx.x] = indptr[min(r0 + (int)threadIdx.x, M)];
+  if (threadIdx.x < kBlockRows) {
+    s_out[threadIdx.x] = r0 + (int)threadIdx.x < M ? row_out[r0 + threadIdx.x] : -1;
+    s_scale[threadIdx.x] = r0 + (int)threadIdx.x < M ? row_scale[r0 + threadIdx.x] : 0.f;
+  }
+  for (int i = threadIdx.x; i < kBlockRows * kChunk; i += kThreads) racc[i] = 0.f;
+  __syncthreads();
+  const uint16_t* v16 = reinterpret_cast<const uint16_t*>(values);
+  const int e_begin = rp[0], e_end = rp[kBlockRows];
+  for (int c0 = e_begin; c0 < e_end; c0 += kStage) {
+    const int n = min(kStage, e_end - c0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += kThreads)
+      sent[i] = make_int4(__ldg(indices + c0 + i), (int)__ldg(v16 + c0 + i), __ldg(edges + c0 + i), 0);
+    __syncthreads();
+    adjoint_sddmm_chunk<L>(rp, c0, n, sent, s_out, G, H, K, racc, dval);
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int f = (warp & 3) * 32 + lane;
+  if (f < K) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const int r = (warp >> 2) * 8 + i;
+      if (s_out[r] >= 0)
+        store_row_feature<F16OUT>(C, K, s_out[r], f, racc[r * kChunk + f] * s_scale[r]);
+    }
+  }
+}
+
 // Any K: one thread per entry.
 __global__ void sddmm_generic_kernel(const int32_t* __restrict__ indptr,
                                      const int32_t* __restrict__ indices, int M,
@@ -776,6 +917,42 @@ int launch_sddmm(const int32_t* indptr, const int32_t* indices, int32_t m, int64
     const int blocks = (int)std::min<int64_t>(m, 148 * 32);
     sddmm_generic_kernel<<<blocks, 128, 0, stream>>>(indptr, indices, m, xh, yh, k, out);
   }
+  TRS_CUDA(cudaGetLastError());
+  return TR_OK;
+}
+
+// dB = A^T . dC through the adjoint plan and dval = SDDMM(dC, B) on A's
+// pattern.  Fused into one pass when the adjoint plan keeps every entry of A
+// in its CUDA-core residual with its entry id (native exact plans without
+// tiles), K <= 128 and K % 8 == 0; otherwise the routed adjoint and the
+// SDDMM run as two launches.
+int launch_adjoint_sddmm(const tr_plan* p, const int32_t* a_indptr, const int32_t* a_indices,
+                         int32_t a_rows, int64_t nnz, const uint16_t* dc, const uint16_t* b,
+                         int32_t k, void* db, int db_dtype, float* dval, cudaStream_t stream) {
+  const PlanView& v = p->view;
+  const bool f16 = db_dtype == TR_OUT_F16;
+  const bool tiles = p->info.tc_tiles + p->info.sptc_tiles + p->info.promoted_tiles > 0;
+  // lane groups of 8 or 16 lanes (K in (32, 128]): the reduce-scatter needs 8+ lanes
+  const bool fused = !tiles && k > 32 && k <= kChunk && k % 8 == 0 && aligned16(dc) && aligned16(b) &&
+                     p->n_edges == nnz && p->info.residual_nnz == nnz && v.n_rows > 0;
+  if (!fused) {
+    int rc = launch_routed(p, dc, k, db, db_dtype, TR_ROUTE_ALL, stream);
+    if (rc) return rc;
+    return launch_sddmm(a_indptr, a_indices, a_rows, nnz, dc, b, k, dval, stream);
+  }
+  const int rows = v.n_windows * kBlockRows;
+  const __half* g = reinterpret_cast<const __half*>(dc);
+  const __half* h = reinterpret_cast<const __half*>(b);
+  const __half* rv = reinterpret_cast<const __half*>(v.res_val);
+#define TRS_ADJ(F16, L)                                                                   \
+  adjoint_sddmm_kernel<F16, L><<<v.n_windows, kThreads, 0, stream>>>(                      \
+      v.res_ptr, v.res_col, rv, v.res_edge, rows, g, k, db, v.row_out, v.row_scale, h, dval)
+  if (k > 64) {
+    if (f16) TRS_ADJ(true, 16); else TRS_ADJ(false, 16);
+  } else {
+    if (f16) TRS_ADJ(true, 8); else TRS_ADJ(false, 8);
+  }
+#undef TRS_ADJ
   TRS_CUDA(cudaGetLastError());
   return TR_OK;
 }

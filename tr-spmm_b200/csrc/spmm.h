@@ -17,6 +17,9 @@ bool pipe_supported(int32_t k, const void* b);
 bool pipe_fits(const tr_plan* p);
 int launch_pipe(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_dtype,
                 bool accumulate, cudaStream_t stream);
+int launch_adjoint_sddmm(const tr_plan* p, const int32_t* a_indptr, const int32_t* a_indices,
+                         int32_t a_rows, int64_t nnz, const uint16_t* dc, const uint16_t* b,
+                         int32_t k, void* db, int db_dtype, float* dval, cudaStream_t stream);
 int launch_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_dtype,
                   int route_mask, cudaStream_t stream);
 

@@ -24,6 +24,7 @@ EXPORTED = [
     "tr_plan_from_tables", "tr_plan_from_csr", "tr_plan_build", "tr_plan_build_host",
     "tr_host_plan_array", "tr_host_plan_upload", "tr_host_plan_free", "tr_plan_info_get",
     "tr_plan_free", "tr_spmm_csr", "tr_spmm_routed", "tr_plan_set_values", "tr_sddmm_csr",
+    "tr_adjoint_sddmm",
     "tr_forward_fp16_tcu_cuda_sptc_mma_parallel_online", "tr_forward_fp16_sptc_online",
     "tr_forward_fp16_sptc_mma_online", "tr_forward_fp16_sptc_mma_packed_online",
 ]
@@ -101,6 +102,7 @@ def lib():
     L.tr_host_plan_free.argtypes = [P]
     L.tr_plan_set_values.argtypes = [P, P, I64, P]
     L.tr_sddmm_csr.argtypes = [P, P, I32, I32, I64, P, P, I32, P, P]
+    L.tr_adjoint_sddmm.argtypes = [P, P, P, I32, I64, P, P, I32, P, ctypes.c_int, P, P]
     L.tr_plan_info_get.argtypes = [P, ctypes.POINTER(PlanInfo)]
     L.tr_plan_free.argtypes = [P]
     L.tr_spmm_csr.argtypes = [P, P, P, I32, I32, I64, P, I32, P, ctypes.c_int, P]

@@ -7,6 +7,8 @@ two routed plans built once: A for the forward, A^T for the adjoint).
   forward    C  = A(w) . B                         (routed kernel, plan of A)
   backward   dB = A(w)^T . dC                      (routed kernel, plan of A^T)
              dw[e] = <dC[row(e)], B[col(e)]>       (SDDMM on A's pattern)
+             both in one pass over A^T when the adjoint plan allows
+             (tr_adjoint_sddmm: each gathered row of dC feeds both products)
 
 The reference has no backward at all; this is the differentiation path a GNN
 built on the reference's operator would need.  Operands are FP16 on the
@@ -84,6 +86,19 @@ class RoutedSpMMFunction(torch.autograd.Function):
             adj.set_values(w)
         dc16, sc = _to_half_scaled(dc.contiguous())
         db = dw = None
+        scale = None
+        if sc is not None:
+            scale = sc
+        if sb.numel():
+            scale = sb if scale is None else scale * sb
+        if ctx.needs_input_grad[1] and ctx.has_w and ctx.needs_input_grad[0]:
+            # both gradients: one pass over A^T gathers each row of dC once
+            db, dw = adj.adj.adjoint_sddmm(adj.indptr, adj.indices, dc16, b16)
+            if sc is not None:
+                db = db * sc
+            if scale is not None:
+                dw = dw * scale
+            return dw, db.to(ctx.b_dtype), None
         if ctx.needs_input_grad[1]:
             db = adj.adj.spmm(dc16, out_dtype=torch.float32)
             if sc is not None:
@@ -91,11 +106,6 @@ class RoutedSpMMFunction(torch.autograd.Function):
             db = db.to(ctx.b_dtype)
         if ctx.has_w and ctx.needs_input_grad[0]:
             dw = sddmm_csr(adj.indptr, adj.indices, dc16, b16)
-            scale = None
-            if sc is not None:
-                scale = sc
-            if sb.numel():
-                scale = sb if scale is None else scale * sb
             if scale is not None:
                 dw = dw * scale
         return dw, db, None

@@ -214,6 +214,34 @@ class Plan:
                                    ctypes.c_void_p(s)))
         return out
 
+    def adjoint_sddmm(self, a_indptr, a_indices, dc, b, db=None, dval=None, db_dtype=None,
+                      stream=None):
+        """For an adjoint plan (built with transpose=True): dB = A^T . dC and
+        dval = SDDMM(dC, B) on A's pattern, fused into one pass where the plan
+        allows (tr_adjoint_sddmm).  dc [A rows, K], b [A cols, K] FP16 CUDA."""
+        import torch
+        _check_b(dc, self.n_cols)
+        if not (b.is_cuda and b.dtype == torch.float16 and b.is_contiguous() and b.dim() == 2
+                and b.shape == (self.n_rows, dc.shape[1])):
+            raise RuntimeError("b must be a contiguous float16 CUDA tensor [A cols, K]")
+        k = dc.shape[1]
+        nnz = a_indices.numel()
+        if db is None:
+            db = torch.empty((self.n_rows, k), dtype=db_dtype or torch.float32, device=dc.device)
+        _check_out(db, self.n_rows, k)
+        if dval is None:
+            dval = torch.empty(nnz, dtype=torch.float32, device=dc.device)
+        if not (dval.is_cuda and dval.dtype == torch.float32 and dval.numel() == nnz):
+            raise RuntimeError("dval must be a float32 CUDA tensor with one item per entry")
+        s = stream if stream is not None else torch.cuda.current_stream(dc.device).cuda_stream
+        check(lib().tr_adjoint_sddmm(self._h, ctypes.c_void_p(a_indptr.data_ptr()),
+                                     ctypes.c_void_p(a_indices.data_ptr()), int(self.n_cols),
+                                     int(nnz), ctypes.c_void_p(dc.data_ptr()),
+                                     ctypes.c_void_p(b.data_ptr()), int(k),
+                                     ctypes.c_void_p(db.data_ptr()), _odt(db),
+                                     ctypes.c_void_p(dval.data_ptr()), ctypes.c_void_p(s)))
+        return db, dval
+
     def close(self):
         if self._h:
             lib().tr_plan_free(self._h)
@@ -272,7 +300,7 @@ HOST_PLAN_ARRAYS = [("win_tile", np.int32), ("win_split", np.int32), ("win_prom"
                     ("tile_col", np.int32), ("tile_a", np.uint16), ("res_ptr", np.int32),
                     ("res_col", np.int32), ("res_val", np.uint16), ("win_order", np.int32),
                     ("row_scale", np.float32), ("row_out", np.int32), ("val_slot", np.int32),
-                    ("edge_row", np.int32)]
+                    ("edge_row", np.int32), ("res_edge", np.int32)]
 
 
 def host_plan(indptr, indices, values, n_rows, n_cols, row_scale=False, promote_min=0,
