@@ -188,6 +188,50 @@ class CpuStep:
                 return el / reps, reps
 
 
+def batched_comparison(dev, flush, n_graphs=512, k=64, reps=20):
+    """The batched workload: 512 power-law graphs (20-500 nodes, degree
+    4-32), forward + fused backward at K=64.  One block-diagonal plan pair,
+    the step captured in a CUDA graph, vs one plan pair per graph launched in
+    a loop (eagerly from Python, and the same loop captured in a graph)."""
+    import torch
+    from trspmm import graphs
+    from trspmm.batched import BatchedStep, PerGraphLoop
+    g = graphs.batched(num_graphs=n_graphs)
+    opts = dict(demote_below=1000, promote_min=0, row_scale=True)
+    bs = BatchedStep(g, k, device=dev, **opts)
+    loop = PerGraphLoop(g, k, device=dev, **opts)
+    b = torch.from_numpy(graphs.dense_features(g.n_cols, k, seed=1)).to(dev)
+    dc = torch.from_numpy(graphs.dense_features(g.n_rows, k, seed=2)).to(dev)
+    for st in (bs, loop):
+        st.b.copy_(b)
+        st.dc.copy_(dc)
+
+    def med(fn):
+        for _ in range(3):
+            fn()
+        ts = []
+        for _ in range(reps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    loop_eager = med(loop.run)
+    bs.capture()
+    batched_graph = med(bs.replay)
+    loop.capture()
+    loop_graph = med(loop.replay)
+    return {"graphs": n_graphs, "nodes": g.n_rows, "nnz": g.nnz, "k": k,
+            "batched_graph_ms": batched_graph, "per_graph_loop_ms": loop_eager,
+            "per_graph_loop_captured_ms": loop_graph,
+            "speedup_vs_loop": loop_eager / batched_graph,
+            "speedup_vs_captured_loop": loop_graph / batched_graph}
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -242,6 +286,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner and use the reference's routing (exact mode)")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the 512-graph batched comparison reported under extra")
+    ap.add_argument("--plan-options", default=None,
+                    help="JSON plan options to use instead of the autotuner's choice "
+                         '(e.g. \'{"demote_below": 1000}\'), for profiling runs')
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -266,7 +315,9 @@ def main():
 
     # ---- plan options: the autotuner's choice for the forward plan ------------
     t0 = time.perf_counter()
-    if args.no_tune:
+    if args.plan_options is not None:
+        opts, tune_report = json.loads(args.plan_options), {"results": []}
+    elif args.no_tune:
         opts, tune_report = {}, {"results": []}
     else:
         opts, tune_report = autotune.tune(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, k,
@@ -399,6 +450,9 @@ def main():
                "sample": f"full workload, the whole step (forward, adjoint, SDDMM), "
                          f"{reps} steps in {sec * reps:.1f} s"}
     clocks = clk.summary()
+    batched = None
+    if rank == 0 and not args.no_batched:
+        batched = batched_comparison(dev, flush)
 
     def launches(p):
         info = p.info
@@ -442,6 +496,7 @@ def main():
                       "plan_build_s": plan_s, "tune_s": tune_s,
                       "autotune": [{"options": r["options"], "ms": r["ms"]}
                                    for r in tune_report.get("results", [])],
+                      "batched_512": batched,
                       "plan_forward": pf.info, "plan_adjoint": pa.info,
                       "e2e_ms_per_step": float(e2e_t.item())},
         }

@@ -3,16 +3,17 @@
 The four operators keep the reference signatures
 (TR-source/SpMM/mGCN_online.cpp:1142-1152): CPU tensors in, a freshly
 allocated FP32 CPU output plus averaged millisecond timings out.  Inside,
-each call builds a device plan from the route tables and runs the fused
-sm_100a routed kernel (libtrspmm.so) ``epoches`` times after 10 warm-ups,
-as the reference's launcher does (mGCNkernel_online.cu:1604-1674).  The
-result is C = A_tables . B in FP32 accumulation for every route; there is
-no CPU fallback.
+each call builds a device plan from the route tables and runs the routed
+product (libtrspmm.so: the CUDA-core residual pass, then the tensor-core
+tiles added into C) ``epoches`` times after 10 warm-ups, as the reference's
+launcher does (mGCNkernel_online.cu:1604-1674).  The result is
+C = A_tables . B in FP32 accumulation for every route; there is no CPU
+fallback.
 
 Per-route times of ``forward_fp16_tcu_cuda_sptc_mma_parallel_online`` come
-from the same fused kernel restricted to one route at a time (TC, CUDA, SPTC);
-the CUDA time is reported for both the long and the short CUDA parts, which
-this library processes together.
+from the one-CTA-per-window kernel restricted to one route at a time (TC,
+CUDA, SPTC); the CUDA time is reported for both the long and the short CUDA
+parts, which this library processes together.
 """
 from __future__ import annotations
 
