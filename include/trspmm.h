@@ -89,6 +89,18 @@ int tr_route_build(const int32_t* indptr, const int32_t* indices, const float* v
                    int32_t n_rows, const tr_route_params* params, tr_route** out);
 /* Table idx in the reference's return order (0..28); `count` is in elements. */
 int tr_route_table(const tr_route* r, int idx, const void** data, int64_t* count);
+/* The router's dense-TC funnel on the device (sm_100a integer kernels:
+ * bitonic sorts, warp-ballot compaction, shared atomics; one CTA per
+ * window): from a device CSR with rows sorted by column, the TC tables
+ * t_row_offset, t_block_offset, t_column, t_value, t_window_row, t_binary
+ * exactly as tr_route_build makes them in exact mode (params.window must be
+ * 16; the 2:4 and CUDA stages and t_atomic, which depends on the 2:4
+ * matching, are not produced).  Replaces the first stage of
+ * block_sptc_2to4_online (TR-source/Block/block_online.cpp:584-620, :215-253,
+ * :444-540).  Read the tables with tr_route_table (indices 0-4, 6; the
+ * others are empty). */
+int tr_route_tc_device(const int32_t* d_indptr, const int32_t* d_indices, const float* d_values,
+                       int32_t n_rows, const tr_route_params* params, tr_route** out);
 /* Seconds spent building the tables (the reference's 30th return). */
 double tr_route_seconds(const tr_route* r);
 void tr_route_free(tr_route* r);

@@ -1,6 +1,7 @@
 // extern "C" entry points of libtrspmm.so (declared in include/trspmm.h).
 #include <cuda_runtime.h>
 
+#include <chrono>
 #include <cstdio>
 #include <cstring>
 #include <memory>
@@ -10,6 +11,7 @@
 #include "../../include/trspmm.h"
 #include "common.cuh"
 #include "plan.h"
+#include "route_gpu.h"
 #include "router.h"
 #include "spmm.h"
 
@@ -181,6 +183,35 @@ int tr_route_table(const tr_route* r, int idx, const void** data, int64_t* count
     default: return fail(TR_ERR_ARG, "table index out of range");
   }
 #undef TRS_T
+}
+
+int tr_route_tc_device(const int32_t* d_indptr, const int32_t* d_indices, const float* d_values,
+                       int32_t n_rows, const tr_route_params* params, tr_route** out) {
+  if (!d_indptr || !params || !out) return fail(TR_ERR_ARG, "null argument");
+  if (n_rows < 0) return fail(TR_ERR_ARG, "negative row count");
+  if (params->window != 16) return fail(TR_ERR_UNSUPPORTED, "the device router uses 16-row windows");
+  RouteGpuParams gp;
+  gp.window = 16;
+  gp.density = params->density;
+  gp.tc_min_util = params->tc_min_util;
+  gp.partsize_t = params->partsize_t;
+  gp.skip_tc = params->skip_tc;
+  TcTables tc;
+  std::string err;
+  const auto t0 = std::chrono::high_resolution_clock::now();
+  int rc = route_tc_gpu(d_indptr, d_indices, d_values, n_rows, gp, tc, err);
+  if (rc) return err.empty() ? rc : fail(rc, err);
+  std::unique_ptr<tr_route> r(new tr_route());
+  r->t.t_row_offset = std::move(tc.t_row_offset);
+  r->t.t_block_offset = std::move(tc.t_block_offset);
+  r->t.t_column = std::move(tc.t_column);
+  r->t.t_value = std::move(tc.t_value);
+  r->t.t_window_row = std::move(tc.t_window_row);
+  r->t.t_binary = std::move(tc.t_binary);
+  r->t.t_edge = std::move(tc.t_edge);
+  r->t.seconds = std::chrono::duration<double>(std::chrono::high_resolution_clock::now() - t0).count();
+  *out = r.release();
+  return TR_OK;
 }
 
 double tr_route_seconds(const tr_route* r) { return r ? r->t.seconds : 0.0; }

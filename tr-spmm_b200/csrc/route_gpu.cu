@@ -1,0 +1,398 @@
+// Dense-TC funnel of the router as sm_100a integer kernels.
+//
+// Restates, on the device, the first stage of the reference router
+// (TR-source/Block/block_online.cpp:584-620 with select_tc_columns_online
+// :215-253 and build_tcu_part_online :444-540) in its exact form (a
+// repeated (row, column) entry keeps only its first occurrence on the
+// tensor cores, as this library's exact mode does), for rows sorted by
+// column:
+//
+//   per 16-row window: the column profile (distinct columns and the rows
+//   that use them), the candidates used by >= density rows ordered by
+//   (count desc, column asc), chunks of 8 kept when their fill
+//   >= tc_min_util, each chunk's columns sorted ascending, and the 16x8
+//   sub-blocks: bit (row*8 + k) of binary_lo (rows 0-7) / binary_hi (rows
+//   8-15), values in bit order, parts of partsize_t sub-blocks.
+//
+// One CTA per window.  The window's keys (column, entry, row) are sorted
+// with a block-wide bitonic sort; distinct columns are found with warp
+// ballots and a block prefix scan (the compaction); row masks are OR-ed per
+// distinct column with shared atomics; candidates are sorted the same way.
+// Windows of up to kSmemKeys entries work in shared memory; larger ones
+// (hub rows) run the same code on their slice of a global scratch buffer.
+// A counting launch gives sub-blocks and values per window, the host scans
+// them into offsets, a filling launch writes the tables.
+//
+// The result equals the CPU router's t_row_offset, t_block_offset,
+// t_column, t_value, t_window_row and t_binary; t_atomic is not produced
+// (the reference sets it from the 2:4 matching's outcome).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <vector>
+
+#include "../../include/trspmm.h"
+#include "common.cuh"
+#include "route_gpu.h"
+
+namespace trs {
+namespace {
+
+constexpr int kRThreads = 256;
+constexpr int kSmemKeys = 2048;          // entries of a window handled in shared memory
+
+__host__ __device__ inline uint32_t next_pow2(uint32_t n) {
+  uint32_t p = 1;
+  while (p < n) p <<= 1;
+  return p;
+}
+
+// Per-window working storage for up to `cap` entries (cap a power of two).
+struct WinWork {
+  uint64_t* keys;      // (column << 32) | (entry << 4) | row; padding = ~0
+  uint64_t* cand;      // (16 - count) << 32 | distinct-column index
+  uint64_t* glo;       // per sub-block bitmaps (rows 0-7 / 8-15)
+  uint64_t* ghi;
+  int* pos;            // per key: distinct-column index
+  int* tmp;            // scan output / per-sub-block value starts
+  int* ucol;           // distinct columns, ascending
+  uint32_t* umask;     // their row masks
+  int* slot;           // per distinct column: tc slot (group*8 + k) or -1
+  int* gcol;           // per sub-block, its 8 columns (-1 padded)
+  uint8_t* flags;
+};
+
+__host__ __device__ inline int64_t storage_bytes(uint32_t cap) {
+  const int64_t groups = cap / 8 + 1;
+  return (int64_t)cap * 8 * 2 + groups * 8 * 2 + (int64_t)cap * 4 * 5 + (groups * 8) * 4 +
+         (int64_t)cap;
+}
+
+__device__ void bind_storage(WinWork& w, uint8_t* base, uint32_t cap) {
+  const uint32_t groups = cap / 8 + 1;
+  w.keys = reinterpret_cast<uint64_t*>(base);
+  w.cand = w.keys + cap;
+  w.glo = w.cand + cap;
+  w.ghi = w.glo + groups;
+  w.pos = reinterpret_cast<int*>(w.ghi + groups);
+  w.tmp = w.pos + cap;
+  w.ucol = w.tmp + cap;
+  w.umask = reinterpret_cast<uint32_t*>(w.ucol + cap);
+  w.slot = reinterpret_cast<int*>(w.umask + cap);
+  w.gcol = w.slot + cap;
+  w.flags = reinterpret_cast<uint8_t*>(w.gcol + groups * 8);
+}
+
+// Ascending block-wide bitonic sort of a[0, n) (n a power of two).
+__device__ void bitonic_sort(uint64_t* a, uint32_t n) {
+  for (uint32_t k = 2; k <= n; k <<= 1)
+    for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+      __syncthreads();
+      for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const uint32_t l = i ^ j;
+        if (l > i) {
+          const uint64_t x = a[i], y = a[l];
+          if ((x > y) == ((i & k) == 0)) {
+            a[i] = y;
+            a[l] = x;
+          }
+        }
+      }
+    }
+  __syncthreads();
+}
+
+// Exclusive scan of flags[0, n) into out (ballot + popc per warp, then the
+// warp totals); returns the number of set flags.  Every thread calls it.
+__device__ int block_flag_scan(const uint8_t* flags, int n, int* out, int* warp_tot) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  int base = 0;
+  for (int c0 = 0; c0 < n; c0 += blockDim.x) {
+    const int i = c0 + threadIdx.x;
+    const bool f = i < n && flags[i];
+    const unsigned bal = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) warp_tot[warp] = __popc(bal);
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int w = 0; w < nw; ++w) {
+      before += w < warp ? warp_tot[w] : 0;
+      total += warp_tot[w];
+    }
+    if (i < n) out[i] = base + before + __popc(bal & ((1u << lane) - 1u));
+    base += total;
+    __syncthreads();
+  }
+  return base;
+}
+
+// Profile, candidates and groups of one window; returns the number of
+// sub-blocks kept (w.slot, w.gcol filled).  Every thread calls it.
+__device__ int window_groups(const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+                             int r0, int r1, const RouteGpuParams& p, WinWork& w, int* s_int) {
+  const int e0 = indptr[r0], e1 = indptr[r1];
+  const int n = e1 - e0;
+  const uint32_t np2 = next_pow2((uint32_t)max(n, 1));
+  for (int i = threadIdx.x; i < (int)np2; i += blockDim.x) w.keys[i] = ~0ull;
+  __syncthreads();
+  for (int r = r0; r < r1; ++r)
+    for (int e = indptr[r] + threadIdx.x; e < indptr[r + 1]; e += blockDim.x)
+      w.keys[e - e0] = ((uint64_t)(uint32_t)indices[e] << 32) |
+                       ((uint64_t)(uint32_t)(e - e0) << 4) | (uint32_t)(r - r0);
+  bitonic_sort(w.keys, np2);
+  // distinct columns: first key of each column
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    w.flags[i] = (i == 0 || (w.keys[i] >> 32) != (w.keys[i - 1] >> 32)) ? 1 : 0;
+  __syncthreads();
+  int* warp_tot = s_int;
+  const int nu = block_flag_scan(w.flags, n, w.pos, warp_tot);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) w.pos[i] += w.flags[i] ? 0 : -1;
+  for (int u = threadIdx.x; u < nu; u += blockDim.x) {
+    w.umask[u] = 0;
+    w.slot[u] = -1;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int u = w.pos[i];
+    if (w.flags[i]) w.ucol[u] = (int)(w.keys[i] >> 32);
+    atomicOr(&w.umask[u], 1u << (uint32_t)(w.keys[i] & 15u));
+  }
+  __syncthreads();
+  if (p.skip_tc) return 0;
+  // candidates: used by >= density rows, ordered by (count desc, column asc)
+  for (int u = threadIdx.x; u < nu; u += blockDim.x)
+    w.flags[u] = __popc(w.umask[u]) >= p.density ? 1 : 0;
+  __syncthreads();
+  const int nc = block_flag_scan(w.flags, nu, w.tmp, warp_tot);
+  const uint32_t cp2 = next_pow2((uint32_t)max(nc, 1));
+  for (int i = threadIdx.x; i < (int)cp2; i += blockDim.x) w.cand[i] = ~0ull;
+  __syncthreads();
+  for (int u = threadIdx.x; u < nu; u += blockDim.x)
+    if (w.flags[u]) w.cand[w.tmp[u]] = ((uint64_t)(16 - __popc(w.umask[u])) << 32) | (uint32_t)u;
+  bitonic_sort(w.cand, cp2);
+  // chunks of 8 in candidate order; a chunk is kept when its count sum over
+  // window * 8 reaches tc_min_util; thread 0 walks the (few) candidates
+  if (threadIdx.x == 0) {
+    int kept = 0;
+    for (int s = 0; s < nc; s += 8) {
+      const int e = min(s + 8, nc), m = e - s;
+      int us[8];
+      int nnz = 0;
+      for (int i = 0; i < m; ++i) {
+        us[i] = (int)(uint32_t)w.cand[s + i];
+        nnz += __popc(w.umask[us[i]]);
+      }
+      const float util = (float)nnz / (float)(p.window * 8);
+      if (util < p.tc_min_util) continue;
+      for (int i = 1; i < m; ++i)
+        for (int j = i; j > 0 && w.ucol[us[j - 1]] > w.ucol[us[j]]; --j) {
+          const int t = us[j - 1];
+          us[j - 1] = us[j];
+          us[j] = t;
+        }
+      for (int k = 0; k < 8; ++k) {
+        if (k < m) w.slot[us[k]] = kept * 8 + k;
+        w.gcol[kept * 8 + k] = k < m ? w.ucol[us[k]] : -1;
+      }
+      ++kept;
+    }
+    s_int[8] = kept;
+  }
+  __syncthreads();
+  return s_int[8];
+}
+
+// A key is on the tensor cores when its column has a slot and it is the
+// first key of its (column, row) (keys of a column ascend by entry, so the
+// entries of one row are adjacent).
+__device__ __forceinline__ bool tc_key(const WinWork& w, int i) {
+  if (w.slot[w.pos[i]] < 0) return false;
+  return i == 0 || (w.keys[i - 1] >> 32) != (w.keys[i] >> 32) ||
+         (w.keys[i - 1] & 15u) != (w.keys[i] & 15u);
+}
+
+constexpr int kSmemRoute = 64 * 4;        // s_int scratch after the storage
+
+// FILL == false: sub-blocks and values per window into n_sub / n_val.
+// FILL == true:  the tables at sub_off / val_off.
+template <bool FILL>
+__global__ void __launch_bounds__(kRThreads) tc_funnel_kernel(
+    const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
+    const float* __restrict__ values, int n_rows, RouteGpuParams p,
+    const int64_t* __restrict__ big_off, uint8_t* big_scratch, int* n_sub, int* n_val,
+    const int* __restrict__ sub_off, const int* __restrict__ val_off, int32_t* t_column,
+    int64_t* t_binary, float* t_value, int32_t* t_edge, int32_t* sub_nval) {
+  extern __shared__ __align__(16) uint8_t smem_route[];
+  int* s_int = reinterpret_cast<int*>(smem_route + storage_bytes(kSmemKeys));
+  const int wi = blockIdx.x;
+  const int r0 = wi * 16, r1 = min(r0 + 16, n_rows);
+  const int e0 = indptr[r0];
+  const int n = indptr[r1] - e0;
+  WinWork w;
+  if (n <= kSmemKeys) bind_storage(w, smem_route, kSmemKeys);
+  else bind_storage(w, big_scratch + big_off[wi], next_pow2((uint32_t)n));
+  const int kept = window_groups(indptr, indices, r0, r1, p, w, s_int);
+  if (!FILL) {
+    int cnt = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) cnt += (kept > 0 && tc_key(w, i)) ? 1 : 0;
+    cnt = __reduce_add_sync(0xffffffffu, cnt);
+    if (threadIdx.x == 0) s_int[9] = 0;
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) atomicAdd(&s_int[9], cnt);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      n_sub[wi] = kept;
+      n_val[wi] = s_int[9];
+    }
+    return;
+  }
+  if (kept == 0) return;
+  for (int s = threadIdx.x; s < kept; s += blockDim.x) w.glo[s] = w.ghi[s] = 0ull;
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (!tc_key(w, i)) continue;
+    const int sl = w.slot[w.pos[i]], lr = (int)(w.keys[i] & 15u), s = sl >> 3, k = sl & 7;
+    if (lr >= 8) atomicOr(reinterpret_cast<unsigned long long*>(&w.ghi[s]), 1ull << ((lr - 8) * 8 + k));
+    else atomicOr(reinterpret_cast<unsigned long long*>(&w.glo[s]), 1ull << (lr * 8 + k));
+  }
+  __syncthreads();
+  const int sb = sub_off[wi];
+  for (int s = threadIdx.x; s < kept; s += blockDim.x) {
+    t_binary[2 * (int64_t)(sb + s)] = (int64_t)w.glo[s];
+    t_binary[2 * (int64_t)(sb + s) + 1] = (int64_t)w.ghi[s];
+    sub_nval[sb + s] = __popcll(w.glo[s]) + __popcll(w.ghi[s]);
+    for (int k = 0; k < 8; ++k) t_column[(int64_t)(sb + s) * 8 + k] = w.gcol[s * 8 + k];
+  }
+  // values start, per sub-block, after the window's earlier sub-blocks
+  if (threadIdx.x == 0) {
+    int acc = 0;
+    for (int s = 0; s < kept; ++s) {
+      w.tmp[s] = acc;
+      acc += __popcll(w.glo[s]) + __popcll(w.ghi[s]);
+    }
+  }
+  __syncthreads();
+  const int vb = val_off[wi];
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (!tc_key(w, i)) continue;
+    const int sl = w.slot[w.pos[i]], lr = (int)(w.keys[i] & 15u), s = sl >> 3, k = sl & 7;
+    const int bit = lr >= 8 ? (lr - 8) * 8 + k : lr * 8 + k;
+    const int rank = lr >= 8 ? __popcll(w.glo[s]) + __popcll(w.ghi[s] & ((1ull << bit) - 1ull))
+                             : __popcll(w.glo[s] & ((1ull << bit) - 1ull));
+    const int e = e0 + (int)((w.keys[i] >> 4) & 0x0FFFFFFFu);
+    t_value[vb + w.tmp[s] + rank] = values[e];
+    t_edge[vb + w.tmp[s] + rank] = e;
+  }
+}
+
+template <typename T>
+struct DevArr {
+  T* p = nullptr;
+  ~DevArr() { if (p) cudaFree(p); }
+  int alloc(size_t n) {
+    cudaError_t e = cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T));
+    return e == cudaSuccess ? TR_OK : cuda_fail(e, "cudaMalloc (gpu router)");
+  }
+};
+
+}  // namespace
+
+int route_tc_gpu(const int32_t* d_indptr, const int32_t* d_indices, const float* d_values,
+                 int32_t n_rows, const RouteGpuParams& p, TcTables& out, std::string& err) {
+  out = TcTables();
+  if (n_rows <= 0) return TR_OK;
+  const int W = (n_rows + 15) / 16;
+  std::vector<int32_t> indptr(n_rows + 1);
+  TRS_CUDA(cudaMemcpy(indptr.data(), d_indptr, (n_rows + 1) * 4, cudaMemcpyDeviceToHost));
+  // global scratch slices for windows beyond shared memory
+  std::vector<int64_t> big_off(W, 0);
+  int64_t big_bytes = 0;
+  for (int w = 0; w < W; ++w) {
+    const int n = indptr[std::min(w * 16 + 16, n_rows)] - indptr[w * 16];
+    if (n > kSmemKeys) {
+      big_off[w] = big_bytes;
+      big_bytes += (storage_bytes(next_pow2((uint32_t)n)) + 255) / 256 * 256;
+    }
+  }
+  DevArr<int64_t> d_big_off;
+  DevArr<uint8_t> d_big;
+  DevArr<int> d_nsub, d_nval, d_soff, d_voff;
+  int rc;
+  if ((rc = d_big_off.alloc(W)) || (rc = d_big.alloc(big_bytes)) || (rc = d_nsub.alloc(W)) ||
+      (rc = d_nval.alloc(W)) || (rc = d_soff.alloc(W)) || (rc = d_voff.alloc(W)))
+    return rc;
+  TRS_CUDA(cudaMemcpy(d_big_off.p, big_off.data(), W * 8, cudaMemcpyHostToDevice));
+  const int smem = (int)storage_bytes(kSmemKeys) + kSmemRoute;
+  static bool attr = false;
+  if (!attr) {
+    TRS_CUDA(cudaFuncSetAttribute(tc_funnel_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    TRS_CUDA(cudaFuncSetAttribute(tc_funnel_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr = true;
+  }
+  tc_funnel_kernel<false><<<W, kRThreads, smem>>>(d_indptr, d_indices, d_values, n_rows, p,
+                                                  d_big_off.p, d_big.p, d_nsub.p, d_nval.p, nullptr,
+                                                  nullptr, nullptr, nullptr, nullptr, nullptr,
+                                                  nullptr);
+  TRS_CUDA(cudaGetLastError());
+  std::vector<int> nsub(W), nval(W), soff(W), voff(W);
+  TRS_CUDA(cudaMemcpy(nsub.data(), d_nsub.p, W * 4, cudaMemcpyDeviceToHost));
+  TRS_CUDA(cudaMemcpy(nval.data(), d_nval.p, W * 4, cudaMemcpyDeviceToHost));
+  int64_t tsub = 0, tval = 0;
+  for (int w = 0; w < W; ++w) {
+    soff[w] = (int)tsub;
+    voff[w] = (int)tval;
+    tsub += nsub[w];
+    tval += nval[w];
+  }
+  if (tsub > INT32_MAX / 8 || tval > INT32_MAX) { err = "too many tensor-core entries"; return TR_ERR_UNSUPPORTED; }
+  TRS_CUDA(cudaMemcpy(d_soff.p, soff.data(), W * 4, cudaMemcpyHostToDevice));
+  TRS_CUDA(cudaMemcpy(d_voff.p, voff.data(), W * 4, cudaMemcpyHostToDevice));
+  DevArr<int32_t> d_col, d_edge, d_snval;
+  DevArr<int64_t> d_bin;
+  DevArr<float> d_val;
+  if ((rc = d_col.alloc(tsub * 8)) || (rc = d_bin.alloc(tsub * 2)) || (rc = d_val.alloc(tval)) ||
+      (rc = d_edge.alloc(tval)) || (rc = d_snval.alloc(tsub)))
+    return rc;
+  tc_funnel_kernel<true><<<W, kRThreads, smem>>>(d_indptr, d_indices, d_values, n_rows, p,
+                                                 d_big_off.p, d_big.p, nullptr, nullptr, d_soff.p,
+                                                 d_voff.p, d_col.p, d_bin.p, d_val.p, d_edge.p,
+                                                 d_snval.p);
+  TRS_CUDA(cudaGetLastError());
+  TRS_CUDA(cudaDeviceSynchronize());
+  out.t_column.resize(tsub * 8);
+  out.t_binary.resize(tsub * 2);
+  out.t_value.resize(tval);
+  out.t_edge.resize(tval);
+  std::vector<int32_t> snval(tsub);
+  if (tsub) {
+    TRS_CUDA(cudaMemcpy(out.t_column.data(), d_col.p, tsub * 8 * 4, cudaMemcpyDeviceToHost));
+    TRS_CUDA(cudaMemcpy(out.t_binary.data(), d_bin.p, tsub * 2 * 8, cudaMemcpyDeviceToHost));
+    TRS_CUDA(cudaMemcpy(snval.data(), d_snval.p, tsub * 4, cudaMemcpyDeviceToHost));
+  }
+  if (tval) {
+    TRS_CUDA(cudaMemcpy(out.t_value.data(), d_val.p, tval * 4, cudaMemcpyDeviceToHost));
+    TRS_CUDA(cudaMemcpy(out.t_edge.data(), d_edge.p, tval * 4, cudaMemcpyDeviceToHost));
+  }
+  // value offsets per sub-block; parts of partsize_t sub-blocks per window
+  out.t_block_offset.assign(1, 0);
+  for (int64_t s = 0; s < tsub; ++s) out.t_block_offset.push_back(out.t_block_offset.back() + snval[s]);
+  out.t_row_offset.assign(1, 0);
+  const int pt = std::max(p.partsize_t, 1);
+  for (int w = 0; w < W; ++w) {
+    const int ns = nsub[w];
+    if (ns == 0) continue;
+    auto part = [&](int cnt) {
+      out.t_row_offset.push_back(out.t_row_offset.back() + cnt);
+      out.t_window_row.push_back(w * 16);
+    };
+    if (ns <= pt) {
+      part(ns);
+    } else {
+      for (int q = 0; q < ns / pt; ++q) part(pt);
+      if (ns % pt) part(ns % pt);
+    }
+  }
+  return TR_OK;
+}
+
+}  // namespace trs

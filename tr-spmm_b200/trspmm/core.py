@@ -98,6 +98,47 @@ def route(indptr, indices, values, partsize_t=32, partsize_c=32, shortsize=3, de
     return out
 
 
+TC_TABLE_IDX = {"t_row_offset": 0, "t_block_offset": 1, "t_column": 2, "t_value": 3,
+                "t_window_row": 4, "t_binary": 6}
+
+
+def route_tc_device(indptr, indices, values, n_rows, partsize_t=32, density=8, tc_min_util=0.0,
+                    skip_tc=False):
+    """The dense-TC funnel of the router on the GPU (tr_route_tc_device):
+    CUDA int32 indptr/indices and float32 values of a CSR whose rows are
+    sorted by column; returns the TC tables (numpy) keyed by name, equal to
+    route(..., mode="exact")'s t_row_offset, t_block_offset, t_column,
+    t_value, t_window_row and t_binary."""
+    import torch
+    for t, dt in ((indptr, torch.int32), (indices, torch.int32), (values, torch.float32)):
+        if not (t.is_cuda and t.dtype == dt and t.is_contiguous()):
+            raise RuntimeError("indptr/indices (int32) and values (float32) must be contiguous CUDA tensors")
+    L = lib()
+    prm = _params(partsize_t=partsize_t, density=density, tc_min_util=tc_min_util,
+                  skip_tc=skip_tc, mode="exact")
+    h = ctypes.c_void_p()
+    check(L.tr_route_tc_device(ctypes.c_void_p(indptr.data_ptr()),
+                               ctypes.c_void_p(indices.data_ptr()),
+                               ctypes.c_void_p(values.data_ptr()), int(n_rows), ctypes.byref(prm),
+                               ctypes.byref(h)))
+    try:
+        out = {}
+        for name, i in TC_TABLE_IDX.items():
+            dt = _DTYPES[i]
+            data = ctypes.c_void_p()
+            n = ctypes.c_int64()
+            check(L.tr_route_table(h, i, ctypes.byref(data), ctypes.byref(n)))
+            if n.value == 0:
+                out[name] = np.zeros(0, dtype=dt)
+            else:
+                buf = (ctypes.c_char * (n.value * np.dtype(dt).itemsize)).from_address(data.value)
+                out[name] = np.frombuffer(buf, dtype=dt, count=n.value).copy()
+        out["seconds"] = L.tr_route_seconds(h)
+    finally:
+        L.tr_route_free(h)
+    return out
+
+
 def _half_bits(x):
     a = np.ascontiguousarray(x)
     if a.dtype != np.float16:
