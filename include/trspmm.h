@@ -101,6 +101,37 @@ int tr_route_table(const tr_route* r, int idx, const void** data, int64_t* count
  * others are empty). */
 int tr_route_tc_device(const int32_t* d_indptr, const int32_t* d_indices, const float* d_values,
                        int32_t n_rows, const tr_route_params* params, tr_route** out);
+/* The device router's dense-TC funnel for callers that cannot allocate GPU
+ * memory — code running under a caller-owned memory pool or arena, a
+ * framework's custom allocator, or any setting where a cudaMalloc /
+ * cudaFree inside the library would synchronise the device or break the
+ * caller's memory accounting.  It calls no cudaMalloc, cudaFree or other
+ * allocating routine: the caller passes the inputs (device CSR, rows sorted
+ * by column) and the output buffers with their capacities (cap_sub
+ * sub-blocks: t_column [cap_sub*8], t_binary [cap_sub*2], t_block_offset
+ * [cap_sub+1]; cap_val values: t_value [cap_val]); the tables written equal
+ * tr_route_tc_device's t_column, t_binary, t_block_offset and t_value, and
+ * *n_sub_out / *n_val_out receive their sizes.  Its scratch (per-window
+ * counts and offsets, status words: 1 MiB + 16 bytes) is one static device
+ * array that every GPU loading the library holds until the process exits.
+ * Nothing has to start at zero: each call clears the array's status words
+ * itself, every count and offset is written before it is read, and the
+ * output buffers are written, not accumulated into.
+ * Limits, each refused with a clear error: at most 1,048,576 rows (65,536
+ * windows), at most 2048 entries in any 16-row window (use
+ * tr_route_tc_device beyond that), capacities large enough for the tables.
+ * The first call on a device takes the array's device address and sets the
+ * kernels' shared-memory limit; make that first call before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race
+ * (run them on one stream, one after another).  The call waits for
+ * `stream` before returning (it reads four status words back).  No
+ * counterpart in the reference. */
+int tr_route_tc_device_noalloc(const int32_t* d_indptr, const int32_t* d_indices,
+                               const float* d_values, int32_t n_rows,
+                               const tr_route_params* params, int32_t* t_column,
+                               int64_t* t_binary, float* t_value, int32_t* t_block_offset,
+                               int64_t cap_sub, int64_t cap_val, int64_t* n_sub_out,
+                               int64_t* n_val_out, void* stream);
 /* Seconds spent building the tables (the reference's 30th return). */
 double tr_route_seconds(const tr_route* r);
 void tr_route_free(tr_route* r);

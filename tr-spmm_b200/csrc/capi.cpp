@@ -214,6 +214,28 @@ int tr_route_tc_device(const int32_t* d_indptr, const int32_t* d_indices, const 
   return TR_OK;
 }
 
+int tr_route_tc_device_noalloc(const int32_t* d_indptr, const int32_t* d_indices,
+                               const float* d_values, int32_t n_rows,
+                               const tr_route_params* params, int32_t* t_column,
+                               int64_t* t_binary, float* t_value, int32_t* t_block_offset,
+                               int64_t cap_sub, int64_t cap_val, int64_t* n_sub_out,
+                               int64_t* n_val_out, void* stream) {
+  if (!d_indptr || !params) return fail(TR_ERR_ARG, "null argument");
+  if (params->window != 16) return fail(TR_ERR_UNSUPPORTED, "the device router uses 16-row windows");
+  if (cap_sub > 0 && (!t_column || !t_binary || !t_block_offset))
+    return fail(TR_ERR_ARG, "null table buffer with a non-zero sub-block capacity");
+  if (cap_val > 0 && !t_value) return fail(TR_ERR_ARG, "null value buffer with a non-zero capacity");
+  RouteGpuParams gp;
+  gp.window = 16;
+  gp.density = params->density;
+  gp.tc_min_util = params->tc_min_util;
+  gp.partsize_t = params->partsize_t;
+  gp.skip_tc = params->skip_tc;
+  return route_tc_gpu_noalloc(d_indptr, d_indices, d_values, n_rows, gp, t_column, t_binary,
+                              t_value, t_block_offset, cap_sub, cap_val, n_sub_out, n_val_out,
+                              (cudaStream_t)stream);
+}
+
 double tr_route_seconds(const tr_route* r) { return r ? r->t.seconds : 0.0; }
 void tr_route_free(tr_route* r) { delete r; }
 

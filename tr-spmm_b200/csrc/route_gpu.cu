@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "../../include/trspmm.h"
@@ -215,13 +216,18 @@ constexpr int kSmemRoute = 64 * 4;        // s_int scratch after the storage
 
 // FILL == false: sub-blocks and values per window into n_sub / n_val.
 // FILL == true:  the tables at sub_off / val_off.
-template <bool FILL>
+// NOALLOC (the entry point that allocates nothing): windows beyond shared
+// memory are refused (status[0] |= 1, no output), nothing is written when
+// the scanned totals exceed the caller's capacities (status[0] |= 2), and
+// each sub-block's value count goes to sub_nval[sb + s] for the caller's
+// t_block_offset (sub_nval = t_block_offset + 1).
+template <bool FILL, bool NOALLOC = false>
 __global__ void __launch_bounds__(kRThreads) tc_funnel_kernel(
     const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
     const float* __restrict__ values, int n_rows, RouteGpuParams p,
     const int64_t* __restrict__ big_off, uint8_t* big_scratch, int* n_sub, int* n_val,
     const int* __restrict__ sub_off, const int* __restrict__ val_off, int32_t* t_column,
-    int64_t* t_binary, float* t_value, int32_t* t_edge, int32_t* sub_nval) {
+    int64_t* t_binary, float* t_value, int32_t* t_edge, int32_t* sub_nval, int* status = nullptr) {
   extern __shared__ __align__(16) uint8_t smem_route[];
   int* s_int = reinterpret_cast<int*>(smem_route + storage_bytes(kSmemKeys));
   const int wi = blockIdx.x;
@@ -229,6 +235,16 @@ __global__ void __launch_bounds__(kRThreads) tc_funnel_kernel(
   const int e0 = indptr[r0];
   const int n = indptr[r1] - e0;
   WinWork w;
+  if (NOALLOC) {
+    if (n > kSmemKeys) {
+      if (threadIdx.x == 0) {
+        atomicOr(status, 1);
+        if (!FILL) n_sub[wi] = n_val[wi] = 0;
+      }
+      return;
+    }
+    if (FILL && (status[0] & 2)) return;
+  }
   if (n <= kSmemKeys) bind_storage(w, smem_route, kSmemKeys);
   else bind_storage(w, big_scratch + big_off[wi], next_pow2((uint32_t)n));
   const int kept = window_groups(indptr, indices, r0, r1, p, w, s_int);
@@ -281,7 +297,7 @@ __global__ void __launch_bounds__(kRThreads) tc_funnel_kernel(
                              : __popcll(w.glo[s] & ((1ull << bit) - 1ull));
     const int e = e0 + (int)((w.keys[i] >> 4) & 0x0FFFFFFFu);
     t_value[vb + w.tmp[s] + rank] = values[e];
-    t_edge[vb + w.tmp[s] + rank] = e;
+    if (t_edge) t_edge[vb + w.tmp[s] + rank] = e;
   }
 }
 
@@ -392,6 +408,178 @@ int route_tc_gpu(const int32_t* d_indptr, const int32_t* d_indices, const float*
       if (ns % pt) part(ns % pt);
     }
   }
+  return TR_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The entry point that allocates nothing (tr_route_tc_device_noalloc)
+// ---------------------------------------------------------------------------
+// Its scratch — per-window sub-block and value counts, their exclusive
+// scans, and four status / total words — lives in one file-scope device
+// array, held by every GPU that loads the library until the process exits.
+// Host code never passes the array's name to a kernel (on the host the name
+// is only a stand-in): the device address comes from cudaGetSymbolAddress,
+// taken once per device with that device current.
+constexpr int kNoAllocMaxWindows = 65536;                 // 1,048,576 rows
+constexpr int kNoAllocWords = 4 * kNoAllocMaxWindows + 4; // 1 MiB + 16 bytes
+static __device__ __align__(256) int g_noalloc_scratch[kNoAllocWords];
+
+namespace {
+
+// Exclusive scans of n_sub and n_val over W windows (one block), totals in
+// status[1] / status[2]; status[0] |= 2 when a total exceeds its capacity.
+__global__ void noalloc_scan_kernel(const int* n_sub, const int* n_val, int W, int* sub_off,
+                                    int* val_off, int* status, long long cap_sub, long long cap_val) {
+  __shared__ long long carry[2];
+  __shared__ int wt[2][32];
+  if (threadIdx.x == 0) carry[0] = carry[1] = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int c0 = 0; c0 < W; c0 += blockDim.x) {
+    const int i = c0 + threadIdx.x;
+    const int a = i < W ? n_sub[i] : 0, b = i < W ? n_val[i] : 0;
+    int xa = a, xb = b;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const int ya = __shfl_up_sync(0xffffffffu, xa, off), yb = __shfl_up_sync(0xffffffffu, xb, off);
+      if (lane >= off) { xa += ya; xb += yb; }
+    }
+    if (lane == 31) { wt[0][warp] = xa; wt[1][warp] = xb; }
+    __syncthreads();
+    long long ba = 0, bb = 0, ta = 0, tb = 0;
+    for (int w = 0; w < nw; ++w) {
+      if (w < warp) { ba += wt[0][w]; bb += wt[1][w]; }
+      ta += wt[0][w];
+      tb += wt[1][w];
+    }
+    if (i < W) {
+      sub_off[i] = (int)(carry[0] + ba + xa - a);
+      val_off[i] = (int)(carry[1] + bb + xb - b);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) { carry[0] += ta; carry[1] += tb; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    status[1] = (int)min(carry[0], (long long)INT32_MAX);
+    status[2] = (int)min(carry[1], (long long)INT32_MAX);
+    if (carry[0] > cap_sub || carry[1] > cap_val) atomicOr(status, 2);
+  }
+}
+
+// In place: a[0] = 0, a[1..n] = inclusive prefix sums of the counts stored
+// there (one block).
+__global__ void noalloc_block_offsets_kernel(int32_t* a, const int* status) {
+  if (status[0] != 0) return;
+  const int n = status[1];
+  __shared__ int wt[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) { carry = 0; a[0] = 0; }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int c0 = 0; c0 < n; c0 += blockDim.x) {
+    const int i = c0 + threadIdx.x;
+    int x = i < n ? a[1 + i] : 0;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, off);
+      if (lane >= off) x += y;
+    }
+    if (lane == 31) wt[warp] = x;
+    __syncthreads();
+    int before = 0, tot = 0;
+    for (int w = 0; w < nw; ++w) {
+      if (w < warp) before += wt[w];
+      tot += wt[w];
+    }
+    if (i < n) a[1 + i] = carry + before + x;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+}
+
+// Per-device set-up: the scratch array's device address and the kernels'
+// shared-memory limit, once per device.
+int noalloc_setup(int** scratch) {
+  static int* addr[128] = {nullptr};
+  int dev = 0;
+  TRS_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) return fail(TR_ERR_UNSUPPORTED, "device ordinal beyond 127");
+  if (!addr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
+    const int smem = (int)storage_bytes(kSmemKeys) + kSmemRoute;
+    TRS_CUDA(cudaFuncSetAttribute(tc_funnel_kernel<false, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    TRS_CUDA(cudaFuncSetAttribute(tc_funnel_kernel<true, true>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    addr[dev] = static_cast<int*>(p);
+  }
+  *scratch = addr[dev];
+  return TR_OK;
+}
+
+}  // namespace
+
+int route_tc_gpu_noalloc(const int32_t* d_indptr, const int32_t* d_indices, const float* d_values,
+                         int32_t n_rows, const RouteGpuParams& p, int32_t* t_column,
+                         int64_t* t_binary, float* t_value, int32_t* t_block_offset,
+                         int64_t cap_sub, int64_t cap_val, int64_t* n_sub_out,
+                         int64_t* n_val_out, cudaStream_t stream) {
+  if (n_rows < 0) return fail(TR_ERR_ARG, "negative row count");
+  const int64_t W64 = ((int64_t)n_rows + 15) / 16;
+  if (W64 > kNoAllocMaxWindows)
+    return fail(TR_ERR_UNSUPPORTED, "the no-alloc router takes at most " +
+                                        std::to_string((int64_t)kNoAllocMaxWindows * 16) +
+                                        " rows (its scratch holds 65536 windows)");
+  if (cap_sub < 0 || cap_val < 0) return fail(TR_ERR_ARG, "negative capacity");
+  int* scratch = nullptr;
+  int rc = noalloc_setup(&scratch);
+  if (rc) return rc;
+  const int W = (int)W64;
+  int* n_sub = scratch;
+  int* n_val = scratch + kNoAllocMaxWindows;
+  int* sub_off = scratch + 2 * kNoAllocMaxWindows;
+  int* val_off = scratch + 3 * kNoAllocMaxWindows;
+  int* status = scratch + 4 * kNoAllocMaxWindows;
+  // The status words still hold the last call's values: the only scratch
+  // that must start at zero (counts and offsets are written before use).
+  TRS_CUDA(cudaMemsetAsync(status, 0, 4 * sizeof(int), stream));
+  int host_status[4] = {0, 0, 0, 0};
+  if (W > 0) {
+    const int smem = (int)storage_bytes(kSmemKeys) + kSmemRoute;
+    tc_funnel_kernel<false, true><<<W, kRThreads, smem, stream>>>(
+        d_indptr, d_indices, d_values, n_rows, p, nullptr, nullptr, n_sub, n_val, nullptr,
+        nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, status);
+    TRS_CUDA(cudaGetLastError());
+    noalloc_scan_kernel<<<1, 1024, 0, stream>>>(n_sub, n_val, W, sub_off, val_off, status,
+                                                cap_sub, cap_val);
+    TRS_CUDA(cudaGetLastError());
+    tc_funnel_kernel<true, true><<<W, kRThreads, smem, stream>>>(
+        d_indptr, d_indices, d_values, n_rows, p, nullptr, nullptr, nullptr, nullptr, sub_off,
+        val_off, t_column, t_binary, t_value, nullptr, t_block_offset ? t_block_offset + 1 : nullptr,
+        status);
+    TRS_CUDA(cudaGetLastError());
+    if (t_block_offset) {
+      noalloc_block_offsets_kernel<<<1, 1024, 0, stream>>>(t_block_offset, status);
+      TRS_CUDA(cudaGetLastError());
+    }
+  } else if (t_block_offset && cap_sub >= 0) {
+    TRS_CUDA(cudaMemsetAsync(t_block_offset, 0, sizeof(int32_t), stream));
+  }
+  TRS_CUDA(cudaMemcpyAsync(host_status, status, sizeof(host_status), cudaMemcpyDeviceToHost, stream));
+  TRS_CUDA(cudaStreamSynchronize(stream));
+  if (host_status[0] & 1)
+    return fail(TR_ERR_UNSUPPORTED, "a 16-row window holds more than " + std::to_string(kSmemKeys) +
+                                        " entries; the no-alloc router keeps windows in shared "
+                                        "memory (tr_route_tc_device handles any size)");
+  if (host_status[0] & 2)
+    return fail(TR_ERR_ARG, "output capacity too small: need " + std::to_string(host_status[1]) +
+                                " sub-blocks and " + std::to_string(host_status[2]) + " values");
+  if (n_sub_out) *n_sub_out = host_status[1];
+  if (n_val_out) *n_val_out = host_status[2];
   return TR_OK;
 }
 

@@ -1,5 +1,7 @@
 // Device router: the dense-TC funnel (route_gpu.cu).
 #pragma once
+#include <cuda_runtime.h>
+
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -27,5 +29,13 @@ struct TcTables {
 // Device CSR in (rows sorted by column), host tables out.
 int route_tc_gpu(const int32_t* d_indptr, const int32_t* d_indices, const float* d_values,
                  int32_t n_rows, const RouteGpuParams& p, TcTables& out, std::string& err);
+
+// The same funnel without any allocation: scratch in a static device array,
+// tables into caller buffers (see tr_route_tc_device_noalloc).
+int route_tc_gpu_noalloc(const int32_t* d_indptr, const int32_t* d_indices, const float* d_values,
+                         int32_t n_rows, const RouteGpuParams& p, int32_t* t_column,
+                         int64_t* t_binary, float* t_value, int32_t* t_block_offset,
+                         int64_t cap_sub, int64_t cap_val, int64_t* n_sub_out,
+                         int64_t* n_val_out, cudaStream_t stream);
 
 }  // namespace trs
