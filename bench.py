@@ -22,9 +22,13 @@ step is timed alone with CUDA events on its stream.
               step B and dC copied from pinned memory, the autograd forward and
               backward of trspmm.autograd.routed_spmm, and C, dB and dval copied
               back to pinned memory
-  roofline    the dominant kernel (the forward's CUDA-core residual pass)
-              against the measured HBM copy bandwidth; algorithmic bytes per
-              launch = res_nnz*(4+2) + (M+1)*4 + N*K*2 + M*K*4
+  roofline    the dominant kernel against the measured HBM copy bandwidth:
+              the fused backward (one launch: dB = A^T dC and dval) with
+              algorithmic bytes per launch = nnz*(4+2+4+4) + (N+1)*4 + M*K*2
+              + N*K*2 + N*K*4, or, when the backward is not fused or is the
+              shorter pass, the forward's CUDA-core residual pass with
+              res_nnz*(4+2) + (M+1)*4 + N*K*2 + M*K*4 (that one is also
+              reported in extra.forward_residual_roofline)
   cpu_baseline / --impl reference: the oracle's C restatement of the same
               step (FP16 operands, FP32 accumulation, OpenMP on all host cores)
   extra       the same step with the plain single-route CSR kernel (forward on
@@ -65,11 +69,11 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def _profile_traffic():
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
-    summary (profiles/csr_residual_pass_large_routed.txt, line
-    'traffic_bytes_per_launch: N'); None when that summary is absent."""
-    path = os.path.join(ROOT, "profiles", "csr_residual_pass_large_routed.txt")
+def _profile_traffic(name):
+    """Per-launch DRAM bytes of a kernel from its committed ncu summary
+    (profiles/<name>, line 'traffic_bytes_per_launch: N'); None when that
+    summary is absent."""
+    path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -140,6 +144,13 @@ class ClockSampler:
 
 def algorithmic_bytes(nnz, m, n_cols, k, out_bytes=4):
     return nnz * (4 + 2) + (m + 1) * 4 + n_cols * k * 2 + m * k * out_bytes
+
+
+def adjoint_sddmm_bytes(nnz, m, n, k, out_bytes=4):
+    """Fused backward over A^T (n rows): per entry its column, value, entry
+    id and dval (4+2+4+4 bytes); dC (m x k FP16) and B (n x k FP16) read
+    once; dB (n x k) written once."""
+    return nnz * (4 + 2 + 4 + 4) + (n + 1) * 4 + m * k * 2 + n * k * 2 + n * k * out_bytes
 
 
 def step_bytes(nnz, m, n, k):
@@ -439,8 +450,8 @@ def main():
 
     peak, peak_kind = _peaks()
     res_nnz = int(pf.info["residual_nnz"])
-    abytes = algorithmic_bytes(res_nnz, g.n_rows, g.n_cols, k, 4)
-    achieved = abytes / (res_ms * 1e-3) / 1e9
+    res_bytes = algorithmic_bytes(res_nnz, g.n_rows, g.n_cols, k, 4)
+    res_gbs = res_bytes / (res_ms * 1e-3) / 1e9
     sbytes = step_bytes(g.nnz, g.n_rows, g.n_cols, k)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -462,6 +473,17 @@ def main():
     fused_bwd = (pa.info["tc_tiles"] + pa.info["sptc_tiles"] + pa.info["promoted_tiles"] == 0
                  and pa.info["residual_nnz"] == g.nnz and k <= 128)
     bwd_launches = 1 if fused_bwd else launches(pa) + 1
+    # the dominant kernel of the step: the fused backward when the adjoint plan
+    # allows it (its one launch takes longer than the forward's residual pass)
+    if fused_bwd and adj_sddmm_ms >= res_ms:
+        dom_kernel = "seg_adjoint_sddmm_kernel (fused backward: dB = A^T dC, dval = SDDMM)"
+        abytes = adjoint_sddmm_bytes(g.nnz, g.n_rows, g.n_cols, k)
+        achieved = abytes / (adj_sddmm_ms * 1e-3) / 1e9
+        traffic = _profile_traffic("seg_adjoint_sddmm_large_routed.txt")
+    else:
+        dom_kernel = "seg_block_kernel (forward residual pass)"
+        abytes, achieved = res_bytes, res_gbs
+        traffic = _profile_traffic("seg_residual_pass_large_routed.txt")
 
     if rank == 0:
         line = {
@@ -474,9 +496,9 @@ def main():
                        "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"replicas{world}", "plan_options": opts},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": _profile_traffic(),
+                         "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind, "algorithmic_bytes": abytes,
-                         "kernel": "csr_block_kernel (forward residual pass)"},
+                         "kernel": dom_kernel},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": UNIT,
                     "h2d_bytes_per_step": int(b.nbytes + dc.nbytes),
@@ -486,6 +508,10 @@ def main():
             "extra": {"forward_ms": fwd_ms, "adjoint_ms": adj_ms, "sddmm_ms": sddmm_ms,
                       "adjoint_sddmm_fused_ms": adj_sddmm_ms,
                       "forward_residual_pass_ms": res_ms,
+                      "forward_residual_roofline": {
+                          "achieved_gbs": res_gbs, "frac": res_gbs / peak,
+                          "algorithmic_bytes": res_bytes,
+                          "traffic": _profile_traffic("seg_residual_pass_large_routed.txt")},
                       "plain_csr_step_ms": plain_ms, "plain_csr_forward_ms": plain_fwd_ms,
                       "routed_vs_plain_step": plain_ms / ms,
                       "routed_vs_plain_forward": plain_fwd_ms / fwd_ms,

@@ -1,16 +1,19 @@
 // sm_100a SpMM kernels.
 //
-//  csr_block_kernel   plain single-route CSR SpMM on CUDA cores: one CTA per
-//                     16-row block, its entries split evenly across 8 warps
-//                     (balanced even with power-law rows), 128-bit loads of
-//                     B rows, FP32 accumulation into a shared-memory block,
-//                     one coalesced store per output element.
+//  seg_block_kernel   CUDA-core CSR SpMM, one CTA per 16-row window: the
+//                     window's entries are cut into one segment per lane
+//                     group, each group streams its segment across rows with
+//                     the row sum in registers (128-bit loads of B rows, FP32
+//                     accumulation).  It is the routed forward's residual
+//                     pass (plan rows, heaviest windows first, row scaling,
+//                     output row map) and, in natural order, the plain
+//                     single-route CSR kernel.
 //  routed_kernel      the fused three-route forward: one CTA per 16-row
 //                     window.  The dense-TC and 2:4 tiles run on tcgen05
 //                     (B rows gathered into 128-byte-swizzled shared memory,
 //                     D^T[feature x row] accumulated in TMEM), the residual
-//                     runs on CUDA cores with the same engine as the plain
-//                     kernel, and the epilogue adds both and stores each
+//                     runs on CUDA cores (row-run engine: block_accumulate),
+//                     and the epilogue adds both and stores each
 //                     output element once (no atomics in global memory, no
 //                     separate 2:4 buffer, no merge kernel — compare
 //                     TR-source/SpMM/mGCNkernel_online.cu:1529-1727).
@@ -19,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "common.cuh"
 #include "plan.h"
@@ -151,48 +155,203 @@ __device__ __forceinline__ void store_row_feature(void* C, int K, int64_t row, i
 }
 
 // ---------------------------------------------------------------------------
-// Plain CSR (single route)
+// Segment-streaming engine (the routed forward's CUDA-core residual pass)
 // ---------------------------------------------------------------------------
-// With PLAN, the rows are a plan's rows (its CUDA-core residual as CSR) and
-// each result row r is scaled by row_scale[r] and stored to row row_out[r]
-// (skipped when negative).
-template <bool F16OUT, bool PLAN = false>
-__global__ void __launch_bounds__(kThreads, 4) csr_block_kernel(
+// One CTA per 16-row window, windows in the plan's launch order (heaviest
+// first, so the longest CTAs start first instead of finishing last).  Each
+// staged chunk of the window's entries is cut into one even-length segment
+// per lane group (L lanes of 8 features), and every group streams its
+// segment across row boundaries with the row's partial sum in registers.
+// When a row ends: a row that lies entirely inside the group's segment is
+// scaled and stored straight to C from registers; a row cut by a segment or
+// chunk boundary is added into the window's rows in shared memory with
+// shared atomics, in a padded layout, slot(f) = f + f/32, where the 8
+// consecutive features of each of the L lanes fall in distinct banks, and is
+// stored at the end of the window together with the window's empty rows.
+//
+// Every group runs the same number of batches of kSegU entries (entries past
+// its segment are predicated), and the full-batch / no-boundary decisions
+// are warp votes, so the lane groups of a warp stay converged; a batch that
+// crosses no row boundary runs without per-entry checks.  Tail padding
+// happens once per segment, not once per row; entry pairs come from 128-bit
+// shared loads; B addresses are 32-bit element offsets from the chunk's
+// feature base.
+constexpr int kSegStride = kChunk + kChunk / 32;     // padded shared row (floats)
+constexpr int kSegU = 4;                             // entries per lane group and batch
+
+__device__ __forceinline__ int seg_slot(int r, int f) { return r * kSegStride + f + (f >> 5); }
+
+// 16 bytes of B row `col` at the lane's feature base Bf.
+template <bool WIDE>
+__device__ __forceinline__ uint4 seg_ldg(const __half* Bf, int col, uint32_t K) {
+  return __ldg(reinterpret_cast<const uint4*>(
+      WIDE ? Bf + (size_t)(uint32_t)col * K : Bf + (uint32_t)col * K));
+}
+
+// Segment length for n staged entries over `groups` lane groups (even, so
+// that entry pairs stay 16-byte aligned in shared memory).
+__device__ __forceinline__ int seg_len(int n, int groups) {
+  return (((n + groups - 1) / groups) + 1) & ~1;
+}
+
+// Whether the entries [a, b) of a row all lie in one segment (then one lane
+// group accumulates and stores the whole row).
+__device__ __forceinline__ bool seg_owned(int a, int b, int e_begin, int e_end, int groups) {
+  if (a >= b) return false;
+  const int ca = (a - e_begin) / kStage, cb = (b - 1 - e_begin) / kStage;
+  if (ca != cb) return false;
+  const int c0 = e_begin + ca * kStage;
+  const int seg = seg_len(min(kStage, e_end - c0), groups);
+  return (a - c0) / seg == (b - 1 - c0) / seg;
+}
+
+// C[row, f .. f+N-1] = s * v[0..N-1] (N = 4 or 8, f a multiple of N; 16-byte
+// streaming stores for FP32, 8- or 16-byte ones for FP16).
+template <bool F16OUT, int N>
+__device__ __forceinline__ void store_vec(void* C, int K, int64_t row, int f, const float* v,
+                                          float s) {
+  if (F16OUT) {
+    uint32_t w[N / 2];
+#pragma unroll
+    for (int i = 0; i < N / 2; ++i) {
+      const __half2 h = __floats2half2_rn(v[2 * i] * s, v[2 * i + 1] * s);
+      w[i] = *reinterpret_cast<const uint32_t*>(&h);
+    }
+    __half* p = reinterpret_cast<__half*>(C) + row * K + f;
+    if (N == 8) __stcs(reinterpret_cast<uint4*>(p), make_uint4(w[0], w[1], w[2], w[3]));
+    else __stcs(reinterpret_cast<uint2*>(p), make_uint2(w[0], w[1]));
+  } else {
+    float4* p = reinterpret_cast<float4*>(reinterpret_cast<float*>(C) + row * K + f);
+#pragma unroll
+    for (int i = 0; i < N / 4; ++i)
+      __stcs(p + i, make_float4(v[4 * i] * s, v[4 * i + 1] * s, v[4 * i + 2] * s, v[4 * i + 3] * s));
+  }
+}
+
+// With PLAN the rows are a plan's rows: result row r is scaled by
+// row_scale[r] and stored to row_out[r] (skipped when negative).  Without
+// WIDE, B offsets are 32-bit (requires (number of B rows) * K < 2^31).
+template <bool F16OUT, bool PLAN, bool WIDE>
+__global__ void __launch_bounds__(kThreads, 4) seg_block_kernel(
     const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
     const __half* __restrict__ values, int M, const __half* __restrict__ B, int K, void* C,
-    const int32_t* __restrict__ row_out = nullptr, const float* __restrict__ row_scale = nullptr) {
-  __shared__ __align__(16) float racc[kBlockRows * kChunk];
-  __shared__ int2 sent[kStage];
+    const int32_t* __restrict__ row_out, const float* __restrict__ row_scale,
+    const int32_t* __restrict__ order) {
+  constexpr int U = kSegU;
+  __shared__ __align__(16) float racc[kBlockRows * kSegStride];
+  __shared__ __align__(16) int2 sent[kStage + 2];
   __shared__ int rp[kBlockRows + 1];
   __shared__ int s_out[kBlockRows];
   __shared__ float s_scale[kBlockRows];
-  const int r0 = blockIdx.x * kBlockRows;
-  if (threadIdx.x <= kBlockRows) rp[threadIdx.x] = indptr[min(r0 + (int)threadIdx.x, M)];
-  if (PLAN && threadIdx.x < kBlockRows) {
-    s_out[threadIdx.x] = r0 + (int)threadIdx.x < M ? row_out[r0 + threadIdx.x] : -1;
-    s_scale[threadIdx.x] = r0 + (int)threadIdx.x < M ? row_scale[r0 + threadIdx.x] : 0.f;
+  __shared__ int s_own[kBlockRows];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int r0 = (order ? order[blockIdx.x] : (int)blockIdx.x) * kBlockRows;
+  if (tid <= kBlockRows) rp[tid] = indptr[min(r0 + tid, M)];
+  if (tid < kBlockRows) {
+    const bool in = r0 + tid < M;
+    s_out[tid] = !in ? -1 : (PLAN ? row_out[r0 + tid] : r0 + tid);
+    s_scale[tid] = (PLAN && in) ? row_scale[r0 + tid] : 1.f;
   }
+  __syncthreads();
+  const int e_begin = rp[0], e_end = rp[kBlockRows];
+  const uint32_t uK = (uint32_t)K;
   for (int f0 = 0; f0 < K; f0 += kChunk) {
     const int fc = min(kChunk, K - f0);
-    for (int i = threadIdx.x; i < kBlockRows * kChunk; i += kThreads) racc[i] = 0.f;
-    __syncthreads();
-    block_accumulate(rp, indices, values, B, K, f0, fc, racc, sent);
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int f = (warp & 3) * 32 + lane;
-    if (f < fc) {
+    int L = 1;
+    while (L * 8 < fc) L <<= 1;
+    const int G = 32 / L, groups = kWarps * G;
+    const int li = lane % L, q = warp * G + lane / L;
+    const bool active = li * 8 < fc;
+    if (tid < kBlockRows) s_own[tid] = seg_owned(rp[tid], rp[tid + 1], e_begin, e_end, groups);
+    {
+      float4* z = reinterpret_cast<float4*>(racc);
+      for (int i = tid; i < kBlockRows * kSegStride / 4; i += kThreads) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    const __half* Bf = B + f0 + (active ? li * 8 : 0);
+    float* dst = racc + seg_slot(0, active ? li * 8 : 0);
+    for (int c0 = e_begin; c0 < e_end; c0 += kStage) {
+      const int n = min(kStage, e_end - c0);
+      __syncthreads();                       // previous chunk consumed, racc zeroed
+      stage_chunk(indices, values, c0, n, sent);
+      __syncthreads();
+      const int seg = seg_len(n, groups);
+      // every group runs the same number of batches (control flow stays
+      // warp-uniform); entries at or past hi are predicated off
+      const int lo0 = q * seg;               // even: entry pairs stay 16-byte aligned
+      const int lo = min(n, lo0), hi = min(n, lo0 + seg);      // chunk-relative
+      int r = 0;
+      while (r < kBlockRows - 1 && rp[r + 1] <= c0 + lo) ++r;
+      int nb = rp[r + 1] - c0;               // chunk-relative end of row r
+      float acc[8];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int r = (warp >> 2) * 8 + i;
-        if (PLAN) {
-          if (s_out[r] >= 0)
-            store_row_feature<F16OUT>(C, K, s_out[r], f0 + f, racc[r * kChunk + f] * s_scale[r]);
-        } else if (r0 + r < M) {
-          store_row_feature<F16OUT>(C, K, r0 + r, f0 + f, racc[r * kChunk + f]);
+      for (int i = 0; i < 8; ++i) acc[i] = 0.f;
+      // row r is done for this group: owned rows go to C, cut rows to racc
+      auto flush = [&]() {
+        if (!active) return;
+        if (rp[r] >= c0 + lo && rp[r + 1] <= c0 + hi) {
+          if (s_out[r] >= 0) store_vec<F16OUT, 8>(C, K, s_out[r], f0 + li * 8, acc, s_scale[r]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 8; ++i) atomicAdd(dst + r * kSegStride + i, acc[i]);
+        }
+      };
+#pragma unroll 1
+      for (int t = lo0; t < lo0 + seg; t += U) {
+        uint4 b[U];
+        uint32_t v[U / 2];
+        if (__all_sync(0xffffffffu, t + U <= hi)) {   // full batch: no predicates
+#pragma unroll
+          for (int u = 0; u < U; u += 2) {
+            const int4 p = *reinterpret_cast<const int4*>(&sent[t + u]);
+            b[u] = seg_ldg<WIDE>(Bf, p.x, uK);
+            b[u + 1] = seg_ldg<WIDE>(Bf, p.z, uK);
+            v[u / 2] = __byte_perm((uint32_t)p.y, (uint32_t)p.w, 0x5410);
+          }
+        } else {                             // a segment's tail
+#pragma unroll
+          for (int u = 0; u < U; u += 2) {
+            // entries at or past hi are not used; their slot is clamped to
+            // stay inside sent[] (even, so the 16-byte load stays aligned)
+            const int4 p = *reinterpret_cast<const int4*>(&sent[min(t + u, kStage)]);
+            b[u] = t + u < hi ? seg_ldg<WIDE>(Bf, p.x, uK) : make_uint4(0u, 0u, 0u, 0u);
+            b[u + 1] = t + u + 1 < hi ? seg_ldg<WIDE>(Bf, p.z, uK) : make_uint4(0u, 0u, 0u, 0u);
+            v[u / 2] = __byte_perm((uint32_t)p.y, (uint32_t)p.w, 0x5410);
+          }
+        }
+        if (__all_sync(0xffffffffu, t + U <= nb && t + U <= hi)) {   // no boundary, full
+#pragma unroll
+          for (int u = 0; u < U; ++u) fma8h(acc, (uint16_t)(v[u / 2] >> (16 * (u & 1))), b[u]);
+        } else {
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int j = t + u;
+            if (j < hi) {
+              if (j >= nb) {                   // row r ends before entry j
+                flush();
+#pragma unroll
+                for (int i = 0; i < 8; ++i) acc[i] = 0.f;
+                do ++r; while (rp[r + 1] - c0 <= j);
+                nb = rp[r + 1] - c0;
+              }
+              fma8h(acc, (uint16_t)(v[u / 2] >> (16 * (u & 1))), b[u]);
+            }
+          }
+          __syncwarp();                      // reconverge the lane groups
         }
       }
+      if (lo < hi) flush();
     }
-    __syncthreads();
+    __syncthreads();                         // every shared atomic has landed
+    // rows cut by a boundary, and empty rows: one 16-byte store per lane
+    for (int r = warp; r < kBlockRows; r += kWarps)
+      if (!s_own[r] && s_out[r] >= 0)
+        for (int f = lane * 4; f < fc; f += 128) {
+          float x[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) x[i] = racc[seg_slot(r, f + i)];
+          store_vec<F16OUT, 4>(C, K, s_out[r], f0 + f, x, s_scale[r]);
+        }
+    __syncthreads();                         // racc and s_own are rewritten next pass
   }
 }
 
@@ -624,11 +783,10 @@ __global__ void __launch_bounds__(256) sddmm_group_kernel(const int32_t* __restr
 // One CTA per 16 rows of the adjoint plan (rows of A^T, i.e. rows of B),
 // K <= 128.  For every residual entry (row j of A^T, column i, value a, A's
 // entry e) a lane group gathers 16-byte chunks of dC[i] once and uses them
-// twice: dB[j] += a * dC[i] (the CUDA-core engine's row-run accumulation)
-// and dval[e] = <dC[i], B[j]> (a dot product with row j of B, held in
-// registers for the run, reduced over the group with shuffles).  The
-// separate SDDMM would gather every dC row a second time.
-constexpr int kUnrollSD = 8;        // entries per lane group and batch in the fused pass
+// twice: dB[j] += a * dC[i] and dval[e] = <dC[i], B[j]> (a dot product with
+// row j of B, held in registers while the row lasts, reduced over the group
+// with shuffles).  The separate SDDMM would gather every dC row a second
+// time.
 
 // Sums 8 per-lane values over a group of L lanes (L = 8 or 16) so that lane
 // (li & 7) ends up with the total of value (li & 7): for L = 16 the two
@@ -654,109 +812,140 @@ __device__ __forceinline__ float group_reduce_scatter8(float (&d)[8], int li) {
   return d[0];
 }
 
-template <int L>
-__device__ __forceinline__ void adjoint_sddmm_chunk(const int* rp, int e0, int n, const int4* sent,
-                                                    const int* s_out, const __half* __restrict__ G,
-                                                    const __half* __restrict__ H, int K,
-                                                    float* racc, float* __restrict__ dval) {
-  constexpr int Gn = 32 / L;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int g = lane / L, li = lane % L;
-  const bool active = li * 8 < K;
-  const int per = (n + kWarps - 1) / kWarps;
-  const int eb = warp * per;
-  const int ee = min(n, eb + per);
-  if (eb >= ee) return;
-  const __half* Gf = G + (active ? li * 8 : 0);
-  int row = 0;
-  while (rp[row + 1] - e0 <= eb) ++row;            // warp-uniform
-  const int c_safe = sent[eb].x;
-  for (int i = eb; i < ee;) {
-    const int rend = min(ee, rp[row + 1] - e0);
-    const int orow = s_out[row];
-    const uint4 hv = (active && orow >= 0)
-                         ? __ldg(reinterpret_cast<const uint4*>(H + (int64_t)orow * K + li * 8))
-                         : make_uint4(0, 0, 0, 0);
-    float acc[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) acc[q] = 0.f;
-    // warp-uniform trip count (the dot products are reduced with full-warp
-    // shuffles inside the loop); entries past the run are predicated off
-    for (int jb = i; jb < rend; jb += Gn * kUnrollSD) {
-      const int j0 = jb + g;
-      uint4 bv[kUnrollSD];
-#pragma unroll
-      for (int u = 0; u < kUnrollSD; ++u) {       // all gathers first
-        const int j = j0 + u * Gn;
-        const int c = j < rend ? sent[j].x : c_safe;
-        bv[u] = __ldg(reinterpret_cast<const uint4*>(Gf + (size_t)c * K));
-      }
-      float d[kUnrollSD];
-      int my_ed = -1;
-#pragma unroll
-      for (int u = 0; u < kUnrollSD; ++u) {       // values and entry ids re-read from shared
-        const int j = j0 + u * Gn;
-        const int4 en = j < rend ? sent[j] : make_int4(0, 0, -1, 0);
-        fma8h(acc, (uint16_t)en.y, bv[u]);
-        d[u] = active ? dot8h(hv, bv[u]) : 0.f;
-        if ((li & 7) == u) my_ed = en.z;
-      }
-      const float tot = group_reduce_scatter8<L>(d, li);
-      if (li < 8 && my_ed >= 0) dval[my_ed] = tot;
-    }
-    for (int off = L; off < 32; off <<= 1)
-#pragma unroll
-      for (int q = 0; q < 8; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
-    if (g == 0 && active) {
-      float* dst = racc + row * kChunk + li * 8;
-#pragma unroll
-      for (int q = 0; q < 8; ++q) atomicAdd(dst + q, acc[q]);
-    }
-    i = rend;
-    while (row < kBlockRows - 1 && rp[row + 1] - e0 <= i) ++row;
-  }
-}
-
-template <bool F16OUT, int L>
-__global__ void __launch_bounds__(kThreads, 3) adjoint_sddmm_kernel(
+// The fused adjoint + SDDMM on the segment-streaming engine (same segments,
+// warp-uniform batches, owned-row stores and cut-row shared atomics as
+// seg_block_kernel).  Batches are 8 entries per lane group: each gathered
+// 16-byte chunk of dC[i] feeds dB[j] += a * dC[i] and the partial dot with
+// row j of B (held in registers, reloaded when the row changes), and the
+// group's 8 partial dots are reduce-scattered so that lane u (< 8) writes
+// dval for the batch's entry u.  K <= 128 (one feature chunk).
+template <bool F16OUT, int L, bool WIDE>
+__global__ void __launch_bounds__(kThreads, 3) seg_adjoint_sddmm_kernel(
     const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
     const __half* __restrict__ values, const int32_t* __restrict__ edges, int M,
     const __half* __restrict__ G, int K, void* C, const int32_t* __restrict__ row_out,
-    const float* __restrict__ row_scale, const __half* __restrict__ H, float* __restrict__ dval) {
-  __shared__ __align__(16) float racc[kBlockRows * kChunk];
-  __shared__ int4 sent[kStage];
+    const float* __restrict__ row_scale, const __half* __restrict__ H, float* __restrict__ dval,
+    const int32_t* __restrict__ order) {
+  constexpr int U = 8;
+  constexpr int Gn = 32 / L, groups = kWarps * Gn;
+  __shared__ __align__(16) float racc[kBlockRows * kSegStride];
+  __shared__ __align__(16) int4 sent[kStage + 1];
   __shared__ int rp[kBlockRows + 1];
   __shared__ int s_out[kBlockRows];
   __shared__ float s_scale[kBlockRows];
-  const int r0 = blockIdx.x * kBlockRows;
-  if (threadIdx.x <= kBlockRows) rp[threadIdx.x] = indptr[min(r0 + (int)threadIdx.x, M)];
-  if (threadIdx.x < kBlockRows) {
-    s_out[threadIdx.x] = r0 + (int)threadIdx.x < M ? row_out[r0 + threadIdx.x] : -1;
-    s_scale[threadIdx.x] = r0 + (int)threadIdx.x < M ? row_scale[r0 + threadIdx.x] : 0.f;
+  __shared__ int s_own[kBlockRows];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int r0 = (order ? order[blockIdx.x] : (int)blockIdx.x) * kBlockRows;
+  if (tid <= kBlockRows) rp[tid] = indptr[min(r0 + tid, M)];
+  if (tid < kBlockRows) {
+    const bool in = r0 + tid < M;
+    s_out[tid] = in ? row_out[r0 + tid] : -1;
+    s_scale[tid] = in ? row_scale[r0 + tid] : 0.f;
   }
-  for (int i = threadIdx.x; i < kBlockRows * kChunk; i += kThreads) racc[i] = 0.f;
   __syncthreads();
-  const uint16_t* v16 = reinterpret_cast<const uint16_t*>(values);
   const int e_begin = rp[0], e_end = rp[kBlockRows];
+  const uint32_t uK = (uint32_t)K;
+  const int li = lane % L, q = warp * Gn + lane / L;
+  const bool active = li * 8 < K;
+  if (tid < kBlockRows) s_own[tid] = seg_owned(rp[tid], rp[tid + 1], e_begin, e_end, groups);
+  {
+    float4* z = reinterpret_cast<float4*>(racc);
+    for (int i = tid; i < kBlockRows * kSegStride / 4; i += kThreads) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
+  const __half* Gf = G + (active ? li * 8 : 0);
+  float* dst = racc + seg_slot(0, active ? li * 8 : 0);
+  const uint16_t* v16 = reinterpret_cast<const uint16_t*>(values);
   for (int c0 = e_begin; c0 < e_end; c0 += kStage) {
     const int n = min(kStage, e_end - c0);
-    __syncthreads();
-    for (int i = threadIdx.x; i < n; i += kThreads)
+    __syncthreads();                         // previous chunk consumed, racc zeroed
+    for (int i = tid; i < n; i += kThreads)
       sent[i] = make_int4(__ldg(indices + c0 + i), (int)__ldg(v16 + c0 + i), __ldg(edges + c0 + i), 0);
     __syncthreads();
-    adjoint_sddmm_chunk<L>(rp, c0, n, sent, s_out, G, H, K, racc, dval);
-  }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int f = (warp & 3) * 32 + lane;
-  if (f < K) {
+    const int seg = seg_len(n, groups);
+    const int lo0 = q * seg;
+    const int lo = min(n, lo0), hi = min(n, lo0 + seg);        // chunk-relative
+    int r = 0;
+    while (r < kBlockRows - 1 && rp[r + 1] <= c0 + lo) ++r;
+    int nb = rp[r + 1] - c0;
+    // row j of B for the dot products of row r's entries
+    auto load_h = [&]() {
+      const int o = s_out[r];
+      return (active && o >= 0) ? __ldg(reinterpret_cast<const uint4*>(H + (int64_t)o * K + li * 8))
+                                : make_uint4(0u, 0u, 0u, 0u);
+    };
+    uint4 hv = load_h();
+    float acc[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const int r = (warp >> 2) * 8 + i;
-      if (s_out[r] >= 0)
-        store_row_feature<F16OUT>(C, K, s_out[r], f, racc[r * kChunk + f] * s_scale[r]);
+    for (int i = 0; i < 8; ++i) acc[i] = 0.f;
+    auto flush = [&]() {
+      if (!active) return;
+      if (rp[r] >= c0 + lo && rp[r + 1] <= c0 + hi) {
+        if (s_out[r] >= 0) store_vec<F16OUT, 8>(C, K, s_out[r], li * 8, acc, s_scale[r]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) atomicAdd(dst + r * kSegStride + i, acc[i]);
+      }
+    };
+#pragma unroll 1
+    for (int t = lo0; t < lo0 + seg; t += U) {
+      uint4 b[U];
+      uint32_t v[U / 2];
+      const bool full = __all_sync(0xffffffffu, t + U <= hi);
+#pragma unroll
+      for (int u = 0; u < U; u += 2) {
+        // entries at or past hi are not used; their slot is clamped into sent[]
+        const int4 p0 = sent[full ? t + u : min(t + u, kStage)];
+        const int4 p1 = sent[full ? t + u + 1 : min(t + u + 1, kStage)];
+        if (full) {
+          b[u] = seg_ldg<WIDE>(Gf, p0.x, uK);
+          b[u + 1] = seg_ldg<WIDE>(Gf, p1.x, uK);
+        } else {
+          b[u] = t + u < hi ? seg_ldg<WIDE>(Gf, p0.x, uK) : make_uint4(0u, 0u, 0u, 0u);
+          b[u + 1] = t + u + 1 < hi ? seg_ldg<WIDE>(Gf, p1.x, uK) : make_uint4(0u, 0u, 0u, 0u);
+        }
+        v[u / 2] = __byte_perm((uint32_t)p0.y, (uint32_t)p1.y, 0x5410);
+      }
+      float d[U];
+      if (__all_sync(0xffffffffu, t + U <= nb && t + U <= hi)) {   // no boundary, full
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          fma8h(acc, (uint16_t)(v[u / 2] >> (16 * (u & 1))), b[u]);
+          d[u] = dot8h(hv, b[u]);
+        }
+      } else {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const int j = t + u;
+          d[u] = 0.f;
+          if (j < hi) {
+            if (j >= nb) {                     // row r ends before entry j
+              flush();
+#pragma unroll
+              for (int i = 0; i < 8; ++i) acc[i] = 0.f;
+              do ++r; while (rp[r + 1] - c0 <= j);
+              nb = rp[r + 1] - c0;
+              hv = load_h();
+            }
+            fma8h(acc, (uint16_t)(v[u / 2] >> (16 * (u & 1))), b[u]);
+            d[u] = dot8h(hv, b[u]);
+          }
+        }
+        __syncwarp();                          // reconverge the lane groups
+      }
+      const float tot = group_reduce_scatter8<L>(d, li);
+      if (li < 8 && t + li < hi) dval[sent[t + li].z] = tot;
     }
+    if (lo < hi) flush();
   }
+  __syncthreads();                             // every shared atomic has landed
+  for (int r = warp; r < kBlockRows; r += kWarps)
+    if (!s_own[r] && s_out[r] >= 0)
+      for (int f = lane * 4; f < K; f += 128) {
+        float x[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) x[i] = racc[seg_slot(r, f + i)];
+        store_vec<F16OUT, 4>(C, K, s_out[r], f, x, s_scale[r]);
+      }
 }
 
 // Any K: one thread per entry.
@@ -786,8 +975,14 @@ int launch_csr(const int32_t* indptr, const int32_t* indices, const uint16_t* va
   const bool f16 = c_dtype == TR_OUT_F16;
   if (k % 8 == 0 && aligned16(b)) {
     const int blocks = (m + kBlockRows - 1) / kBlockRows;
-    if (f16) csr_block_kernel<true><<<blocks, kThreads, 0, stream>>>(indptr, indices, vh, m, bh, k, c);
-    else csr_block_kernel<false><<<blocks, kThreads, 0, stream>>>(indptr, indices, vh, m, bh, k, c);
+    // natural row order, no row scaling, 64-bit B offsets (B's row count is
+    // not known here)
+    if (f16)
+      seg_block_kernel<true, false, true><<<blocks, kThreads, 0, stream>>>(
+          indptr, indices, vh, m, bh, k, c, nullptr, nullptr, nullptr);
+    else
+      seg_block_kernel<false, false, true><<<blocks, kThreads, 0, stream>>>(
+          indptr, indices, vh, m, bh, k, c, nullptr, nullptr, nullptr);
   } else {
     const int64_t n = (int64_t)m * k;
     const int blocks = (int)((n + 255) / 256);
@@ -806,12 +1001,22 @@ int launch_residual(const PlanView& v, const __half* bh, int32_t k, void* c, boo
                     cudaStream_t stream) {
   const int rows = v.n_windows * kBlockRows;
   const __half* rv = reinterpret_cast<const __half*>(v.res_val);
-  if (f16)
-    csr_block_kernel<true, true><<<v.n_windows, kThreads, 0, stream>>>(v.res_ptr, v.res_col, rv, rows,
-                                                                       bh, k, c, v.row_out, v.row_scale);
-  else
-    csr_block_kernel<false, true><<<v.n_windows, kThreads, 0, stream>>>(v.res_ptr, v.res_col, rv, rows,
-                                                                        bh, k, c, v.row_out, v.row_scale);
+  const bool wide = (int64_t)v.n_cols * k >= ((int64_t)1 << 31);
+  if (f16) {
+    if (wide)
+      seg_block_kernel<true, true, true><<<v.n_windows, kThreads, 0, stream>>>(
+          v.res_ptr, v.res_col, rv, rows, bh, k, c, v.row_out, v.row_scale, v.win_order);
+    else
+      seg_block_kernel<true, true, false><<<v.n_windows, kThreads, 0, stream>>>(
+          v.res_ptr, v.res_col, rv, rows, bh, k, c, v.row_out, v.row_scale, v.win_order);
+  } else {
+    if (wide)
+      seg_block_kernel<false, true, true><<<v.n_windows, kThreads, 0, stream>>>(
+          v.res_ptr, v.res_col, rv, rows, bh, k, c, v.row_out, v.row_scale, v.win_order);
+    else
+      seg_block_kernel<false, true, false><<<v.n_windows, kThreads, 0, stream>>>(
+          v.res_ptr, v.res_col, rv, rows, bh, k, c, v.row_out, v.row_scale, v.win_order);
+  }
   TRS_CUDA(cudaGetLastError());
   return TR_OK;
 }
@@ -944,15 +1149,19 @@ int launch_adjoint_sddmm(const tr_plan* p, const int32_t* a_indptr, const int32_
   const __half* g = reinterpret_cast<const __half*>(dc);
   const __half* h = reinterpret_cast<const __half*>(b);
   const __half* rv = reinterpret_cast<const __half*>(v.res_val);
-#define TRS_ADJ(F16, L)                                                                   \
-  adjoint_sddmm_kernel<F16, L><<<v.n_windows, kThreads, 0, stream>>>(                      \
-      v.res_ptr, v.res_col, rv, v.res_edge, rows, g, k, db, v.row_out, v.row_scale, h, dval)
+#define TRS_SEGADJ(F16, L, W)                                                             \
+  seg_adjoint_sddmm_kernel<F16, L, W><<<v.n_windows, kThreads, 0, stream>>>(               \
+      v.res_ptr, v.res_col, rv, v.res_edge, rows, g, k, db, v.row_out, v.row_scale, h, dval,   \
+      v.win_order)
+  const bool wide = (int64_t)v.n_cols * k >= ((int64_t)1 << 31);
   if (k > 64) {
-    if (f16) TRS_ADJ(true, 16); else TRS_ADJ(false, 16);
+    if (wide) { if (f16) TRS_SEGADJ(true, 16, true); else TRS_SEGADJ(false, 16, true); }
+    else { if (f16) TRS_SEGADJ(true, 16, false); else TRS_SEGADJ(false, 16, false); }
   } else {
-    if (f16) TRS_ADJ(true, 8); else TRS_ADJ(false, 8);
+    if (wide) { if (f16) TRS_SEGADJ(true, 8, true); else TRS_SEGADJ(false, 8, true); }
+    else { if (f16) TRS_SEGADJ(true, 8, false); else TRS_SEGADJ(false, 8, false); }
   }
-#undef TRS_ADJ
+#undef TRS_SEGADJ
   TRS_CUDA(cudaGetLastError());
   return TR_OK;
 }
