@@ -250,9 +250,9 @@ def dist_setup():
     return world, rank, local
 
 
-def workload():
+def workload(name=WORKLOAD):
     from trspmm import graphs
-    g, b = graphs.make_workload(WORKLOAD)
+    g, b = graphs.make_workload(name)
     dc = graphs.dense_features(g.n_rows, b.shape[1], "normal", seed=g.seed + 101)
     return g, b, dc
 
@@ -261,7 +261,7 @@ def run_reference(args):
     world, rank, _ = dist_setup()
     if rank != 0:
         return
-    g, b, dc = workload()
+    g, b, dc = workload(args.workload)
     gt = transpose_csr(g.indptr, g.indices, g.values, g.n_rows, g.n_cols)
     k = int(b.shape[1])
     step = CpuStep(g, gt, b, dc)
@@ -277,7 +277,7 @@ def run_reference(args):
             "steps": steps, "warmup": args.warmup, "ms_per_step": el / steps * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_nodes": g.n_rows, "nnz": g.nnz, "k": k,
+            "config": {"workload": args.workload, "n_nodes": g.n_rows, "nnz": g.nnz, "k": k,
                        "step": "forward + adjoint + SDDMM", "out": "f32"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": step.threads, "kind": "port",
                              "sample": f"full workload, {steps} steps"},
@@ -299,6 +299,10 @@ def main():
                     help="skip the autotuner and use the reference's routing (exact mode)")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the 512-graph batched comparison reported under extra")
+    ap.add_argument("--workload", default=WORKLOAD,
+                    choices=["large_routed", "route_mix", "gcn_diff", "plain_small"],
+                    help="graph of the step (default: the headline workload); the others "
+                         "are for profiling the routes they exercise")
     ap.add_argument("--plan-options", default=None,
                     help="JSON plan options to use instead of the autotuner's choice "
                          '(e.g. \'{"demote_below": 1000}\'), for profiling runs')
@@ -320,7 +324,7 @@ def main():
     dev = torch.device("cuda", local if world > 1 else 0)
     torch.cuda.set_device(dev)
 
-    g, b, dc = workload()
+    g, b, dc = workload(args.workload)
     k = int(b.shape[1])
     gt = transpose_csr(g.indptr, g.indices, g.values, g.n_rows, g.n_cols)
 
@@ -491,7 +495,7 @@ def main():
             "steps": args.steps, "warmup": warm, "ms_per_step": ms_max,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "n_nodes": g.n_rows, "nnz": g.nnz, "k": k,
+            "config": {"workload": args.workload, "n_nodes": g.n_rows, "nnz": g.nnz, "k": k,
                        "step": "forward + adjoint + SDDMM", "out": "f32",
                        "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"replicas{world}", "plan_options": opts},
