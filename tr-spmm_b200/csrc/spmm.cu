@@ -818,9 +818,10 @@ __device__ __forceinline__ float group_reduce_scatter8(float (&d)[8], int li) {
 // 16-byte chunk of dC[i] feeds dB[j] += a * dC[i] and the partial dot with
 // row j of B (held in registers, reloaded when the row changes), and the
 // group's 8 partial dots are reduce-scattered so that lane u (< 8) writes
-// dval for the batch's entry u.  K <= 128 (one feature chunk).
+// dval for the batch's entry u.  K <= 128 (one feature chunk).  Four CTAs
+// per SM (64 registers, a few bytes of spill) beat three without spill.
 template <bool F16OUT, int L, bool WIDE>
-__global__ void __launch_bounds__(kThreads, 3) seg_adjoint_sddmm_kernel(
+__global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
     const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
     const __half* __restrict__ values, const int32_t* __restrict__ edges, int M,
     const __half* __restrict__ G, int K, void* C, const int32_t* __restrict__ row_out,
