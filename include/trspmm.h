@@ -137,6 +137,42 @@ double tr_route_seconds(const tr_route* r);
 void tr_route_free(tr_route* r);
 
 /* ------------------------------------------------------------------------
+ * 2:4 matching statistics: how well each window's columns pair into 2:4
+ * groups (the reference's ablation extensions).  Host CSR in, counters out;
+ * deterministic (each window's columns in column-id order); counters are
+ * 64-bit.  Replaces
+ *   TR_MATCH_SLIDING  matching_utils.match_2to4
+ *                     (TR-source/Block/block_matching_window_para_dr.cpp:346-412)
+ *   TR_MATCH_HASH     matching_utils_hash.match_2to4_hash
+ *                     (TR-source/Block/block_matching_hash.cpp:373-420)
+ *   TR_MATCH_BUCKET   matching_utils_bucket.match_2to4_bucket
+ *                     (TR-source/Block/block_matching_bucket.cpp:430-480)
+ * dense_threshold and t_max apply to TR_MATCH_SLIDING (the others use their
+ * fixed constants).  Errors: window_size outside [1, 64], dense_threshold
+ * < 1 (the reference loops forever there), no rows or no columns.
+ * ---------------------------------------------------------------------- */
+enum { TR_MATCH_SLIDING = 0, TR_MATCH_HASH = 1, TR_MATCH_BUCKET = 2 };
+
+typedef struct tr_match_stats {
+  int32_t total_rows, total_cols;   /* total_cols = largest column index + 1 */
+  int64_t total_nnz;
+  double sparsity;
+  int32_t num_row_panels;           /* windows */
+  int32_t reserved;
+  int64_t num_groups;               /* 2:4 groups (num_sptc_groups of the sliding variant) */
+  int64_t num_tc_blocks;            /* dense 16x8 blocks (sliding variant; 0 otherwise) */
+  int64_t num_16x16_blocks;         /* groups packed four to a 16x16 block, per window */
+  int64_t block_padding_groups;
+  int64_t fine_fallback;            /* columns left unpaired */
+  int64_t coarse_fallback;          /* columns of pairs left ungrouped */
+  int64_t fake_zeros;               /* zero slots the groups carry */
+} tr_match_stats;
+
+int tr_match_2to4(const int32_t* indptr, const int32_t* indices, int32_t n_rows, int variant,
+                  int32_t window_size, int32_t dense_threshold, int32_t t_max,
+                  tr_match_stats* out);
+
+/* ------------------------------------------------------------------------
  * Device plan: the routed operand laid out for the fused sm_100a kernel.
  * Built once per graph (on the host from route tables, uploaded), reused
  * by every forward / adjoint call.

@@ -9,6 +9,8 @@ Contents
                      (TR-source/Block/block_online.cpp:545-871), via liboracle.so.
   ref_route()        the reference router itself, compiled from its source into
                      oracle/_ref (present only where it was built).
+  ref_match()        the reference's matching-stats functions (matching_utils,
+                     _hash, _bucket), compiled the same way.
   decode_tables()    rebuilds the matrix the 29 route tables encode (TC bitmap
                      sub-blocks, SPTC groups, CUDA parts), i.e. the operand the
                      reference's routed forward multiplies.
@@ -18,10 +20,12 @@ Contents
                      each CSR entry's value through the entry -> slot map.
   spmm_f64() / spmm_f16_f32() / sddmm_f64()   CSR arithmetic in C (OpenMP).
 """
-from .core import (TABLE_NAMES, route, ref_route, ref_available, decode_tables,
+from .core import (TABLE_NAMES, route, ref_route, ref_available, ref_match, ref_match_available,
+                   decode_tables,
                    decode_sptc_tiles, decode_plan, plan_value_of_entries, spmm_f64,
                    spmm_f16_f32, sddmm_f64, sddmm_f16_f32, max_threads, lib_path)
 
-__all__ = ["TABLE_NAMES", "route", "ref_route", "ref_available", "decode_tables",
+__all__ = ["TABLE_NAMES", "route", "ref_route", "ref_available", "ref_match",
+           "ref_match_available", "decode_tables",
            "decode_sptc_tiles", "decode_plan", "plan_value_of_entries", "spmm_f64", "spmm_f16_f32", "sddmm_f64", "sddmm_f16_f32", "max_threads",
            "lib_path"]

@@ -153,6 +153,37 @@ def ref_route(indptr, indices, values, *args, quiet=True):
     return [t.numpy() for t in out]
 
 
+def ref_match_available(module="matching_utils"):
+    return bool(glob.glob(os.path.join(_ref_dir(), module + "*.so")))
+
+
+def ref_match(module, func, indptr, indices, values, quiet=True, **kw):
+    """A matching-stats function of the reference compiled from its own
+    source (oracle/_ref: matching_utils.match_2to4, matching_utils_hash.
+    match_2to4_hash, matching_utils_bucket.match_2to4_bucket); returns its
+    dict.  The reference prints a summary box on stdout; ``quiet`` drops it."""
+    import importlib
+    if _ref_dir() not in sys.path:
+        sys.path.insert(0, _ref_dir())
+    mod = importlib.import_module(module)
+    rp = np.ascontiguousarray(indptr, dtype=np.int32)
+    ci = np.ascontiguousarray(indices, dtype=np.int32)
+    vv = np.ascontiguousarray(values, dtype=np.float32)
+    if quiet:
+        sys.stdout.flush()
+        fd = os.dup(1)
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(devnull, 1)
+    try:
+        return dict(getattr(mod, func)(rp, ci, vv, **kw))
+    finally:
+        if quiet:
+            sys.stdout.flush()
+            os.dup2(fd, 1)
+            os.close(fd)
+            os.close(devnull)
+
+
 def _half(x):
     return np.asarray(x, dtype=np.float32).astype(np.float16)
 

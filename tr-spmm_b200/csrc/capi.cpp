@@ -17,6 +17,10 @@
 
 namespace trs {
 
+int match_2to4(const int32_t* indptr, const int32_t* indices, int32_t n_rows, int variant,
+               int32_t window_size, int32_t dense_threshold, int32_t t_max, tr_match_stats* out,
+               std::string& err);
+
 namespace {
 thread_local std::string g_error;
 }
@@ -234,6 +238,17 @@ int tr_route_tc_device_noalloc(const int32_t* d_indptr, const int32_t* d_indices
   return route_tc_gpu_noalloc(d_indptr, d_indices, d_values, n_rows, gp, t_column, t_binary,
                               t_value, t_block_offset, cap_sub, cap_val, n_sub_out, n_val_out,
                               (cudaStream_t)stream);
+}
+
+int tr_match_2to4(const int32_t* indptr, const int32_t* indices, int32_t n_rows, int variant,
+                  int32_t window_size, int32_t dense_threshold, int32_t t_max,
+                  tr_match_stats* out) {
+  if (!indptr || !out || (n_rows > 0 && indptr[n_rows] > 0 && !indices))
+    return fail(TR_ERR_ARG, "null argument");
+  std::string err;
+  const int rc = match_2to4(indptr, indices, n_rows, variant, window_size, dense_threshold, t_max,
+                            out, err);
+  return rc ? fail(rc, err) : TR_OK;
 }
 
 double tr_route_seconds(const tr_route* r) { return r ? r->t.seconds : 0.0; }

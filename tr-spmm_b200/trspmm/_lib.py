@@ -21,7 +21,7 @@ TR_ROUTE_COMPAT, TR_ROUTE_EXACT = 0, 1
 EXPORTED = [
     "tr_last_error", "tr_version", "tr_device_info",
     "tr_route_build", "tr_route_tc_device", "tr_route_tc_device_noalloc", "tr_route_table",
-    "tr_route_seconds", "tr_route_free",
+    "tr_route_seconds", "tr_route_free", "tr_match_2to4",
     "tr_plan_from_tables", "tr_plan_from_csr", "tr_plan_build", "tr_plan_build_host",
     "tr_host_plan_array", "tr_host_plan_upload", "tr_host_plan_free", "tr_plan_info_get",
     "tr_plan_free", "tr_spmm_csr", "tr_spmm_routed", "tr_plan_set_values", "tr_sddmm_csr",
@@ -29,6 +29,20 @@ EXPORTED = [
     "tr_forward_fp16_tcu_cuda_sptc_mma_parallel_online", "tr_forward_fp16_sptc_online",
     "tr_forward_fp16_sptc_mma_online", "tr_forward_fp16_sptc_mma_packed_online",
 ]
+
+
+TR_MATCH_SLIDING, TR_MATCH_HASH, TR_MATCH_BUCKET = 0, 1, 2
+
+
+class MatchStats(ctypes.Structure):
+    """tr_match_stats (include/trspmm.h)."""
+    _fields_ = [("total_rows", ctypes.c_int32), ("total_cols", ctypes.c_int32),
+                ("total_nnz", ctypes.c_int64), ("sparsity", ctypes.c_double),
+                ("num_row_panels", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("num_groups", ctypes.c_int64), ("num_tc_blocks", ctypes.c_int64),
+                ("num_16x16_blocks", ctypes.c_int64), ("block_padding_groups", ctypes.c_int64),
+                ("fine_fallback", ctypes.c_int64), ("coarse_fallback", ctypes.c_int64),
+                ("fake_zeros", ctypes.c_int64)]
 
 
 class TrError(RuntimeError):
@@ -92,6 +106,7 @@ def lib():
     L.tr_route_tc_device.argtypes = [P, P, P, I32, ctypes.POINTER(RouteParams), P]
     L.tr_route_tc_device_noalloc.argtypes = [P, P, P, I32, ctypes.POINTER(RouteParams), P, P, P, P,
                                              I64, I64, P, P, P]
+    L.tr_match_2to4.argtypes = [P, P, I32, ctypes.c_int, I32, I32, I32, ctypes.POINTER(MatchStats)]
     L.tr_route_seconds.restype = ctypes.c_double
     L.tr_route_seconds.argtypes = [P]
     L.tr_route_free.argtypes = [P]

@@ -19,8 +19,9 @@ import os
 import numpy as np
 
 from . import _lib
-from ._lib import (TR_OUT_F16, TR_OUT_F32, TR_ROUTE_ALL, TR_ROUTE_COMPAT, TR_ROUTE_EXACT,
-                   PlanInfo, PlanOpts, RouteParams, Tables, check, lib)
+from ._lib import (TR_MATCH_BUCKET, TR_MATCH_HASH, TR_MATCH_SLIDING, TR_OUT_F16, TR_OUT_F32,
+                   TR_ROUTE_ALL, TR_ROUTE_COMPAT, TR_ROUTE_EXACT, MatchStats, PlanInfo, PlanOpts,
+                   RouteParams, Tables, check, lib)
 
 TABLE_NAMES = [
     "t_row_offset", "t_block_offset", "t_column", "t_value", "t_window_row", "t_atomic",
@@ -400,3 +401,20 @@ def sddmm_csr(indptr, indices, x, y, out=None, stream=None):
                              ctypes.c_void_p(y.data_ptr()), int(x.shape[1]),
                              ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(s)))
     return out
+
+
+MATCH_VARIANTS = {"sliding": TR_MATCH_SLIDING, "hash": TR_MATCH_HASH, "bucket": TR_MATCH_BUCKET}
+
+
+def match_2to4(indptr, indices, variant="sliding", window_size=16, dense_threshold=8, t_max=8):
+    """2:4 matching statistics of a host CSR (tr_match_2to4): how the columns
+    of each window pair into 1:2 pairs and 2:4 groups, and, for the sliding
+    variant, which leftover columns form dense 16x8 blocks.  Returns a dict
+    with every counter of tr_match_stats (num_groups counts 2:4 groups)."""
+    rp = np.ascontiguousarray(indptr, dtype=np.int32)
+    ci = np.ascontiguousarray(indices, dtype=np.int32)
+    st = MatchStats()
+    check(lib().tr_match_2to4(_vp(rp), _vp(ci), int(rp.shape[0] - 1), int(MATCH_VARIANTS[variant]),
+                              int(window_size), int(dense_threshold), int(t_max),
+                              ctypes.byref(st)))
+    return {name: getattr(st, name) for name, _ in MatchStats._fields_ if name != "reserved"}
