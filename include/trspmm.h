@@ -262,6 +262,16 @@ int tr_plan_build_host(const int32_t* indptr, const int32_t* indices, const floa
 int tr_host_plan_array(const tr_host_plan* h, int idx, const void** data, int64_t* count);
 int tr_host_plan_upload(const tr_host_plan* h, tr_plan** out);
 void tr_host_plan_free(tr_host_plan* h);
+/* Plan files: a host plan written to disk once per graph so later runs skip
+ * routing and layout (a plan cache; the reference routes on every call,
+ * TR-source/spmm/tr_csr_fp16/mdataset2_online.py:100-153).  Versioned binary
+ * with a checksum; the file is written beside `path` and renamed into place.
+ * Loading refuses (with the reason) files that are not plan files, damaged
+ * or truncated ones, other versions and arrays whose sizes or index ranges
+ * are inconsistent.  Host only (no device needed); upload with
+ * tr_host_plan_upload. */
+int tr_host_plan_save(const tr_host_plan* h, const char* path);
+int tr_host_plan_load(const char* path, tr_host_plan** out);
 int tr_plan_info_get(const tr_plan* p, tr_plan_info* info);
 void tr_plan_free(tr_plan* p);
 

@@ -17,6 +17,9 @@
 
 namespace trs {
 
+int save_host_plan(const HostPlan& hp, const char* path, std::string& err);
+int load_host_plan(const char* path, HostPlan& hp, std::string& err);
+
 int match_2to4(const int32_t* indptr, const int32_t* indices, int32_t n_rows, int variant,
                int32_t window_size, int32_t dense_threshold, int32_t t_max, tr_match_stats* out,
                std::string& err);
@@ -249,6 +252,23 @@ int tr_match_2to4(const int32_t* indptr, const int32_t* indices, int32_t n_rows,
   const int rc = match_2to4(indptr, indices, n_rows, variant, window_size, dense_threshold, t_max,
                             out, err);
   return rc ? fail(rc, err) : TR_OK;
+}
+
+int tr_host_plan_save(const tr_host_plan* h, const char* path) {
+  if (!h || !path) return fail(TR_ERR_ARG, "null argument");
+  std::string err;
+  const int rc = save_host_plan(h->hp, path, err);
+  return rc ? fail(rc, err) : TR_OK;
+}
+
+int tr_host_plan_load(const char* path, tr_host_plan** out) {
+  if (!path || !out) return fail(TR_ERR_ARG, "null argument");
+  std::unique_ptr<tr_host_plan> h(new tr_host_plan());
+  std::string err;
+  const int rc = load_host_plan(path, h->hp, err);
+  if (rc) return fail(rc, err);
+  *out = h.release();
+  return TR_OK;
 }
 
 double tr_route_seconds(const tr_route* r) { return r ? r->t.seconds : 0.0; }

@@ -23,7 +23,8 @@ EXPORTED = [
     "tr_route_build", "tr_route_tc_device", "tr_route_tc_device_noalloc", "tr_route_table",
     "tr_route_seconds", "tr_route_free", "tr_match_2to4",
     "tr_plan_from_tables", "tr_plan_from_csr", "tr_plan_build", "tr_plan_build_host",
-    "tr_host_plan_array", "tr_host_plan_upload", "tr_host_plan_free", "tr_plan_info_get",
+    "tr_host_plan_array", "tr_host_plan_upload", "tr_host_plan_free", "tr_host_plan_save",
+    "tr_host_plan_load", "tr_plan_info_get",
     "tr_plan_free", "tr_spmm_csr", "tr_spmm_routed", "tr_plan_set_values", "tr_sddmm_csr",
     "tr_adjoint_sddmm",
     "tr_forward_fp16_tcu_cuda_sptc_mma_parallel_online", "tr_forward_fp16_sptc_online",
@@ -119,6 +120,8 @@ def lib():
     L.tr_host_plan_array.argtypes = [P, ctypes.c_int, ctypes.POINTER(P), ctypes.POINTER(I64)]
     L.tr_host_plan_upload.argtypes = [P, P]
     L.tr_host_plan_free.argtypes = [P]
+    L.tr_host_plan_save.argtypes = [P, ctypes.c_char_p]
+    L.tr_host_plan_load.argtypes = [ctypes.c_char_p, ctypes.POINTER(P)]
     L.tr_plan_set_values.argtypes = [P, P, I64, P]
     L.tr_sddmm_csr.argtypes = [P, P, I32, I32, I64, P, P, I32, P, P]
     L.tr_adjoint_sddmm.argtypes = [P, P, P, I32, I64, P, P, I32, P, ctypes.c_int, P, P]

@@ -30,15 +30,24 @@ class RoutedAdjacency:
     """Sparse A (n_rows x n_cols, CSR) with its forward and adjoint plans."""
 
     def __init__(self, indptr, indices, values, n_rows, n_cols, device="cuda",
-                 row_scale=True, promote_min=2, reorder=False, **route_kw):
+                 row_scale=True, promote_min=2, reorder=False, plan_cache=None, **route_kw):
+        """plan_cache: None builds both plans; True or a directory takes them
+        from the on-disk plan cache (trspmm.plan_cache), routing once per
+        graph."""
         indptr = np.ascontiguousarray(indptr, dtype=np.int32)
         indices = np.ascontiguousarray(indices, dtype=np.int32)
         values = np.ascontiguousarray(values, dtype=np.float32)
         self.n_rows, self.n_cols = int(n_rows), int(n_cols)
         self.nnz = int(indices.size)
         kw = dict(row_scale=row_scale, promote_min=promote_min, reorder=reorder, **route_kw)
-        self.fwd = Plan.build(indptr, indices, values, n_rows, n_cols, transpose=False, **kw)
-        self.adj = Plan.build(indptr, indices, values, n_rows, n_cols, transpose=True, **kw)
+        if plan_cache:
+            from .plan_cache import cached_plan
+            d = None if plan_cache is True else str(plan_cache)
+            self.fwd = cached_plan(indptr, indices, values, n_rows, n_cols, d, transpose=False, **kw)
+            self.adj = cached_plan(indptr, indices, values, n_rows, n_cols, d, transpose=True, **kw)
+        else:
+            self.fwd = Plan.build(indptr, indices, values, n_rows, n_cols, transpose=False, **kw)
+            self.adj = Plan.build(indptr, indices, values, n_rows, n_cols, transpose=True, **kw)
         self.device = torch.device(device)
         self.indptr = torch.from_numpy(indptr).to(self.device)
         self.indices = torch.from_numpy(indices).to(self.device)

@@ -360,20 +360,27 @@ def host_plan(indptr, indices, values, n_rows, n_cols, row_scale=False, promote_
     check(L.tr_plan_build_host(_vp(rp), _vp(ci), _vp(vv), int(n_rows), int(n_cols),
                                ctypes.byref(prm), ctypes.byref(opts), ctypes.byref(h)))
     try:
-        out = {}
-        for i, (name, dt) in enumerate(HOST_PLAN_ARRAYS):
-            data = ctypes.c_void_p()
-            n = ctypes.c_int64()
-            check(L.tr_host_plan_array(h, i, ctypes.byref(data), ctypes.byref(n)))
-            if n.value == 0:
-                out[name] = np.zeros(0, dtype=dt)
-            else:
-                nbytes = n.value * np.dtype(dt).itemsize
-                buf = (ctypes.c_char * nbytes).from_address(data.value)
-                out[name] = np.frombuffer(buf, dtype=dt, count=n.value).copy()
+        out = host_plan_arrays(h)
     finally:
         L.tr_host_plan_free(h)
     out["n_rows"], out["n_cols"] = (n_cols, n_rows) if transpose else (n_rows, n_cols)
+    return out
+
+
+def host_plan_arrays(h):
+    """Copies of a host plan handle's arrays (tr_host_plan_array), by name."""
+    L = lib()
+    out = {}
+    for i, (name, dt) in enumerate(HOST_PLAN_ARRAYS):
+        data = ctypes.c_void_p()
+        n = ctypes.c_int64()
+        check(L.tr_host_plan_array(h, i, ctypes.byref(data), ctypes.byref(n)))
+        if n.value == 0:
+            out[name] = np.zeros(0, dtype=dt)
+        else:
+            nbytes = n.value * np.dtype(dt).itemsize
+            buf = (ctypes.c_char * nbytes).from_address(data.value)
+            out[name] = np.frombuffer(buf, dtype=dt, count=n.value).copy()
     return out
 
 
