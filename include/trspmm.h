@@ -147,11 +147,16 @@ void tr_route_free(tr_route* r);
  *                     (TR-source/Block/block_matching_hash.cpp:373-420)
  *   TR_MATCH_BUCKET   matching_utils_bucket.match_2to4_bucket
  *                     (TR-source/Block/block_matching_bucket.cpp:430-480)
- * dense_threshold and t_max apply to TR_MATCH_SLIDING (the others use their
- * fixed constants).  Errors: window_size outside [1, 64], dense_threshold
- * < 1 (the reference loops forever there), no rows or no columns.
+ *   TR_MATCH_ONLINE   the host restatement of matching_utils_online.match_2to4_online
+ *                     (TR-source/Block/block_matching_online.cu:554-668): the
+ *                     sliding variant's decisions on 16-row windows, 32 slots per
+ *                     group; tr_match_2to4_online runs it on the GPU.
+ * dense_threshold and t_max apply to TR_MATCH_SLIDING and TR_MATCH_ONLINE
+ * (the others use their fixed constants).  Errors: window_size outside
+ * [1, 64] (exactly 16 for TR_MATCH_ONLINE), dense_threshold < 1 (the
+ * reference loops forever there), no rows or no columns.
  * ---------------------------------------------------------------------- */
-enum { TR_MATCH_SLIDING = 0, TR_MATCH_HASH = 1, TR_MATCH_BUCKET = 2 };
+enum { TR_MATCH_SLIDING = 0, TR_MATCH_HASH = 1, TR_MATCH_BUCKET = 2, TR_MATCH_ONLINE = 3 };
 
 typedef struct tr_match_stats {
   int32_t total_rows, total_cols;   /* total_cols = largest column index + 1 */
@@ -166,11 +171,24 @@ typedef struct tr_match_stats {
   int64_t fine_fallback;            /* columns left unpaired */
   int64_t coarse_fallback;          /* columns of pairs left ungrouped */
   int64_t fake_zeros;               /* zero slots the groups carry */
+  int64_t dense_to_tc_cols;         /* pool columns in dense blocks (sliding / online) */
+  int64_t dense_to_sptc_cols;       /* pool columns in 2:4 fallback groups (sliding / online) */
 } tr_match_stats;
 
 int tr_match_2to4(const int32_t* indptr, const int32_t* indices, int32_t n_rows, int variant,
                   int32_t window_size, int32_t dense_threshold, int32_t t_max,
                   tr_match_stats* out);
+/* TR_MATCH_ONLINE on the GPU (replaces matching_utils_online.match_2to4_online,
+ * TR-source/Block/block_matching_online.cu:554-668): host CSR in; like the
+ * reference's entry point it copies the matrix to the current device, runs
+ * one CTA per 16-row window and waits for the result (this entry point
+ * allocates device memory and synchronises).  Columns are taken in id order
+ * (deterministic); windows with more than 2048 entries are counted on the
+ * host by the same rules (the reference drops their columns past 2048).
+ * window_size must be 16.  The result equals tr_match_2to4(TR_MATCH_ONLINE). */
+int tr_match_2to4_online(const int32_t* indptr, const int32_t* indices, int32_t n_rows,
+                         int32_t window_size, int32_t dense_threshold, int32_t t_max,
+                         tr_match_stats* out);
 
 /* ------------------------------------------------------------------------
  * Device plan: the routed operand laid out for the fused sm_100a kernel.

@@ -111,3 +111,21 @@ def test_rejects_bad_arguments():
     with pytest.raises(trspmm.TrError, match="empty matrix"):
         matching_utils_hash.match_2to4_hash(np.zeros(5, np.int32), np.zeros(0, np.int32),
                                             np.zeros(0, np.float32))
+
+
+@pytest.mark.parametrize("name", ["chung_lu_4096", "route_mix_2048", "sbm_6000", "dup_300x200"])
+def test_online_rules_are_the_sliding_decisions(name):
+    """The online variant (host restatement) takes the sliding variant's
+    decisions; only the group size behind fake_zeros differs (32 slots,
+    against 2 x window rows), which shows in windows of fewer than 16 rows."""
+    g = _graph(name)
+    a = trspmm.match_2to4(g.indptr, g.indices, "sliding", 16)
+    b = trspmm.match_2to4(g.indptr, g.indices, "online", 16)
+    for k in a:
+        if k != "fake_zeros":
+            assert a[k] == b[k], k
+    if g.n_rows % 16 == 0:
+        assert a["fake_zeros"] == b["fake_zeros"]
+    assert b["dense_to_tc_cols"] == b["num_tc_blocks"] * 8
+    with pytest.raises(trspmm.TrError, match="16-row windows"):
+        trspmm.match_2to4(g.indptr, g.indices, "online", 8)

@@ -17,6 +17,9 @@
 
 namespace trs {
 
+int match_online_gpu(const int32_t* indptr, const int32_t* indices, int32_t n_rows,
+                     int32_t dense_threshold, int32_t t_max, tr_match_stats* st,
+                     std::string& err);
 int save_host_plan(const HostPlan& hp, const char* path, std::string& err);
 int load_host_plan(const char* path, HostPlan& hp, std::string& err);
 
@@ -251,6 +254,17 @@ int tr_match_2to4(const int32_t* indptr, const int32_t* indices, int32_t n_rows,
   std::string err;
   const int rc = match_2to4(indptr, indices, n_rows, variant, window_size, dense_threshold, t_max,
                             out, err);
+  return rc ? fail(rc, err) : TR_OK;
+}
+
+int tr_match_2to4_online(const int32_t* indptr, const int32_t* indices, int32_t n_rows,
+                         int32_t window_size, int32_t dense_threshold, int32_t t_max,
+                         tr_match_stats* out) {
+  if (!indptr || !out || (n_rows > 0 && indptr[n_rows] > 0 && !indices))
+    return fail(TR_ERR_ARG, "null argument");
+  if (window_size != 16) return fail(TR_ERR_ARG, "the online matcher uses 16-row windows");
+  std::string err;
+  const int rc = match_online_gpu(indptr, indices, n_rows, dense_threshold, t_max, out, err);
   return rc ? fail(rc, err) : TR_OK;
 }
 

@@ -16,6 +16,13 @@
 //            (matching_utils_bucket.match_2to4_bucket): columns split by
 //            whether rows 0-7 or 8-15 hold more entries, matched across
 //            buckets first, 16-candidate look-aheads.
+//   online   TR-source/Block/block_matching_online.cu:112-411
+//            (matching_utils_online.match_2to4_online, a CUDA kernel): the
+//            sliding variant's decisions over 16-row windows, with each 2:4
+//            group counted as 32 slots and the pool's split between dense
+//            blocks and 2:4 groups reported.  The reference orders a
+//            window's columns by hash-slot arrival (not deterministic); here
+//            they are in id order, on the host and in match_gpu.cu.
 //
 // Every variant encodes a window's column as a 16-bit row mask with the
 // reference's truncation (rows past the 16th set no bit) and sorts the
@@ -48,6 +55,7 @@ struct MPair {
 struct WinStats {
   int64_t groups = 0, tc_blocks = 0, blocks16 = 0, pad_groups = 0;
   int64_t fine_fb = 0, coarse_fb = 0, fake_zeros = 0;
+  int64_t to_tc = 0, to_sptc = 0;      // pool columns routed to dense blocks / to 2:4 groups
 };
 
 inline int popc16(uint32_t x) { return __builtin_popcount(x & 0xFFFFu); }
@@ -113,8 +121,10 @@ void tail_blocks(WinStats& s) {
   s.pad_groups += ((s.groups + 3) / 4) * 4 - s.groups;
 }
 
-// block_matching_window_para_dr.cpp:80-243
-WinStats match_sliding(const std::vector<MCol>& c, int win_rows, int dense_threshold, int t_max) {
+// block_matching_window_para_dr.cpp:80-243.  `slots` is what one 2:4 group
+// holds: 2 * window rows in the sliding variant, always 32 in the CUDA
+// variant (block_matching_online.cu:318-320, :378).
+WinStats match_sliding(const std::vector<MCol>& c, int slots, int dense_threshold, int t_max) {
   WinStats s;
   const int n = (int)c.size();
   std::vector<char> used(n, 0);
@@ -143,7 +153,7 @@ WinStats match_sliding(const std::vector<MCol>& c, int win_rows, int dense_thres
     if (j < std::min(i + 1 + 1024, np)) {
       pused[j] = 1;
       s.groups++;
-      s.fake_zeros += (int64_t)win_rows * 2 - (pairs[i].nnz + pairs[j].nnz);
+      s.fake_zeros += slots - (pairs[i].nnz + pairs[j].nnz);
     } else {
       if (pairs[i].c1 >= 0) pool.push_back(pairs[i].c1);
       if (pairs[i].c2 >= 0) pool.push_back(pairs[i].c2);
@@ -153,12 +163,14 @@ WinStats match_sliding(const std::vector<MCol>& c, int win_rows, int dense_thres
   const int64_t nd = (int64_t)pool.size();
   const int64_t full = nd / dense_threshold;
   s.tc_blocks = full;
+  s.to_tc = full * dense_threshold;
+  s.to_sptc = nd - s.to_tc;
   int64_t idx = full * dense_threshold;
   while (idx < nd) {                      // groups of at most two real columns
     int64_t g_nnz = nnz_of(c, pool[idx++]);
     if (idx < nd) g_nnz += nnz_of(c, pool[idx++]);
     s.groups++;
-    s.fake_zeros += (int64_t)win_rows * 2 - g_nnz;
+    s.fake_zeros += slots - g_nnz;
   }
   tail_blocks(s);
   return s;
@@ -325,8 +337,12 @@ int match_2to4(const int32_t* indptr, const int32_t* indices, int32_t n_rows, in
     err = "dense_threshold must be at least 1";
     return TR_ERR_ARG;
   }
-  if (variant < TR_MATCH_SLIDING || variant > TR_MATCH_BUCKET) {
+  if (variant < TR_MATCH_SLIDING || variant > TR_MATCH_ONLINE) {
     err = "unknown matching variant";
+    return TR_ERR_ARG;
+  }
+  if (variant == TR_MATCH_ONLINE && (window_size != 16 || dense_threshold < 1)) {
+    err = "the online variant uses 16-row windows and dense_threshold >= 1";
     return TR_ERR_ARG;
   }
   const int64_t nnz = n_rows > 0 ? indptr[n_rows] : 0;
@@ -351,9 +367,10 @@ int match_2to4(const int32_t* indptr, const int32_t* indices, int32_t n_rows, in
         window_columns(indptr, indices, r0, r1, scratch, cols);
         if (cols.empty()) continue;
         const int wr = r1 - r0;
-        ws[w] = variant == TR_MATCH_SLIDING ? match_sliding(cols, wr, dense_threshold, t_max)
-                : variant == TR_MATCH_HASH  ? match_hash(cols, wr)
-                                            : match_bucket(cols);
+        ws[w] = variant == TR_MATCH_SLIDING ? match_sliding(cols, 2 * wr, dense_threshold, t_max)
+                : variant == TR_MATCH_ONLINE ? match_sliding(cols, 32, dense_threshold, t_max)
+                : variant == TR_MATCH_HASH   ? match_hash(cols, wr)
+                                             : match_bucket(cols);
       }
     }
   };
@@ -380,9 +397,27 @@ int match_2to4(const int32_t* indptr, const int32_t* indices, int32_t n_rows, in
     s.fine_fallback += w.fine_fb;
     s.coarse_fallback += w.coarse_fb;
     s.fake_zeros += w.fake_zeros;
+    s.dense_to_tc_cols += w.to_tc;
+    s.dense_to_sptc_cols += w.to_sptc;
   }
   *out = s;
   return TR_OK;
+}
+
+// One 16-row window of the online variant on the host (the GPU matcher
+// hands back windows too large for its shared memory).  Counters in the
+// order groups, tc_blocks, fine_fb, coarse_fb, fake_zeros, to_tc, to_sptc.
+void match_online_window(const int32_t* indptr, const int32_t* indices, int32_t n_rows, int w,
+                         int32_t dense_threshold, int32_t t_max, int64_t* out7) {
+  std::vector<std::pair<int32_t, uint16_t>> scratch;
+  std::vector<MCol> cols;
+  const int32_t r0 = w * 16, r1 = std::min(r0 + 16, n_rows);
+  window_columns(indptr, indices, r0, r1, scratch, cols);
+  WinStats s;
+  if (!cols.empty()) s = match_sliding(cols, 32, dense_threshold, t_max);
+  const int64_t v[7] = {s.groups, s.tc_blocks, s.fine_fb, s.coarse_fb, s.fake_zeros, s.to_tc,
+                        s.to_sptc};
+  for (int i = 0; i < 7; ++i) out7[i] = v[i];
 }
 
 }  // namespace trs

@@ -21,7 +21,7 @@ TR_ROUTE_COMPAT, TR_ROUTE_EXACT = 0, 1
 EXPORTED = [
     "tr_last_error", "tr_version", "tr_device_info",
     "tr_route_build", "tr_route_tc_device", "tr_route_tc_device_noalloc", "tr_route_table",
-    "tr_route_seconds", "tr_route_free", "tr_match_2to4",
+    "tr_route_seconds", "tr_route_free", "tr_match_2to4", "tr_match_2to4_online",
     "tr_plan_from_tables", "tr_plan_from_csr", "tr_plan_build", "tr_plan_build_host",
     "tr_host_plan_array", "tr_host_plan_upload", "tr_host_plan_free", "tr_host_plan_save",
     "tr_host_plan_load", "tr_plan_info_get",
@@ -32,7 +32,7 @@ EXPORTED = [
 ]
 
 
-TR_MATCH_SLIDING, TR_MATCH_HASH, TR_MATCH_BUCKET = 0, 1, 2
+TR_MATCH_SLIDING, TR_MATCH_HASH, TR_MATCH_BUCKET, TR_MATCH_ONLINE = 0, 1, 2, 3
 
 
 class MatchStats(ctypes.Structure):
@@ -43,7 +43,8 @@ class MatchStats(ctypes.Structure):
                 ("num_groups", ctypes.c_int64), ("num_tc_blocks", ctypes.c_int64),
                 ("num_16x16_blocks", ctypes.c_int64), ("block_padding_groups", ctypes.c_int64),
                 ("fine_fallback", ctypes.c_int64), ("coarse_fallback", ctypes.c_int64),
-                ("fake_zeros", ctypes.c_int64)]
+                ("fake_zeros", ctypes.c_int64), ("dense_to_tc_cols", ctypes.c_int64),
+                ("dense_to_sptc_cols", ctypes.c_int64)]
 
 
 class TrError(RuntimeError):
@@ -108,6 +109,7 @@ def lib():
     L.tr_route_tc_device_noalloc.argtypes = [P, P, P, I32, ctypes.POINTER(RouteParams), P, P, P, P,
                                              I64, I64, P, P, P]
     L.tr_match_2to4.argtypes = [P, P, I32, ctypes.c_int, I32, I32, I32, ctypes.POINTER(MatchStats)]
+    L.tr_match_2to4_online.argtypes = [P, P, I32, I32, I32, I32, ctypes.POINTER(MatchStats)]
     L.tr_route_seconds.restype = ctypes.c_double
     L.tr_route_seconds.argtypes = [P]
     L.tr_route_free.argtypes = [P]

@@ -19,7 +19,8 @@ import os
 import numpy as np
 
 from . import _lib
-from ._lib import (TR_MATCH_BUCKET, TR_MATCH_HASH, TR_MATCH_SLIDING, TR_OUT_F16, TR_OUT_F32,
+from ._lib import (TR_MATCH_BUCKET, TR_MATCH_HASH, TR_MATCH_ONLINE, TR_MATCH_SLIDING, TR_OUT_F16,
+                   TR_OUT_F32,
                    TR_ROUTE_ALL, TR_ROUTE_COMPAT, TR_ROUTE_EXACT, MatchStats, PlanInfo, PlanOpts,
                    RouteParams, Tables, check, lib)
 
@@ -410,7 +411,8 @@ def sddmm_csr(indptr, indices, x, y, out=None, stream=None):
     return out
 
 
-MATCH_VARIANTS = {"sliding": TR_MATCH_SLIDING, "hash": TR_MATCH_HASH, "bucket": TR_MATCH_BUCKET}
+MATCH_VARIANTS = {"sliding": TR_MATCH_SLIDING, "hash": TR_MATCH_HASH, "bucket": TR_MATCH_BUCKET,
+                  "online": TR_MATCH_ONLINE}
 
 
 def match_2to4(indptr, indices, variant="sliding", window_size=16, dense_threshold=8, t_max=8):
@@ -424,4 +426,15 @@ def match_2to4(indptr, indices, variant="sliding", window_size=16, dense_thresho
     check(lib().tr_match_2to4(_vp(rp), _vp(ci), int(rp.shape[0] - 1), int(MATCH_VARIANTS[variant]),
                               int(window_size), int(dense_threshold), int(t_max),
                               ctypes.byref(st)))
+    return {name: getattr(st, name) for name, _ in MatchStats._fields_ if name != "reserved"}
+
+
+def match_2to4_online(indptr, indices, window_size=16, dense_threshold=8, t_max=8):
+    """The online variant's statistics computed on the GPU
+    (tr_match_2to4_online); equal to match_2to4(..., "online")."""
+    rp = np.ascontiguousarray(indptr, dtype=np.int32)
+    ci = np.ascontiguousarray(indices, dtype=np.int32)
+    st = MatchStats()
+    check(lib().tr_match_2to4_online(_vp(rp), _vp(ci), int(rp.shape[0] - 1), int(window_size),
+                                     int(dense_threshold), int(t_max), ctypes.byref(st)))
     return {name: getattr(st, name) for name, _ in MatchStats._fields_ if name != "reserved"}
