@@ -30,7 +30,9 @@ step is timed alone with CUDA events on its stream.
               res_nnz*(4+2) + (M+1)*4 + N*K*2 + M*K*4 (that one is also
               reported in extra.forward_residual_roofline)
   cpu_baseline / --impl reference: the oracle's C restatement of the same
-              step (FP16 operands, FP32 accumulation, OpenMP on all host cores)
+              step (FP16 operands, FP32 accumulation, OpenMP on all host cores);
+              extra.cpu_torch_sparse_forward: the forward alone with
+              torch.sparse CSR (FP32) on all host cores
   extra       the same step with the plain single-route CSR kernel (forward on
               A, adjoint on a CSR of A^T, same SDDMM), per-pass times and the
               autotuner's table
@@ -164,6 +166,33 @@ def transpose_csr(indptr, indices, values, n_rows, n_cols):
     a = sp.csr_matrix((values, indices, indptr), shape=(n_rows, n_cols)).T.tocsr()
     a.sort_indices()
     return a.indptr.astype(np.int32), a.indices.astype(np.int32), a.data.astype(np.float32)
+
+
+def torch_sparse_cpu_forward(g, b, reps=5):
+    """C = A.B with torch.sparse CSR on all host cores (FP32: the CPU CSR
+    matmul has no FP16 kernel): the CPU baseline the survey names, reported
+    beside the oracle's whole-step baseline.  Median of `reps` after one
+    warm-up."""
+    import torch
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    import warnings
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")            # "beta state" notice of sparse CSR
+        A = torch.sparse_csr_tensor(torch.from_numpy(g.indptr.astype(np.int64)),
+                                    torch.from_numpy(g.indices.astype(np.int64)),
+                                    torch.from_numpy(g.values.astype(np.float32)),
+                                    size=(g.n_rows, g.n_cols), check_invariants=False)
+    B = torch.from_numpy(np.asarray(b, dtype=np.float32))
+    A @ B
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        A @ B
+        ts.append(time.perf_counter() - t0)
+    t = float(np.median(ts))
+    return {"value": 2.0 * g.nnz * B.shape[1] / t / 1e12, "unit": UNIT, "cores": threads,
+            "dtype": "f32", "op": "forward C = A.B, torch.sparse CSR", "ms": t * 1e3}
 
 
 class CpuStep:
@@ -458,7 +487,9 @@ def main():
     res_gbs = res_bytes / (res_ms * 1e-3) / 1e9
     sbytes = step_bytes(g.nnz, g.n_rows, g.n_cols, k)
     cpu = None
+    cpu_torch = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu_torch = torch_sparse_cpu_forward(g, b)
         cs = CpuStep(g, gt, b, dc)
         sec, reps = cs.time(budget_s=12.0)
         cpu = {"value": flops / sec / 1e12, "unit": UNIT, "cores": cs.threads, "kind": "port",
@@ -511,6 +542,7 @@ def main():
             "clocks": clocks,
             "extra": {"forward_ms": fwd_ms, "adjoint_ms": adj_ms, "sddmm_ms": sddmm_ms,
                       "adjoint_sddmm_fused_ms": adj_sddmm_ms,
+                      "cpu_torch_sparse_forward": cpu_torch,
                       "forward_residual_pass_ms": res_ms,
                       "forward_residual_roofline": {
                           "achieved_gbs": res_gbs, "frac": res_gbs / peak,
