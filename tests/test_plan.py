@@ -28,6 +28,10 @@ OPTS = [
     dict(reorder=True, transpose=True, promote_min=2, row_scale=True),
     dict(demote_below=3),
     dict(demote_below=4, promote_min=4, reorder=True, row_scale=True),
+    # every 2:4 column demoted: the group entries go straight to the residual
+    dict(demote_below=1000, row_scale=True),
+    dict(demote_below=17, transpose=True, promote_min=2),
+    dict(demote_below=1000, reorder=True, transpose=True, row_scale=True),
 ]
 
 

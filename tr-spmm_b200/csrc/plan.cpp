@@ -361,9 +361,39 @@ int add_packed_tiles(const int32_t* tile_column, int64_t n_tile_column, const ui
 }
 
 // ---- 2:4 groups (s_column / s_value / s_pos) -------------------------------------
+// With to_residual (every 2:4 column would be demoted: no column of a
+// window holds more than 16 entries) the group entries go straight to the
+// CUDA-core residual, by the rule demote() applies, without being laid out
+// as tiles first.
 int add_groups(const int32_t* s_column, const float* s_value, const int8_t* s_pos,
                const int32_t* s_edge, int64_t groups, const std::vector<int32_t>& gwin,
-               int32_t n_rows, int32_t n_cols, int W, Staging& st, std::string& err) {
+               int32_t n_rows, int32_t n_cols, int W, Staging& st, std::string& err,
+               bool to_residual = false) {
+  if (to_residual) {
+    for (int64_t g = 0; g < groups; ++g) {
+      const int w = gwin[g];
+      if (!in_range(w, 0, W)) continue;                     // beyond the matrix
+      int32_t c[4];
+      for (int p = 0; p < 4; ++p) {
+        c[p] = s_column[g * 4 + p];
+        if (c[p] < -1 || c[p] >= n_cols) { err = "s_column out of range"; return TR_ERR_ARG; }
+      }
+      for (int lr = 0; lr < 16; ++lr) {
+        if ((int64_t)w * 16 + lr >= n_rows) continue;
+        const int64_t at0 = (g * 16 + lr) * 2;
+        for (int s = 0; s < 2; ++s) {
+          const int64_t at = at0 + s;
+          const int pos = s_pos[at];
+          if (pos < 0 || pos > 3 || c[pos] < 0) continue;
+          if (s == 0 && s_pos[at0 + 1] == pos) continue;    // the later slot wins, as in a tile
+          const float v = s_value[at];
+          const int32_t e = s_edge ? s_edge[at] : -1;
+          if (v != 0.f || e >= 0) st.res.push_back({w * 16 + lr, c[pos], v, e});
+        }
+      }
+    }
+    return TR_OK;
+  }
   std::vector<std::vector<int64_t>> wg(W);
   for (int64_t g = 0; g < groups; ++g)
     if (in_range(gwin[g], 0, W)) wg[gwin[g]].push_back(g);   // others lie beyond the matrix
@@ -465,7 +495,7 @@ int plan_from_route(const RouteTables& T, int32_t n_rows, int32_t n_cols, int64_
   if (rc) return rc;
   const int64_t groups = (int64_t)T.s_window.size();
   rc = add_groups(T.s_column.data(), T.s_value.data(), T.s_pos.data(), T.s_edge.data(), groups,
-                  T.s_window, n_rows, n_cols, hp.n_windows, st, err);
+                  T.s_window, n_rows, n_cols, hp.n_windows, st, err, opt.demote_below > 16);
   if (rc) return rc;
   rc = add_parts(T.c_row_offset.data(), (int64_t)T.c_row_offset.size(), T.c_row.data(),
                  (int64_t)T.c_row.size(), T.c_column.data(), (int64_t)T.c_column.size(),
