@@ -177,9 +177,16 @@ __device__ __forceinline__ void store_row_feature(void* C, int K, int64_t row, i
 // shared loads; B addresses are 32-bit element offsets from the chunk's
 // feature base.
 constexpr int kSegStride = kChunk + kChunk / 32;     // padded shared row (floats)
+// The forward engine takes up to 256 features per pass (one 32-lane group per
+// warp at K = 256: a second pass would repeat the staging, the row tracking
+// and the flushes for the other half); the padded layout stays conflict-free
+// for 32 lanes of 8 features.
+constexpr int kSegChunk = 256;
+constexpr int kSegStrideW = kSegChunk + kSegChunk / 32;
 constexpr int kSegU = 4;                             // entries per lane group and batch
 
 __device__ __forceinline__ int seg_slot(int r, int f) { return r * kSegStride + f + (f >> 5); }
+__device__ __forceinline__ int seg_slot_w(int r, int f) { return r * kSegStrideW + f + (f >> 5); }
 
 // 16 bytes of B row `col` at the lane's feature base Bf.
 template <bool WIDE>
@@ -238,7 +245,7 @@ __global__ void __launch_bounds__(kThreads, 4) seg_block_kernel(
     const int32_t* __restrict__ row_out, const float* __restrict__ row_scale,
     const int32_t* __restrict__ order) {
   constexpr int U = kSegU;
-  __shared__ __align__(16) float racc[kBlockRows * kSegStride];
+  __shared__ __align__(16) float racc[kBlockRows * kSegStrideW];
   __shared__ __align__(16) int2 sent[kStage + 2];
   __shared__ int rp[kBlockRows + 1];
   __shared__ int s_out[kBlockRows];
@@ -255,8 +262,8 @@ __global__ void __launch_bounds__(kThreads, 4) seg_block_kernel(
   __syncthreads();
   const int e_begin = rp[0], e_end = rp[kBlockRows];
   const uint32_t uK = (uint32_t)K;
-  for (int f0 = 0; f0 < K; f0 += kChunk) {
-    const int fc = min(kChunk, K - f0);
+  for (int f0 = 0; f0 < K; f0 += kSegChunk) {
+    const int fc = min(kSegChunk, K - f0);
     int L = 1;
     while (L * 8 < fc) L <<= 1;
     const int G = 32 / L, groups = kWarps * G;
@@ -265,10 +272,10 @@ __global__ void __launch_bounds__(kThreads, 4) seg_block_kernel(
     if (tid < kBlockRows) s_own[tid] = seg_owned(rp[tid], rp[tid + 1], e_begin, e_end, groups);
     {
       float4* z = reinterpret_cast<float4*>(racc);
-      for (int i = tid; i < kBlockRows * kSegStride / 4; i += kThreads) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+      for (int i = tid; i < kBlockRows * kSegStrideW / 4; i += kThreads) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     const __half* Bf = B + f0 + (active ? li * 8 : 0);
-    float* dst = racc + seg_slot(0, active ? li * 8 : 0);
+    float* dst = racc + seg_slot_w(0, active ? li * 8 : 0);
     for (int c0 = e_begin; c0 < e_end; c0 += kStage) {
       const int n = min(kStage, e_end - c0);
       __syncthreads();                       // previous chunk consumed, racc zeroed
@@ -292,7 +299,7 @@ __global__ void __launch_bounds__(kThreads, 4) seg_block_kernel(
           if (s_out[r] >= 0) store_vec<F16OUT, 8>(C, K, s_out[r], f0 + li * 8, acc, s_scale[r]);
         } else {
 #pragma unroll
-          for (int i = 0; i < 8; ++i) atomicAdd(dst + r * kSegStride + i, acc[i]);
+          for (int i = 0; i < 8; ++i) atomicAdd(dst + r * kSegStrideW + i, acc[i]);
         }
       };
 #pragma unroll 1
@@ -348,7 +355,7 @@ __global__ void __launch_bounds__(kThreads, 4) seg_block_kernel(
         for (int f = lane * 4; f < fc; f += 128) {
           float x[4];
 #pragma unroll
-          for (int i = 0; i < 4; ++i) x[i] = racc[seg_slot(r, f + i)];
+          for (int i = 0; i < 4; ++i) x[i] = racc[seg_slot_w(r, f + i)];
           store_vec<F16OUT, 4>(C, K, s_out[r], f0 + f, x, s_scale[r]);
         }
     __syncthreads();                         // racc and s_own are rewritten next pass
