@@ -117,7 +117,10 @@ FUSED_CASES = [
     ("ragged", 40, dict()),                                      # fused, K not a power of 2
     ("sbm", 128, dict(reorder=True, demote_below=1000, row_scale=True)),   # fused, reordered
     ("route_mix", 128, dict()),                                  # tiles: two launches
-    ("chung_lu", 256, dict()),                                   # K > 128: two launches
+    ("chung_lu", 256, dict()),                                   # fused, 32-lane groups
+    ("ragged", 200, dict(row_scale=True)),                       # fused, 25 of 32 lanes active
+    ("sbm", 256, dict(reorder=True, demote_below=1000)),         # fused, 32-lane groups, reordered
+    ("chung_lu", 264, dict()),                                   # K > 256: two launches
 ]
 
 

@@ -185,8 +185,8 @@ constexpr int kSegChunk = 256;
 constexpr int kSegStrideW = kSegChunk + kSegChunk / 32;
 constexpr int kSegU = 4;                             // entries per lane group and batch
 
-__device__ __forceinline__ int seg_slot(int r, int f) { return r * kSegStride + f + (f >> 5); }
-__device__ __forceinline__ int seg_slot_w(int r, int f) { return r * kSegStrideW + f + (f >> 5); }
+template <int S = kSegStrideW>
+__device__ __forceinline__ int seg_slot_w(int r, int f) { return r * S + f + (f >> 5); }
 
 // 16 bytes of B row `col` at the lane's feature base Bf.
 template <bool WIDE>
@@ -795,13 +795,18 @@ __global__ void __launch_bounds__(256) sddmm_group_kernel(const int32_t* __restr
 // with shuffles).  The separate SDDMM would gather every dC row a second
 // time.
 
-// Sums 8 per-lane values over a group of L lanes (L = 8 or 16) so that lane
-// (li & 7) ends up with the total of value (li & 7): for L = 16 the two
-// halves are folded first, then each reduce-scatter step halves the values a
-// lane keeps (15 shuffles for 8 sums instead of 8 * log2(L)).
+// Sums 8 per-lane values over a group of L lanes (L = 8, 16 or 32) so that
+// lane (li & 7) ends up with the total of value (li & 7): for L > 8 the
+// group's 8-lane quarters are folded first, then each reduce-scatter step
+// halves the values a lane keeps (15 shuffles for 8 sums instead of
+// 8 * log2(L) at L = 8).
 template <int L>
 __device__ __forceinline__ float group_reduce_scatter8(float (&d)[8], int li) {
-  if (L == 16) {
+  if (L == 32) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) d[u] += __shfl_xor_sync(0xffffffffu, d[u], 16);
+  }
+  if (L >= 16) {
 #pragma unroll
     for (int u = 0; u < 8; ++u) d[u] += __shfl_xor_sync(0xffffffffu, d[u], 8);
   }
@@ -825,8 +830,9 @@ __device__ __forceinline__ float group_reduce_scatter8(float (&d)[8], int li) {
 // 16-byte chunk of dC[i] feeds dB[j] += a * dC[i] and the partial dot with
 // row j of B (held in registers, reloaded when the row changes), and the
 // group's 8 partial dots are reduce-scattered so that lane u (< 8) writes
-// dval for the batch's entry u.  K <= 128 (one feature chunk).  Four CTAs
-// per SM (64 registers, a few bytes of spill) beat three without spill.
+// dval for the batch's entry u.  K <= 256 in one pass (lane groups of 8,
+// 16 or 32 lanes).  Four CTAs per SM (64 registers, a few bytes of spill)
+// beat three without spill.
 template <bool F16OUT, int L, bool WIDE>
 __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
     const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
@@ -836,7 +842,8 @@ __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
     const int32_t* __restrict__ order) {
   constexpr int U = 8;
   constexpr int Gn = 32 / L, groups = kWarps * Gn;
-  __shared__ __align__(16) float racc[kBlockRows * kSegStride];
+  constexpr int S = L == 32 ? kSegStrideW : kSegStride;   // padded shared row (floats)
+  __shared__ __align__(16) float racc[kBlockRows * S];
   __shared__ __align__(16) int4 sent[kStage + 1];
   __shared__ int rp[kBlockRows + 1];
   __shared__ int s_out[kBlockRows];
@@ -858,10 +865,10 @@ __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
   if (tid < kBlockRows) s_own[tid] = seg_owned(rp[tid], rp[tid + 1], e_begin, e_end, groups);
   {
     float4* z = reinterpret_cast<float4*>(racc);
-    for (int i = tid; i < kBlockRows * kSegStride / 4; i += kThreads) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = tid; i < kBlockRows * S / 4; i += kThreads) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
   const __half* Gf = G + (active ? li * 8 : 0);
-  float* dst = racc + seg_slot(0, active ? li * 8 : 0);
+  float* dst = racc + seg_slot_w<S>(0, active ? li * 8 : 0);
   const uint16_t* v16 = reinterpret_cast<const uint16_t*>(values);
   for (int c0 = e_begin; c0 < e_end; c0 += kStage) {
     const int n = min(kStage, e_end - c0);
@@ -891,7 +898,7 @@ __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
         if (s_out[r] >= 0) store_vec<F16OUT, 8>(C, K, s_out[r], li * 8, acc, s_scale[r]);
       } else {
 #pragma unroll
-        for (int i = 0; i < 8; ++i) atomicAdd(dst + r * kSegStride + i, acc[i]);
+        for (int i = 0; i < 8; ++i) atomicAdd(dst + r * S + i, acc[i]);
       }
     };
 #pragma unroll 1
@@ -951,7 +958,7 @@ __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
       for (int f = lane * 4; f < K; f += 128) {
         float x[4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) x[i] = racc[seg_slot(r, f + i)];
+        for (int i = 0; i < 4; ++i) x[i] = racc[seg_slot_w<S>(r, f + i)];
         store_vec<F16OUT, 4>(C, K, s_out[r], f, x, s_scale[r]);
       }
 }
@@ -1137,7 +1144,7 @@ int launch_sddmm(const int32_t* indptr, const int32_t* indices, int32_t m, int64
 // dB = A^T . dC through the adjoint plan and dval = SDDMM(dC, B) on A's
 // pattern.  Fused into one pass when the adjoint plan keeps every entry of A
 // in its CUDA-core residual with its entry id (native exact plans without
-// tiles), K <= 128 and K % 8 == 0; otherwise the routed adjoint and the
+// tiles), K <= 256 and K % 8 == 0; otherwise the routed adjoint and the
 // SDDMM run as two launches.
 int launch_adjoint_sddmm(const tr_plan* p, const int32_t* a_indptr, const int32_t* a_indices,
                          int32_t a_rows, int64_t nnz, const uint16_t* dc, const uint16_t* b,
@@ -1145,8 +1152,8 @@ int launch_adjoint_sddmm(const tr_plan* p, const int32_t* a_indptr, const int32_
   const PlanView& v = p->view;
   const bool f16 = db_dtype == TR_OUT_F16;
   const bool tiles = p->info.tc_tiles + p->info.sptc_tiles + p->info.promoted_tiles > 0;
-  // lane groups of 8 or 16 lanes (K in (32, 128]): the reduce-scatter needs 8+ lanes
-  const bool fused = !tiles && k > 32 && k <= kChunk && k % 8 == 0 && aligned16(dc) && aligned16(b) &&
+  // lane groups of 8, 16 or 32 lanes (K in (32, 256]): the reduce-scatter needs 8+ lanes
+  const bool fused = !tiles && k > 32 && k <= kSegChunk && k % 8 == 0 && aligned16(dc) && aligned16(b) &&
                      p->n_edges == nnz && p->info.residual_nnz == nnz && v.n_rows > 0;
   if (!fused) {
     int rc = launch_routed(p, dc, k, db, db_dtype, TR_ROUTE_ALL, stream);
@@ -1162,7 +1169,10 @@ int launch_adjoint_sddmm(const tr_plan* p, const int32_t* a_indptr, const int32_
       v.res_ptr, v.res_col, rv, v.res_edge, rows, g, k, db, v.row_out, v.row_scale, h, dval,   \
       v.win_order)
   const bool wide = (int64_t)v.n_cols * k >= ((int64_t)1 << 31);
-  if (k > 64) {
+  if (k > 128) {
+    if (wide) { if (f16) TRS_SEGADJ(true, 32, true); else TRS_SEGADJ(false, 32, true); }
+    else { if (f16) TRS_SEGADJ(true, 32, false); else TRS_SEGADJ(false, 32, false); }
+  } else if (k > 64) {
     if (wide) { if (f16) TRS_SEGADJ(true, 16, true); else TRS_SEGADJ(false, 16, true); }
     else { if (f16) TRS_SEGADJ(true, 16, false); else TRS_SEGADJ(false, 16, false); }
   } else {
