@@ -251,13 +251,54 @@ typedef struct tr_plan_opts {
                               the tensor cores (0: keep the CUDA-core residual) */
   int32_t transpose;       /* 1: plan for A^T (the adjoint dB = A^T dC); entry
                               indices still refer to A's CSR */
-  int32_t reorder;         /* 1: cluster rows with shared columns into the same
-                              windows before routing; results are written to the
-                              original row positions */
+  int32_t reorder;         /* TR_REORDER_*: rows with shared columns are put into
+                              the same windows before routing; results are
+                              written to the original row positions */
   int32_t demote_below;    /* 2:4 tile columns holding fewer than demote_below
                               entries of their window go to the CUDA-core
                               residual (0 or 1: keep the router's 2:4 tiles) */
+  const int32_t* row_order;  /* TR_REORDER_GIVEN: host array [rows of the
+                              (transposed) matrix], plan row i = row_order[i],
+                              a permutation (e.g. from tr_tca_order) */
 } tr_plan_opts;
+
+/* Row orders of tr_plan_opts.reorder:
+ *   TR_REORDER_NONE     natural order
+ *   TR_REORDER_LABEL    label propagation with a 256-row label cap
+ *   TR_REORDER_TCA      the TCA clustering of tr_tca_order (default
+ *                       parameters, host threads)
+ *   TR_REORDER_GIVEN    the caller's permutation in row_order */
+enum { TR_REORDER_NONE = 0, TR_REORDER_LABEL = 1, TR_REORDER_TCA = 2, TR_REORDER_GIVEN = 3 };
+
+/* TCA row clustering (replaces spmm/tr_csr_fp16/tr_tca_reorder.py:44-357,
+ * apply_tca_reorder): MinHash-LSH (128 permutations, bands tuned for
+ * lsh_threshold) proposes pairs of rows, pairs are merged most similar
+ * (exact Jaccard of the column sets) first into clusters of at most `thres`
+ * rows, and the clusters the same way into groups of at most `cluster_thres`
+ * clusters.  Host CSR in; order[n_rows] out (new position -> old row, the
+ * reference's reorder_id).  device = 1 runs the signatures and the Jaccard
+ * similarities on the current GPU (same result); the bucket sort and the
+ * clustering stay on the host.  Graphs with more than max_pairs candidate
+ * pairs are refused (TR_ERR_UNSUPPORTED).  NULL params: the defaults below. */
+typedef struct tr_tca_params {
+  int32_t thres;           /* 16 */
+  int32_t cluster_thres;   /* 128 */
+  double lsh_threshold;    /* 0.2 */
+  uint64_t seed;           /* 1 */
+  int64_t max_pairs;       /* 2^25 */
+  int32_t device;          /* 0 */
+} tr_tca_params;
+typedef struct tr_tca_stats {
+  int32_t bands, rows_per_band;   /* LSH banding used */
+  int64_t pairs1, clusters1;      /* candidate row pairs, row clusters */
+  int64_t pairs2, clusters2;      /* candidate cluster pairs, final groups */
+} tr_tca_stats;
+int tr_tca_order(const int32_t* indptr, const int32_t* indices, int32_t n_rows,
+                 const tr_tca_params* params, int32_t* order, tr_tca_stats* stats);
+/* The LSH banding tr_tca_order uses: b bands of r rows (b * r <= num_perm)
+ * minimising 0.5 * (false-positive + false-negative) probability integrals
+ * around the threshold. */
+int tr_lsh_params(double threshold, int32_t num_perm, int32_t* bands, int32_t* rows);
 
 /* Native plan builder: validate the CSR, optionally transpose and reorder it,
  * route it (params; mode TR_ROUTE_EXACT keeps every entry) and lay it out.

@@ -19,13 +19,16 @@ Contents
                      scales, output rows); plan_value_of_entries() reads back
                      each CSR entry's value through the entry -> slot map.
   spmm_f64() / spmm_f16_f32() / sddmm_f64()   CSR arithmetic in C (OpenMP).
+  tca.tca_order()    Python restatement of the TCA row reorder
+                     (spmm/tr_csr_fp16/tr_tca_reorder.py:44-357).
 """
+from . import tca
 from .core import (TABLE_NAMES, route, ref_route, ref_available, ref_match, ref_match_available,
                    decode_tables,
                    decode_sptc_tiles, decode_plan, plan_value_of_entries, spmm_f64,
                    spmm_f16_f32, sddmm_f64, sddmm_f16_f32, max_threads, lib_path)
 
-__all__ = ["TABLE_NAMES", "route", "ref_route", "ref_available", "ref_match",
+__all__ = ["tca", "TABLE_NAMES", "route", "ref_route", "ref_available", "ref_match",
            "ref_match_available", "decode_tables",
            "decode_sptc_tiles", "decode_plan", "plan_value_of_entries", "spmm_f64", "spmm_f16_f32", "sddmm_f64", "sddmm_f16_f32", "max_threads",
            "lib_path"]

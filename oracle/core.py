@@ -125,15 +125,33 @@ def ref_available():
     return bool(glob.glob(os.path.join(_ref_dir(), "Libra5BlockOnline*.so")))
 
 
+_REF_MODULES = {}
+
+
+def _load_ref(module):
+    """A module of oracle/_ref loaded from its file, neither put on sys.path
+    nor entered in sys.modules: the library's drop-in modules have the same
+    names and must keep resolving to the library's own files."""
+    if module not in _REF_MODULES:
+        import importlib.util
+        paths = (glob.glob(os.path.join(_ref_dir(), module + ".*.so")) +
+                 glob.glob(os.path.join(_ref_dir(), module + ".so")))
+        if not paths:
+            raise ImportError(f"{module} not built under oracle/_ref")
+        spec = importlib.util.spec_from_file_location(module, paths[0])
+        mod = importlib.util.module_from_spec(spec)
+        spec.loader.exec_module(mod)
+        _REF_MODULES[module] = mod
+    return _REF_MODULES[module]
+
+
 def ref_route(indptr, indices, values, *args, quiet=True):
     """The reference router compiled from its own source (oracle/_ref).
 
     Same arguments as block_sptc_2to4_online; returns numpy arrays.  The
     reference prints per-window diagnostics on stdout; ``quiet`` drops them."""
     import torch
-    if _ref_dir() not in sys.path:
-        sys.path.insert(0, _ref_dir())
-    import Libra5BlockOnline  # noqa: E402  (built by oracle/Makefile)
+    Libra5BlockOnline = _load_ref("Libra5BlockOnline")     # built by oracle/Makefile
     rp = torch.from_numpy(np.ascontiguousarray(indptr, dtype=np.int32))
     ci = torch.from_numpy(np.ascontiguousarray(indices, dtype=np.int32))
     vv = torch.from_numpy(np.ascontiguousarray(values, dtype=np.float32))
@@ -154,7 +172,8 @@ def ref_route(indptr, indices, values, *args, quiet=True):
 
 
 def ref_match_available(module="matching_utils"):
-    return bool(glob.glob(os.path.join(_ref_dir(), module + "*.so")))
+    return bool(glob.glob(os.path.join(_ref_dir(), module + ".*.so")) +
+                glob.glob(os.path.join(_ref_dir(), module + ".so")))
 
 
 def ref_match(module, func, indptr, indices, values, quiet=True, **kw):
@@ -162,10 +181,7 @@ def ref_match(module, func, indptr, indices, values, quiet=True, **kw):
     source (oracle/_ref: matching_utils.match_2to4, matching_utils_hash.
     match_2to4_hash, matching_utils_bucket.match_2to4_bucket); returns its
     dict.  The reference prints a summary box on stdout; ``quiet`` drops it."""
-    import importlib
-    if _ref_dir() not in sys.path:
-        sys.path.insert(0, _ref_dir())
-    mod = importlib.import_module(module)
+    mod = _load_ref(module)
     rp = np.ascontiguousarray(indptr, dtype=np.int32)
     ci = np.ascontiguousarray(indices, dtype=np.int32)
     vv = np.ascontiguousarray(values, dtype=np.float32)

@@ -32,6 +32,8 @@ OPTS = [
     dict(demote_below=1000, row_scale=True),
     dict(demote_below=17, transpose=True, promote_min=2),
     dict(demote_below=1000, reorder=True, transpose=True, row_scale=True),
+    dict(reorder="tca"),
+    dict(reorder="tca", transpose=True, promote_min=2, row_scale=True),
 ]
 
 

@@ -5,15 +5,16 @@
 // each entry of A lives (learnable edge weights re-value the plan on the
 // device without rebuilding it).
 //
-// Row clustering (opts.reorder) is this library's counterpart of the
+// Row orders (opts.reorder) put rows that share columns into the same 16-row
+// windows, so that a gathered feature row serves several output rows: the
 // reference's optional row reorder (spmm/tr_csr_fp16/tr_tca_reorder.py:44-357,
 // MinHash-LSH Jaccard clustering, off by default at
-// spmm/tr_csr_fp16/mdataset2_online.py:73): rows that share columns are put
-// into the same 16-row windows so that a gathered feature row serves several
-// output rows.  Here it is label propagation over the bipartite row/column
-// graph (deterministic sweeps, seeded visiting order), then a stable sort of
-// rows by label.  Only rows move; B is never permuted, and the kernels write
-// every result row back to its original position.
+// spmm/tr_csr_fp16/mdataset2_online.py:73) is TR_REORDER_TCA (tca.cpp);
+// TR_REORDER_LABEL is label propagation over the bipartite row/column graph
+// (deterministic sweeps, seeded visiting order), then a stable sort of rows
+// by label; TR_REORDER_GIVEN takes the caller's permutation.  Only rows move;
+// B is never permuted, and the kernels write every result row back to its
+// original position.
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
@@ -25,6 +26,7 @@
 #include "common.cuh"
 #include "plan.h"
 #include "router.h"
+#include "tca.h"
 
 namespace trs {
 
@@ -235,9 +237,28 @@ int build_plan(const int32_t* indptr, const int32_t* indices, const float* value
     transpose(a, t);
     a = std::move(t);
   }
+  if (opts.reorder < TR_REORDER_NONE || opts.reorder > TR_REORDER_GIVEN) {
+    err = "unknown reorder mode " + std::to_string(opts.reorder);
+    return TR_ERR_ARG;
+  }
   std::vector<int32_t> perm;
-  if (opts.reorder) {
+  if (opts.reorder == TR_REORDER_LABEL) {
     cluster_rows(a, perm, 8, 256);
+  } else if (opts.reorder == TR_REORDER_TCA) {
+    TcaParams tp;
+    TcaStats ts;
+    rc = tca_order(a.ptr.data(), a.idx.data(), a.n_rows, tp, perm, ts, err);
+    if (rc) return rc;
+  } else if (opts.reorder == TR_REORDER_GIVEN) {
+    if (!opts.row_order && a.n_rows > 0) { err = "TR_REORDER_GIVEN needs row_order"; return TR_ERR_ARG; }
+    perm.assign(opts.row_order, opts.row_order + a.n_rows);
+    std::vector<char> seen(a.n_rows, 0);
+    for (int32_t r : perm) {
+      if (r < 0 || r >= a.n_rows || seen[r]) { err = "row_order is not a permutation of the rows"; return TR_ERR_ARG; }
+      seen[r] = 1;
+    }
+  }
+  if (opts.reorder) {
     Csr p;
     permute_rows(a, perm, p);
     a = std::move(p);

@@ -14,6 +14,7 @@
 #include "route_gpu.h"
 #include "router.h"
 #include "spmm.h"
+#include "tca.h"
 
 namespace trs {
 
@@ -266,6 +267,54 @@ int tr_match_2to4_online(const int32_t* indptr, const int32_t* indices, int32_t 
   std::string err;
   const int rc = match_online_gpu(indptr, indices, n_rows, dense_threshold, t_max, out, err);
   return rc ? fail(rc, err) : TR_OK;
+}
+
+int tr_tca_order(const int32_t* indptr, const int32_t* indices, int32_t n_rows,
+                 const tr_tca_params* params, int32_t* order, tr_tca_stats* stats) {
+  if (!indptr || (n_rows > 0 && !order)) return fail(TR_ERR_ARG, "null argument");
+  if (n_rows < 0) return fail(TR_ERR_ARG, "negative row count");
+  if (indptr[0] != 0) return fail(TR_ERR_ARG, "indptr must start at 0");
+  for (int32_t r = 0; r < n_rows; ++r)
+    if (indptr[r + 1] < indptr[r]) return fail(TR_ERR_ARG, "indptr must be non-decreasing");
+  const int64_t nnz = indptr[n_rows];
+  if (nnz > 0 && !indices) return fail(TR_ERR_ARG, "null indices");
+  for (int64_t e = 0; e < nnz; ++e)
+    if (indices[e] < 0) return fail(TR_ERR_ARG, "column indices must be >= 0");
+  TcaParams p;
+  if (params) {
+    p.thres = params->thres;
+    p.cluster_thres = params->cluster_thres;
+    p.lsh_threshold = params->lsh_threshold;
+    p.seed = params->seed;
+    p.max_pairs = params->max_pairs;
+    p.device = params->device;
+  }
+  std::vector<int32_t> ord;
+  TcaStats st;
+  std::string err;
+  const int rc = tca_order(indptr, indices, n_rows, p, ord, st, err);
+  if (rc) return fail(rc, err);
+  std::copy(ord.begin(), ord.end(), order);
+  if (stats) {
+    stats->bands = st.bands;
+    stats->rows_per_band = st.rows_per_band;
+    stats->pairs1 = st.pairs1;
+    stats->clusters1 = st.clusters1;
+    stats->pairs2 = st.pairs2;
+    stats->clusters2 = st.clusters2;
+  }
+  return TR_OK;
+}
+
+int tr_lsh_params(double threshold, int32_t num_perm, int32_t* bands, int32_t* rows) {
+  if (!bands || !rows) return fail(TR_ERR_ARG, "null argument");
+  if (!(threshold > 0.0 && threshold < 1.0)) return fail(TR_ERR_ARG, "threshold must be in (0, 1)");
+  if (num_perm < 1 || num_perm > 1024) return fail(TR_ERR_ARG, "num_perm must be in [1, 1024]");
+  int b = 0, r = 0;
+  tca_lsh_params(threshold, num_perm, b, r);
+  *bands = b;
+  *rows = r;
+  return TR_OK;
 }
 
 int tr_host_plan_save(const tr_host_plan* h, const char* path) {

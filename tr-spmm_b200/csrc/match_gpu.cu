@@ -236,7 +236,10 @@ int match_online_gpu(const int32_t* indptr, const int32_t* indices, int32_t n_ro
   cudaFree(d_ptr);
   cudaFree(d_idx);
   cudaFree(d_out);
-  if (e != cudaSuccess) return cuda_fail(e, "online matching");
+  if (e != cudaSuccess) {
+    err = std::string("online matching: ") + cudaGetErrorString(e);
+    return TR_ERR_CUDA;
+  }
   tr_match_stats s{};
   s.total_rows = n_rows;
   s.total_cols = n_cols;

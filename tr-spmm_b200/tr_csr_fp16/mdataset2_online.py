@@ -8,8 +8,12 @@ FP16 and random FP16 features ``x`` (mdataset2_online.py:100-167).
 
 Besides the reference's ``.npz`` loader, ``from_csr`` accepts an in-memory
 CSR (the synthetic workloads use it; the reference ships no datasets).
+LIBRA_TCA_REORDER=1 reorders the rows first (tr_tca_reorder.apply_tca_reorder),
+as the reference's loader does (mdataset2_online.py:72-91).
 """
 from __future__ import annotations
+
+import os
 
 import numpy as np
 import scipy.sparse as sp
@@ -17,6 +21,7 @@ import torch
 
 import Libra5BlockOnline
 from tr_csr_fp16.tr_paths import load_graph_npz
+from tr_csr_fp16.tr_tca_reorder import apply_tca_reorder
 
 _NAMES = [
     "t_rowNew_offsetTensor", "t_blockTensor", "t_columnTensor", "t_valueTensor",
@@ -69,10 +74,22 @@ class GCN_dataset_tcu_sptc_cuda_online(torch.nn.Module):
         src_li = np.asarray(self.graph["src_li"])
         dst_li = np.asarray(self.graph["dst_li"])
         self.edge_index = np.stack([src_li, dst_li])
+        self.reorder_id = None
+        tca = os.environ.get("LIBRA_TCA_REORDER", "0") == "1"
         if self._values is None:
             val = np.ones(len(src_li), dtype=np.float32)
             adj = sp.coo_matrix((val, self.edge_index),
                                 shape=(self.num_nodes, self.num_nodes_dst)).tocsr()
+            if tca:
+                # mdataset2_online.py:72-91: rows of the first num_nodes_ori
+                # rows reordered, edge_index and CSR rebuilt from the result
+                # (here from correct row pointers: the reference's are all zero)
+                rptr, ridx, self.reorder_id = apply_tca_reorder(
+                    adj.indptr, adj.indices, self.num_nodes_ori, thres=16, verbose=self.verbose)
+                new_src = np.repeat(np.arange(self.num_nodes_ori), np.diff(rptr))
+                self.edge_index = np.stack([new_src, ridx])
+                adj = sp.coo_matrix((np.ones(len(ridx), dtype=np.float32), (new_src, ridx)),
+                                    shape=(self.num_nodes, self.num_nodes_dst)).tocsr()
             self.column_index = torch.IntTensor(adj.indices)
             self.row_pointers = torch.IntTensor(adj.indptr)
             self.num_edges = self.column_index.numel()
@@ -84,6 +101,16 @@ class GCN_dataset_tcu_sptc_cuda_online(torch.nn.Module):
             vals = np.asarray(self._values, dtype=np.float32)[order]
             indptr = np.zeros(self.num_nodes + 1, dtype=np.int64)
             indptr[1:] = np.cumsum(np.bincount(rows, minlength=self.num_nodes))
+            if tca:
+                _, _, self.reorder_id = apply_tca_reorder(indptr, cols, self.num_nodes_ori,
+                                                          thres=16, verbose=self.verbose)
+                perm = np.concatenate([self.reorder_id,
+                                       np.arange(self.num_nodes_ori, self.num_nodes)])
+                new_of = np.empty_like(perm)
+                new_of[perm] = np.arange(perm.size)
+                keep = np.lexsort((np.arange(rows.size), new_of[rows]))
+                rows, cols, vals = new_of[rows][keep], cols[keep], vals[keep]
+                indptr[1:] = np.cumsum(np.bincount(rows, minlength=self.num_nodes))
             self.column_index = torch.from_numpy(cols.astype(np.int32))
             self.row_pointers = torch.from_numpy(indptr.astype(np.int32))
             self.num_edges = self.column_index.numel()

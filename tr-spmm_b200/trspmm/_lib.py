@@ -29,6 +29,7 @@ EXPORTED = [
     "tr_adjoint_sddmm",
     "tr_forward_fp16_tcu_cuda_sptc_mma_parallel_online", "tr_forward_fp16_sptc_online",
     "tr_forward_fp16_sptc_mma_online", "tr_forward_fp16_sptc_mma_packed_online",
+    "tr_tca_order", "tr_lsh_params",
 ]
 
 
@@ -75,7 +76,24 @@ class PlanInfo(ctypes.Structure):
 class PlanOpts(ctypes.Structure):
     _fields_ = [("row_scale", ctypes.c_int32), ("promote_min", ctypes.c_int32),
                 ("transpose", ctypes.c_int32), ("reorder", ctypes.c_int32),
-                ("demote_below", ctypes.c_int32)]
+                ("demote_below", ctypes.c_int32), ("row_order", ctypes.c_void_p)]
+
+
+TR_REORDER_NONE, TR_REORDER_LABEL, TR_REORDER_TCA, TR_REORDER_GIVEN = 0, 1, 2, 3
+
+
+class TcaParams(ctypes.Structure):
+    """tr_tca_params (include/trspmm.h)."""
+    _fields_ = [("thres", ctypes.c_int32), ("cluster_thres", ctypes.c_int32),
+                ("lsh_threshold", ctypes.c_double), ("seed", ctypes.c_uint64),
+                ("max_pairs", ctypes.c_int64), ("device", ctypes.c_int32)]
+
+
+class TcaStats(ctypes.Structure):
+    """tr_tca_stats (include/trspmm.h)."""
+    _fields_ = [("bands", ctypes.c_int32), ("rows_per_band", ctypes.c_int32),
+                ("pairs1", ctypes.c_int64), ("clusters1", ctypes.c_int64),
+                ("pairs2", ctypes.c_int64), ("clusters2", ctypes.c_int64)]
 
 
 _TABLE_FIELDS = ["t_row_offset", "t_block_offset", "t_column", "t_value", "t_window_row",
@@ -110,6 +128,8 @@ def lib():
                                              I64, I64, P, P, P]
     L.tr_match_2to4.argtypes = [P, P, I32, ctypes.c_int, I32, I32, I32, ctypes.POINTER(MatchStats)]
     L.tr_match_2to4_online.argtypes = [P, P, I32, I32, I32, I32, ctypes.POINTER(MatchStats)]
+    L.tr_tca_order.argtypes = [P, P, I32, ctypes.POINTER(TcaParams), P, ctypes.POINTER(TcaStats)]
+    L.tr_lsh_params.argtypes = [ctypes.c_double, I32, ctypes.POINTER(I32), ctypes.POINTER(I32)]
     L.tr_route_seconds.restype = ctypes.c_double
     L.tr_route_seconds.argtypes = [P]
     L.tr_route_free.argtypes = [P]

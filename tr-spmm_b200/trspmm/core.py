@@ -21,8 +21,9 @@ import numpy as np
 from . import _lib
 from ._lib import (TR_MATCH_BUCKET, TR_MATCH_HASH, TR_MATCH_ONLINE, TR_MATCH_SLIDING, TR_OUT_F16,
                    TR_OUT_F32,
+                   TR_REORDER_GIVEN, TR_REORDER_LABEL, TR_REORDER_NONE, TR_REORDER_TCA,
                    TR_ROUTE_ALL, TR_ROUTE_COMPAT, TR_ROUTE_EXACT, MatchStats, PlanInfo, PlanOpts,
-                   RouteParams, Tables, check, lib)
+                   RouteParams, Tables, TcaParams, TcaStats, check, lib)
 
 TABLE_NAMES = [
     "t_row_offset", "t_block_offset", "t_column", "t_value", "t_window_row", "t_atomic",
@@ -42,6 +43,29 @@ _DTYPES = [np.int32, np.int32, np.int32, np.float32, np.int32, np.int32, np.int6
 
 def _vp(a):
     return ctypes.c_void_p(a.ctypes.data) if a is not None and a.size else ctypes.c_void_p(0)
+
+
+REORDER_MODES = {False: TR_REORDER_NONE, None: TR_REORDER_NONE, "none": TR_REORDER_NONE,
+                 True: TR_REORDER_LABEL, "label": TR_REORDER_LABEL, "tca": TR_REORDER_TCA}
+
+
+def plan_opts(row_scale=False, promote_min=0, transpose=False, reorder=False, demote_below=0):
+    """(tr_plan_opts, keep-alive array).  ``reorder``: False / "none", True /
+    "label" (label propagation), "tca" (TCA clustering, tr_tca_order's
+    defaults) or an int array, the caller's row permutation (plan row i is row
+    reorder[i] of the matrix the plan is built for: A, or A^T when
+    transpose)."""
+    order = None
+    if isinstance(reorder, (str, bool)) or reorder is None:
+        if reorder not in REORDER_MODES:
+            raise ValueError(f"unknown reorder mode {reorder!r}")
+        mode = REORDER_MODES[reorder]
+    else:
+        order = np.ascontiguousarray(reorder, dtype=np.int32)
+        mode = TR_REORDER_GIVEN
+    opts = PlanOpts(int(bool(row_scale)), int(promote_min), int(bool(transpose)), int(mode),
+                    int(demote_below), _vp(order) if order is not None else ctypes.c_void_p(0))
+    return opts, order
 
 
 def _params(partsize_t=32, partsize_c=32, shortsize=3, density=8, window=16, wide=16,
@@ -226,8 +250,7 @@ class Plan:
         ci = np.ascontiguousarray(indices, dtype=np.int32)
         vv = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
         prm = _params(mode=mode, **route_kw)
-        opts = PlanOpts(int(bool(row_scale)), int(promote_min), int(bool(transpose)),
-                        int(bool(reorder)), int(demote_below))
+        opts, keep = plan_opts(row_scale, promote_min, transpose, reorder, demote_below)
         h = ctypes.c_void_p()
         check(lib().tr_plan_build(_vp(rp), _vp(ci), _vp(vv), int(n_rows), int(n_cols),
                                   ctypes.byref(prm), ctypes.byref(opts), ctypes.byref(h)))
@@ -354,8 +377,7 @@ def host_plan(indptr, indices, values, n_rows, n_cols, row_scale=False, promote_
     ci = np.ascontiguousarray(indices, dtype=np.int32)
     vv = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
     prm = _params(mode=mode, **route_kw)
-    opts = PlanOpts(int(bool(row_scale)), int(promote_min), int(bool(transpose)),
-                    int(bool(reorder)), int(demote_below))
+    opts, keep = plan_opts(row_scale, promote_min, transpose, reorder, demote_below)
     L = lib()
     h = ctypes.c_void_p()
     check(L.tr_plan_build_host(_vp(rp), _vp(ci), _vp(vv), int(n_rows), int(n_cols),
@@ -409,6 +431,31 @@ def sddmm_csr(indptr, indices, x, y, out=None, stream=None):
                              ctypes.c_void_p(y.data_ptr()), int(x.shape[1]),
                              ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(s)))
     return out
+
+
+def tca_order(indptr, indices, n_rows=None, thres=16, cluster_thres=128, lsh_threshold=0.2,
+              seed=1, max_pairs=1 << 25, device=False):
+    """TCA row order of a host CSR (tr_tca_order): (order int32 [n_rows],
+    new position -> old row; stats dict).  ``device=True`` computes the
+    MinHash signatures and the Jaccard similarities on the current GPU."""
+    rp = np.ascontiguousarray(indptr, dtype=np.int32)
+    ci = np.ascontiguousarray(indices, dtype=np.int32)
+    n = int(rp.shape[0] - 1) if n_rows is None else int(n_rows)
+    if rp.shape[0] < n + 1:
+        raise ValueError("indptr shorter than n_rows + 1")
+    prm = TcaParams(int(thres), int(cluster_thres), float(lsh_threshold), int(seed),
+                    int(max_pairs), int(bool(device)))
+    order = np.empty(max(n, 0), dtype=np.int32)
+    st = TcaStats()
+    check(lib().tr_tca_order(_vp(rp), _vp(ci), n, ctypes.byref(prm), _vp(order), ctypes.byref(st)))
+    return order, {name: getattr(st, name) for name, _ in TcaStats._fields_}
+
+
+def lsh_params(threshold=0.2, num_perm=128):
+    """(bands, rows per band) of the LSH banding tr_tca_order uses."""
+    b, r = ctypes.c_int32(), ctypes.c_int32()
+    check(lib().tr_lsh_params(float(threshold), int(num_perm), ctypes.byref(b), ctypes.byref(r)))
+    return b.value, r.value
 
 
 MATCH_VARIANTS = {"sliding": TR_MATCH_SLIDING, "hash": TR_MATCH_HASH, "bucket": TR_MATCH_BUCKET,

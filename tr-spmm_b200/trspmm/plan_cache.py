@@ -22,7 +22,7 @@ import os
 import numpy as np
 
 from . import core
-from ._lib import PlanOpts, TrError, check, lib
+from ._lib import TrError, check, lib
 
 FORMAT = 1          # bump when the plan layout or the key's meaning changes
 
@@ -34,8 +34,14 @@ def default_dir():
 
 def _options(row_scale=False, promote_min=0, transpose=False, reorder=False, demote_below=0,
              mode="exact", **route_kw):
+    if not (isinstance(reorder, (str, bool)) or reorder is None):
+        raise ValueError("the plan cache takes named reorder modes (False, True / 'label', 'tca')")
+    if reorder not in core.REORDER_MODES:
+        raise ValueError(f"unknown reorder mode {reorder!r}")
+    # False / True as before ('none' / 'label'), 'tca' by name
+    reorder = {0: False, 1: True, 2: "tca"}[core.REORDER_MODES[reorder]]
     opts = {"row_scale": bool(row_scale), "promote_min": int(promote_min),
-            "transpose": bool(transpose), "reorder": bool(reorder),
+            "transpose": bool(transpose), "reorder": reorder,
             "demote_below": int(demote_below), "mode": mode}
     return opts, route_kw
 
@@ -63,8 +69,8 @@ def _build_host(indptr, indices, values, n_rows, n_cols, **plan_kw):
     ci = np.ascontiguousarray(indices, dtype=np.int32)
     vv = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
     prm = core._params(mode=opts["mode"], **route_kw)
-    po = PlanOpts(int(opts["row_scale"]), opts["promote_min"], int(opts["transpose"]),
-                  int(opts["reorder"]), opts["demote_below"])
+    po, _ = core.plan_opts(opts["row_scale"], opts["promote_min"], opts["transpose"],
+                           opts["reorder"], opts["demote_below"])
     h = ctypes.c_void_p()
     check(lib().tr_plan_build_host(core._vp(rp), core._vp(ci), core._vp(vv), int(n_rows),
                                    int(n_cols), ctypes.byref(prm), ctypes.byref(po),
