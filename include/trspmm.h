@@ -380,6 +380,24 @@ int tr_sddmm_csr(const int32_t* indptr, const int32_t* indices, int32_t m, int32
                  int64_t nnz, const uint16_t* x, const uint16_t* y, int32_t k, float* out,
                  void* stream);
 
+/* FP32-feature route (replaces the reference's TF32 route for FP32
+ * features, TR-source/SpMM/mGCNkernel.cu:2885-3031 and :3513-3674, which no
+ * reference operator binds): C = A_plan . B with B [n_cols, k] FP32 on the
+ * CUDA cores in FP32 -- the residual on the segment engine (4 features per
+ * 16-byte load), the plan's tiles (dense TC, 2:4, promoted) by a CUDA-core
+ * tile pass added to C.  A keeps the plan's precision (FP16 significand,
+ * FP32 row scale when row-scaled, as precise as TF32); B is not rounded
+ * (TF32 would keep 10 of its 23 fraction bits).  c [n_rows, k] FP32 or FP16,
+ * every row overwritten; route_mask as in tr_spmm_routed (TR_ROUTE_ALL
+ * bits).  K % 4 == 0 with 16-byte aligned b and c takes the vector kernels,
+ * anything else a scalar kernel. */
+int tr_spmm_routed_f32(const tr_plan* p, const float* b, int32_t k, void* c, int c_dtype,
+                       int route_mask, void* stream);
+/* tr_sddmm_csr with FP32 x [m, k] and y [n_cols, k]. */
+int tr_sddmm_csr_f32(const int32_t* indptr, const int32_t* indices, int32_t m, int32_t n_cols,
+                     int64_t nnz, const float* x, const float* y, int32_t k, float* out,
+                     void* stream);
+
 /* ------------------------------------------------------------------------
  * Reference-compatible entry points (host tensors in, FP32 host out; device
  * memory allocated, copied and freed inside each call; `epoches` timed

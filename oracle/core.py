@@ -301,9 +301,9 @@ def decode_plan(P):
     element (n, k) of tile t sits at (n//8)*128 + (k//8)*64 + (n%8)*8 + k%8
     and multiplies B[tile_col[t*16+k]] into plan row 16*w + n; residual
     entries are CSR over plan rows; every plan row r is scaled by
-    row_scale[r] and lands in output row row_out[r].  Returns
-    {'tiles': (tc, sptc, promoted) CSR float64 matrices, 'res', 'all'} in the
-    output row space, values as the kernels see them (FP16 x FP32 scale)."""
+    row_scale[r] and lands in output row row_out[r].  Returns CSR float64
+    matrices {'tc', 'sptc', 'prom' (tile parts), 'res', 'all'} in the output
+    row space, values as the kernels see them (FP16 x FP32 scale)."""
     n_rows, n_cols = int(P["n_rows"]), int(P["n_cols"])
     wt, split, prom = P["win_tile"], P["win_split"], P["win_prom"]
     W = len(wt) - 1

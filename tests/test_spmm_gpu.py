@@ -170,8 +170,11 @@ def test_bad_device_arguments_raise(cuda):
     plan = trspmm.Plan.from_csr(g.indptr, g.indices, g.values, g.n_rows, g.n_cols)
     with pytest.raises(RuntimeError):
         plan.spmm(torch.zeros((41, 8), dtype=torch.float16, device=cuda))
+    for dt in (torch.float64, torch.bfloat16):       # FP32 B is the FP32-feature route
+        with pytest.raises(RuntimeError):
+            plan.spmm(torch.zeros((40, 8), dtype=dt, device=cuda))
     with pytest.raises(RuntimeError):
-        plan.spmm(torch.zeros((40, 8), dtype=torch.float32, device=cuda))
+        plan.spmm(torch.zeros((41, 8), dtype=torch.float32, device=cuda))
     tabs = trspmm.route(g.indptr, g.indices, g.values)
     for idx in (10, 15, 25):          # CUDA long / short / SPTC tile columns out of range
         if tabs[idx].size == 0:

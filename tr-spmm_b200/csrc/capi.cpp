@@ -432,6 +432,24 @@ int tr_spmm_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int 
                        (cudaStream_t)stream);
 }
 
+int tr_spmm_routed_f32(const tr_plan* p, const float* b, int32_t k, void* c, int c_dtype,
+                       int route_mask, void* stream) {
+  if (!p) return fail(TR_ERR_ARG, "null plan");
+  if (k < 0) return fail(TR_ERR_ARG, "negative K");
+  if (c_dtype != TR_OUT_F32 && c_dtype != TR_OUT_F16) return fail(TR_ERR_ARG, "bad output dtype");
+  if (p->view.n_rows > 0 && k > 0 && (!b || !c)) return fail(TR_ERR_ARG, "null device pointer");
+  return launch_routed_f32(p, b, k, c, c_dtype, route_mask & TR_ROUTE_ALL, (cudaStream_t)stream);
+}
+
+int tr_sddmm_csr_f32(const int32_t* indptr, const int32_t* indices, int32_t m, int32_t n_cols,
+                     int64_t nnz, const float* x, const float* y, int32_t k, float* out,
+                     void* stream) {
+  if (m < 0 || n_cols < 0 || nnz < 0 || k < 0) return fail(TR_ERR_ARG, "negative size");
+  if (nnz > 0 && (!indptr || !indices || !out || (k > 0 && (!x || !y))))
+    return fail(TR_ERR_ARG, "null device pointer");
+  return launch_sddmm_f32(indptr, indices, m, nnz, x, y, k, out, (cudaStream_t)stream);
+}
+
 int tr_plan_set_values(tr_plan* p, const float* values, int64_t n_edges, void* stream) {
   if (!p) return fail(TR_ERR_ARG, "null plan");
   if (n_edges != p->n_edges)

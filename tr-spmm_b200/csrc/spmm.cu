@@ -74,6 +74,20 @@ __device__ __forceinline__ void fma8h(float (&acc)[8], uint16_t v, const uint4& 
   }
 }
 
+// acc[0..3] += v * b[0..3]: FP16 plan value, FP32 features (16 bytes of a B
+// row) and accumulation.
+__device__ __forceinline__ void fma4f(float (&acc)[4], uint16_t v, const uint4& b) {
+  const float fv = __half2float(__ushort_as_half(v));
+  acc[0] = fmaf(__uint_as_float(b.x), fv, acc[0]);
+  acc[1] = fmaf(__uint_as_float(b.y), fv, acc[1]);
+  acc[2] = fmaf(__uint_as_float(b.z), fv, acc[2]);
+  acc[3] = fmaf(__uint_as_float(b.w), fv, acc[3]);
+}
+
+// One entry's contribution to a lane's features, by feature type.
+__device__ __forceinline__ void seg_fma(float (&acc)[8], uint16_t v, const uint4& b) { fma8h(acc, v, b); }
+__device__ __forceinline__ void seg_fma(float (&acc)[4], uint16_t v, const uint4& b) { fma4f(acc, v, b); }
+
 __device__ __forceinline__ void stage_chunk(const int32_t* __restrict__ col,
                                             const __half* __restrict__ val, int e0, int n,
                                             int2* sent) {
@@ -188,9 +202,14 @@ constexpr int kSegU = 4;                             // entries per lane group a
 template <int S = kSegStrideW>
 __device__ __forceinline__ int seg_slot_w(int r, int f) { return r * S + f + (f >> 5); }
 
+// Features per 16-byte load of a B row: 8 FP16 or 4 FP32 (the FP32-feature
+// route); a pass covers 32 lanes' worth (256 FP16 / 128 FP32 features).
+template <class TB> struct SegFeat { static constexpr int kPer = 8; };
+template <> struct SegFeat<float> { static constexpr int kPer = 4; };
+
 // 16 bytes of B row `col` at the lane's feature base Bf.
-template <bool WIDE>
-__device__ __forceinline__ uint4 seg_ldg(const __half* Bf, int col, uint32_t K) {
+template <bool WIDE, class TB>
+__device__ __forceinline__ uint4 seg_ldg(const TB* Bf, int col, uint32_t K) {
   return __ldg(reinterpret_cast<const uint4*>(
       WIDE ? Bf + (size_t)(uint32_t)col * K : Bf + (uint32_t)col * K));
 }
@@ -237,14 +256,17 @@ __device__ __forceinline__ void store_vec(void* C, int K, int64_t row, int f, co
 
 // With PLAN the rows are a plan's rows: result row r is scaled by
 // row_scale[r] and stored to row_out[r] (skipped when negative).  Without
-// WIDE, B offsets are 32-bit (requires (number of B rows) * K < 2^31).
-template <bool F16OUT, bool PLAN, bool WIDE>
+// WIDE, B offsets are 32-bit (requires (number of B rows) * K < 2^31).  TB is
+// the feature type: __half, or float for the FP32-feature route (FP32 B,
+// FP16 plan values widened to FP32, FP32 accumulation).
+template <bool F16OUT, bool PLAN, bool WIDE, class TB = __half>
 __global__ void __launch_bounds__(kThreads, 4) seg_block_kernel(
     const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
-    const __half* __restrict__ values, int M, const __half* __restrict__ B, int K, void* C,
+    const __half* __restrict__ values, int M, const TB* __restrict__ B, int K, void* C,
     const int32_t* __restrict__ row_out, const float* __restrict__ row_scale,
     const int32_t* __restrict__ order) {
   constexpr int U = kSegU;
+  constexpr int NPL = SegFeat<TB>::kPer, PASS = 32 * NPL;   // features per lane / per pass
   __shared__ __align__(16) float racc[kBlockRows * kSegStrideW];
   __shared__ __align__(16) int2 sent[kStage + 2];
   __shared__ int rp[kBlockRows + 1];
@@ -262,20 +284,20 @@ __global__ void __launch_bounds__(kThreads, 4) seg_block_kernel(
   __syncthreads();
   const int e_begin = rp[0], e_end = rp[kBlockRows];
   const uint32_t uK = (uint32_t)K;
-  for (int f0 = 0; f0 < K; f0 += kSegChunk) {
-    const int fc = min(kSegChunk, K - f0);
+  for (int f0 = 0; f0 < K; f0 += PASS) {
+    const int fc = min(PASS, K - f0);
     int L = 1;
-    while (L * 8 < fc) L <<= 1;
+    while (L * NPL < fc) L <<= 1;
     const int G = 32 / L, groups = kWarps * G;
     const int li = lane % L, q = warp * G + lane / L;
-    const bool active = li * 8 < fc;
+    const bool active = li * NPL < fc;
     if (tid < kBlockRows) s_own[tid] = seg_owned(rp[tid], rp[tid + 1], e_begin, e_end, groups);
     {
       float4* z = reinterpret_cast<float4*>(racc);
       for (int i = tid; i < kBlockRows * kSegStrideW / 4; i += kThreads) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    const __half* Bf = B + f0 + (active ? li * 8 : 0);
-    float* dst = racc + seg_slot_w(0, active ? li * 8 : 0);
+    const TB* Bf = B + f0 + (active ? li * NPL : 0);
+    float* dst = racc + seg_slot_w(0, active ? li * NPL : 0);
     for (int c0 = e_begin; c0 < e_end; c0 += kStage) {
       const int n = min(kStage, e_end - c0);
       __syncthreads();                       // previous chunk consumed, racc zeroed
@@ -289,17 +311,17 @@ __global__ void __launch_bounds__(kThreads, 4) seg_block_kernel(
       int r = 0;
       while (r < kBlockRows - 1 && rp[r + 1] <= c0 + lo) ++r;
       int nb = rp[r + 1] - c0;               // chunk-relative end of row r
-      float acc[8];
+      float acc[NPL];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) acc[i] = 0.f;
+      for (int i = 0; i < NPL; ++i) acc[i] = 0.f;
       // row r is done for this group: owned rows go to C, cut rows to racc
       auto flush = [&]() {
         if (!active) return;
         if (rp[r] >= c0 + lo && rp[r + 1] <= c0 + hi) {
-          if (s_out[r] >= 0) store_vec<F16OUT, 8>(C, K, s_out[r], f0 + li * 8, acc, s_scale[r]);
+          if (s_out[r] >= 0) store_vec<F16OUT, NPL>(C, K, s_out[r], f0 + li * NPL, acc, s_scale[r]);
         } else {
 #pragma unroll
-          for (int i = 0; i < 8; ++i) atomicAdd(dst + r * kSegStrideW + i, acc[i]);
+          for (int i = 0; i < NPL; ++i) atomicAdd(dst + r * kSegStrideW + i, acc[i]);
         }
       };
 #pragma unroll 1
@@ -327,7 +349,7 @@ __global__ void __launch_bounds__(kThreads, 4) seg_block_kernel(
         }
         if (__all_sync(0xffffffffu, t + U <= nb && t + U <= hi)) {   // no boundary, full
 #pragma unroll
-          for (int u = 0; u < U; ++u) fma8h(acc, (uint16_t)(v[u / 2] >> (16 * (u & 1))), b[u]);
+          for (int u = 0; u < U; ++u) seg_fma(acc, (uint16_t)(v[u / 2] >> (16 * (u & 1))), b[u]);
         } else {
 #pragma unroll
           for (int u = 0; u < U; ++u) {
@@ -336,11 +358,11 @@ __global__ void __launch_bounds__(kThreads, 4) seg_block_kernel(
               if (j >= nb) {                   // row r ends before entry j
                 flush();
 #pragma unroll
-                for (int i = 0; i < 8; ++i) acc[i] = 0.f;
+                for (int i = 0; i < NPL; ++i) acc[i] = 0.f;
                 do ++r; while (rp[r + 1] - c0 <= j);
                 nb = rp[r + 1] - c0;
               }
-              fma8h(acc, (uint16_t)(v[u / 2] >> (16 * (u & 1))), b[u]);
+              seg_fma(acc, (uint16_t)(v[u / 2] >> (16 * (u & 1))), b[u]);
             }
           }
           __syncwarp();                      // reconverge the lane groups
@@ -611,8 +633,11 @@ __global__ void __launch_bounds__(kThreads, 3) routed_kernel(PlanView pv, const 
 }
 
 // Any K: one thread per (window row, feature), scalar loads.
-template <bool F16OUT>
-__global__ void routed_generic_kernel(PlanView pv, const __half* __restrict__ B, int K, void* C,
+__device__ __forceinline__ float feat_f32(__half x) { return __half2float(x); }
+__device__ __forceinline__ float feat_f32(float x) { return x; }
+
+template <bool F16OUT, class TB = __half>
+__global__ void routed_generic_kernel(PlanView pv, const TB* __restrict__ B, int K, void* C,
                                       int route_mask) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= (int64_t)pv.n_rows * K) return;
@@ -627,16 +652,137 @@ __global__ void routed_generic_kernel(PlanView pv, const __half* __restrict__ B,
       const int c = pv.tile_col[(int64_t)t * 16 + k];
       if (c < 0) continue;
       const uint16_t a = pv.tile_a[(int64_t)t * 256 + (n / 8) * 128 + (k / 8) * 64 + (n % 8) * 8 + k % 8];
-      acc = fmaf(__half2float(__ushort_as_half(a)), __half2float(B[(int64_t)c * K + f]), acc);
+      acc = fmaf(__half2float(__ushort_as_half(a)), feat_f32(B[(int64_t)c * K + f]), acc);
     }
   }
   if (route_mask & TR_ROUTE_CUDA) {
     for (int e = pv.res_ptr[row]; e < pv.res_ptr[row + 1]; ++e)
       acc = fmaf(__half2float(__ushort_as_half(pv.res_val[e])),
-                 __half2float(B[(int64_t)pv.res_col[e] * K + f]), acc);
+                 feat_f32(B[(int64_t)pv.res_col[e] * K + f]), acc);
   }
   const int out = pv.row_out[row];
   if (out >= 0) store_row_feature<F16OUT>(C, K, out, f, acc * pv.row_scale[row]);
+}
+
+// ---------------------------------------------------------------------------
+// FP32-feature tile pass (CUDA cores)
+// ---------------------------------------------------------------------------
+// The plan's 16x16 tiles (dense TC, 2:4 and promoted columns) times FP32
+// features, added to C (which the residual pass has written): one CTA per
+// window, warp i takes the window's tiles i, i + 8, ...  Tiles are mostly
+// empty slots (a 2:4 tile holds at most half, on power-law graphs a few
+// percent), so a warp first compacts its tile's nonzeros: lane l holds 8
+// values of one row (row (l/16)*8 + l%8, columns 8*((l/8)%2) .. +7), counts
+// its nonzeros, and a warp prefix sum places them, lane by lane, into a
+// per-warp list of (column of B, row, value).  The warp then streams the
+// list like residual entries: lanes over features (one 16-byte load of 4
+// FP32 features per entry and lane, 4 entries in flight), the row sum in
+// registers, added into the window's shared rows at each row change.
+constexpr int kTileF32Chunk = 128;
+constexpr int kTileF32Stride = kTileF32Chunk + kTileF32Chunk / 32;    // padded shared row
+
+template <bool F16OUT>
+__global__ void __launch_bounds__(kThreads) tile_f32_kernel(PlanView pv, const float* __restrict__ B,
+                                                           int K, void* C, int route_mask) {
+  __shared__ __align__(16) float racc[kBlockRows * kTileF32Stride];
+  __shared__ __align__(16) int2 ent[kWarps][256 + 4];    // (column, row | value << 16)
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int w = pv.win_order[blockIdx.x];
+  int ta0, ta1, tb0, tb1;
+  route_ranges(pv, w, route_mask, ta0, ta1, tb0, tb1);
+  const int n_tc = ta1 - ta0, nt = n_tc + (tb1 - tb0);
+  if (nt == 0) return;                       // the whole CTA: no tiles in this window
+  const int my_row = (lane >> 4) * 8 + (lane & 7), my_k0 = ((lane >> 3) & 1) * 8;
+  for (int f0 = 0; f0 < K; f0 += kTileF32Chunk) {
+    const int fc = min(kTileF32Chunk, K - f0);
+    const bool active = lane * 4 < fc;
+    for (int i = tid; i < kBlockRows * kTileF32Stride; i += kThreads) racc[i] = 0.f;
+    __syncthreads();
+    const float* Bf = B + f0 + (active ? lane * 4 : 0);
+    float* dst = racc + seg_slot_w<kTileF32Stride>(0, active ? lane * 4 : 0);
+    for (int ti = warp; ti < nt; ti += kWarps) {
+      const int t = ti < n_tc ? ta0 + ti : tb0 + (ti - n_tc);
+      // ---- compact the tile's nonzeros into ent[warp][0 .. nz) -------------
+      const uint4 q = __ldg(reinterpret_cast<const uint4*>(pv.tile_a + (int64_t)t * 256) + lane);
+      const uint32_t hv[4] = {q.x, q.y, q.z, q.w};
+      const int my_col = lane < 16 ? __ldg(pv.tile_col + (int64_t)t * 16 + lane) : -1;
+      int cj[8];
+      int cnt = 0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        // a slot counts when its value is nonzero and its column is a column
+        // of B (an empty column slot holds zeros)
+        cj[j] = __shfl_sync(0xffffffffu, my_col, my_k0 + j);
+        if (((hv[j >> 1] >> (16 * (j & 1))) & 0x7FFFu) == 0) cj[j] = -1;
+        cnt += cj[j] >= 0 ? 1 : 0;
+      }
+      int pos = cnt;                          // inclusive warp scan
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, pos, off);
+        if (lane >= off) pos += y;
+      }
+      const int nz = __shfl_sync(0xffffffffu, pos, 31);
+      pos -= cnt;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const uint32_t h = (hv[j >> 1] >> (16 * (j & 1))) & 0xFFFFu;
+        if (cj[j] >= 0) ent[warp][pos++] = make_int2(cj[j], my_row | (int)(h << 16));
+      }
+      __syncwarp();
+      // ---- stream the entries ------------------------------------------------
+      float acc[4] = {0.f, 0.f, 0.f, 0.f};
+      int cur = nz > 0 ? (ent[warp][0].y & 0xFFFF) : 0;
+#pragma unroll 1
+      for (int e0 = 0; e0 < nz; e0 += 4) {
+        int2 p[4];
+        uint4 b[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          p[u] = ent[warp][min(e0 + u, nz - 1)];
+          b[u] = (active && e0 + u < nz)
+                     ? __ldg(reinterpret_cast<const uint4*>(Bf + (int64_t)p[u].x * K))
+                     : make_uint4(0u, 0u, 0u, 0u);
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          if (e0 + u < nz) {                  // warp-uniform
+            const int r = p[u].y & 0xFFFF;
+            if (r != cur) {
+              if (active)
+#pragma unroll
+                for (int i = 0; i < 4; ++i) atomicAdd(dst + cur * kTileF32Stride + i, acc[i]);
+              acc[0] = acc[1] = acc[2] = acc[3] = 0.f;
+              cur = r;
+            }
+            fma4f(acc, (uint16_t)((uint32_t)p[u].y >> 16), b[u]);
+          }
+        }
+      }
+      if (nz > 0 && active)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) atomicAdd(dst + cur * kTileF32Stride + i, acc[i]);
+      __syncwarp();                          // ent[warp] is rewritten by the next tile
+    }
+    __syncthreads();
+    for (int r = warp; r < kBlockRows; r += kWarps) {
+      const int64_t pr = (int64_t)w * kBlockRows + r;
+      const int out = pv.row_out[pr];
+      if (out < 0) continue;
+      const float sc = pv.row_scale[pr];
+      for (int f = lane; f < fc; f += 32) {
+        const int64_t at = (int64_t)out * K + f0 + f;
+        const float x = racc[seg_slot_w<kTileF32Stride>(r, f)] * sc;
+        if (F16OUT) {
+          __half* cp = reinterpret_cast<__half*>(C) + at;
+          *cp = __float2half_rn(__half2float(*cp) + x);
+        } else {
+          reinterpret_cast<float*>(C)[at] += x;
+        }
+      }
+    }
+    __syncthreads();                         // racc is cleared for the next chunk
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -691,13 +837,24 @@ __device__ __forceinline__ float dot8h(const uint4& a, const uint4& b) {
   return acc;
 }
 
+// The FP32-feature form: 4 FP32 products per 16-byte chunk.
+__device__ __forceinline__ float dot4f(const uint4& a, const uint4& b) {
+  float acc = __uint_as_float(a.x) * __uint_as_float(b.x);
+  acc = fmaf(__uint_as_float(a.y), __uint_as_float(b.y), acc);
+  acc = fmaf(__uint_as_float(a.z), __uint_as_float(b.z), acc);
+  return fmaf(__uint_as_float(a.w), __uint_as_float(b.w), acc);
+}
+__device__ __forceinline__ float dot_chunk(const uint4& a, const uint4& b, __half) { return dot8h(a, b); }
+__device__ __forceinline__ float dot_chunk(const uint4& a, const uint4& b, float) { return dot4f(a, b); }
+
+template <class TB = __half>
 __global__ void __launch_bounds__(256) sddmm_kernel(const int32_t* __restrict__ indptr,
                                                     const int32_t* __restrict__ indices, int M,
-                                                    const __half* __restrict__ X,
-                                                    const __half* __restrict__ Y, int K,
+                                                    const TB* __restrict__ X,
+                                                    const TB* __restrict__ Y, int K,
                                                     float* __restrict__ out) {
   const int lane = threadIdx.x & 31;
-  const int nchunk = K / 8;
+  const int nchunk = K / SegFeat<TB>::kPer;
   int L = 1;
   while (L < nchunk && L < 32) L <<= 1;
   const int G = 32 / L, g = lane / L, li = lane % L;
@@ -710,7 +867,7 @@ __global__ void __launch_bounds__(256) sddmm_kernel(const int32_t* __restrict__ 
       float acc = 0.f;
       if (e < e1) {
         const uint4* yr = reinterpret_cast<const uint4*>(Y + (int64_t)__ldg(indices + e) * K);
-        for (int c = li; c < nchunk; c += L) acc += dot8h(__ldg(xr + c), __ldg(yr + c));
+        for (int c = li; c < nchunk; c += L) acc += dot_chunk(__ldg(xr + c), __ldg(yr + c), TB());
       }
       for (int off = 1; off < L; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
       if (li == 0 && e < e1) out[e] = acc;
@@ -718,23 +875,25 @@ __global__ void __launch_bounds__(256) sddmm_kernel(const int32_t* __restrict__ 
   }
 }
 
-// K = 8 * L with L in {8, 16, 32}: groups of L lanes, one row per group, the
-// lane's 16-byte chunk of the row of x held in a register.  A group takes
-// the row's entries U at a time: every lane loads its chunk of the U rows of
-// y (coalesced: the group reads whole rows), forms U partial dot products,
-// and the group finishes them with a reduce-scatter over its lanes (each
-// step halves the values a lane holds and the lanes that share them), after
-// which lane i holds entry i's sum: L - 1 shuffles per U entries instead of
-// log2(L) per entry, and U loads in flight per lane.  Groups of one warp
-// step through their rows' batches together (warp-uniform trip count, idle
-// groups predicated), so every shuffle sees the whole warp.
-template <int L>
+// K = L * CH * (8 FP16 or 4 FP32 features) with L in {8, 16, 32} lanes and
+// CH 16-byte chunks per lane: groups of L lanes, one row per group, the
+// lane's chunks of the row of x held in registers.  A group takes the row's
+// entries U at a time: every lane loads its chunks of the U rows of y
+// (coalesced: the group reads whole rows), forms U partial dot products, the
+// lanes are folded down to U, and the group finishes the sums with a
+// reduce-scatter over its lanes (each step halves the values a lane holds
+// and the lanes that share them), after which lane i holds entry i's sum:
+// U - 1 shuffles per U entries instead of log2(L) per entry, and U * CH
+// loads in flight per lane.  Groups of one warp step through their rows'
+// batches together (warp-uniform trip count, idle groups predicated), so
+// every shuffle sees the whole warp.
+template <int L, int CH = 1, class TB = __half>
 __global__ void __launch_bounds__(256) sddmm_group_kernel(const int32_t* __restrict__ indptr,
                                                           const int32_t* __restrict__ indices,
-                                                          int M, const __half* __restrict__ X,
-                                                          const __half* __restrict__ Y,
+                                                          int M, const TB* __restrict__ X,
+                                                          const TB* __restrict__ Y,
                                                           float* __restrict__ out) {
-  constexpr int K = L * 8, G = 32 / L, U = L > 16 ? 16 : L;
+  constexpr int K = L * CH * SegFeat<TB>::kPer, G = 32 / L, U = (L > 16 ? 16 : L) / CH;
   const int lane = threadIdx.x & 31, grp = lane / L, li = lane % L;
   const int warps = gridDim.x * (blockDim.x >> 5);
   const int warp_id = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -742,8 +901,11 @@ __global__ void __launch_bounds__(256) sddmm_group_kernel(const int32_t* __restr
     const int r = rb + grp;
     const bool has_row = r < M;
     const int e0 = has_row ? __ldg(indptr + r) : 0, e1 = has_row ? __ldg(indptr + r + 1) : 0;
-    const uint4 xv = has_row ? __ldg(reinterpret_cast<const uint4*>(X + (int64_t)r * K) + li)
-                             : make_uint4(0, 0, 0, 0);
+    uint4 xv[CH];
+#pragma unroll
+    for (int h = 0; h < CH; ++h)
+      xv[h] = has_row ? __ldg(reinterpret_cast<const uint4*>(X + (int64_t)r * K) + li + h * L)
+                      : make_uint4(0, 0, 0, 0);
     int nb = (e1 - e0 + U - 1) / U;
 #pragma unroll
     for (int off = L; off < 32; off <<= 1) nb = max(nb, __shfl_xor_sync(0xffffffffu, nb, off));
@@ -753,19 +915,31 @@ __global__ void __launch_bounds__(256) sddmm_group_kernel(const int32_t* __restr
       // eb + li), then broadcast; every row load is issued before any use,
       // slots past the row's end reading row 0 and being dropped
       const int my_c = (li < U && eb + li < e1) ? __ldg(indices + eb + li) : 0;
-      uint4 yv[U];
+      uint4 yv[U][CH];
 #pragma unroll
       for (int u = 0; u < U; ++u) {
         const int c = __shfl_sync(0xffffffffu, my_c, grp * L + u);
-        yv[u] = __ldg(reinterpret_cast<const uint4*>(Y + (int64_t)c * K) + li);
+#pragma unroll
+        for (int h = 0; h < CH; ++h)
+          yv[u][h] = __ldg(reinterpret_cast<const uint4*>(Y + (int64_t)c * K) + li + h * L);
       }
       float v[U];
 #pragma unroll
-      for (int u = 0; u < U; ++u) v[u] = eb + u < e1 ? dot8h(xv, yv[u]) : 0.f;
-      if (L > U) {                                // K = 256: first fold the two half-groups
+      for (int u = 0; u < U; ++u) {
+        if constexpr (CH == 1) {
+          v[u] = eb + u < e1 ? dot_chunk(xv[0], yv[u][0], TB()) : 0.f;
+        } else {
+          float d = dot_chunk(xv[0], yv[u][0], TB());
 #pragma unroll
-        for (int u = 0; u < U; ++u) v[u] += __shfl_xor_sync(0xffffffffu, v[u], 16);
+          for (int h = 1; h < CH; ++h) d += dot_chunk(xv[h], yv[u][h], TB());
+          v[u] = eb + u < e1 ? d : 0.f;
+        }
       }
+      // fold the group's lanes down to U (lane bits above log2(U))
+#pragma unroll
+      for (int off = L / 2; off >= U; off >>= 1)
+#pragma unroll
+        for (int u = 0; u < U; ++u) v[u] += __shfl_xor_sync(0xffffffffu, v[u], off);
       // reduce-scatter over U lanes (lane bits li % U): value index bits follow lane bits
 #pragma unroll
       for (int c = U; c > 1; c >>= 1) {
@@ -964,16 +1138,17 @@ __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
 }
 
 // Any K: one thread per entry.
+template <class TB = __half>
 __global__ void sddmm_generic_kernel(const int32_t* __restrict__ indptr,
                                      const int32_t* __restrict__ indices, int M,
-                                     const __half* __restrict__ X, const __half* __restrict__ Y,
+                                     const TB* __restrict__ X, const TB* __restrict__ Y,
                                      int K, float* __restrict__ out) {
   for (int r = blockIdx.x; r < M; r += gridDim.x)
     for (int e = indptr[r] + threadIdx.x; e < indptr[r + 1]; e += blockDim.x) {
       const int64_t c = indices[e];
       float acc = 0.f;
       for (int f = 0; f < K; ++f)
-        acc = fmaf(__half2float(X[(int64_t)r * K + f]), __half2float(Y[c * K + f]), acc);
+        acc = fmaf(feat_f32(X[(int64_t)r * K + f]), feat_f32(Y[c * K + f]), acc);
       out[e] = acc;
     }
 }
@@ -1093,6 +1268,72 @@ int launch_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c
   const int blocks = (int)((n + 255) / 256);
   if (f16) routed_generic_kernel<true><<<blocks, 256, 0, stream>>>(v, bh, k, c, route_mask);
   else routed_generic_kernel<false><<<blocks, 256, 0, stream>>>(v, bh, k, c, route_mask);
+  TRS_CUDA(cudaGetLastError());
+  return TR_OK;
+}
+
+// FP32-feature route: the residual on the segment engine with FP32 B rows
+// (writes every output row; zeros are stored instead when the residual is
+// not selected), then the selected tiles on CUDA cores added to C.  K not a
+// multiple of 4 or unaligned buffers take the scalar kernel.
+int launch_routed_f32(const tr_plan* p, const float* b, int32_t k, void* c, int c_dtype,
+                      int route_mask, cudaStream_t stream) {
+  const PlanView& v = p->view;
+  if (v.n_rows == 0 || k == 0) return TR_OK;
+  const bool f16 = c_dtype == TR_OUT_F16;
+  route_mask &= TR_ROUTE_ALL;
+  const bool vec = k % 4 == 0 && aligned16(b) && aligned16(c);
+  if (!vec) {
+    const int64_t n = (int64_t)v.n_rows * k;
+    const int blocks = (int)((n + 255) / 256);
+    if (f16) routed_generic_kernel<true, float><<<blocks, 256, 0, stream>>>(v, b, k, c, route_mask);
+    else routed_generic_kernel<false, float><<<blocks, 256, 0, stream>>>(v, b, k, c, route_mask);
+    TRS_CUDA(cudaGetLastError());
+    return TR_OK;
+  }
+  if (route_mask & TR_ROUTE_CUDA) {
+    const int rows = v.n_windows * kBlockRows;
+    const __half* rv = reinterpret_cast<const __half*>(v.res_val);
+    const bool wide = (int64_t)v.n_cols * k >= ((int64_t)1 << 31);
+#define TRS_SEGF32(F16, W)                                                                   \
+  seg_block_kernel<F16, true, W, float><<<v.n_windows, kThreads, 0, stream>>>(                \
+      v.res_ptr, v.res_col, rv, rows, b, k, c, v.row_out, v.row_scale, v.win_order)
+    if (f16) { if (wide) TRS_SEGF32(true, true); else TRS_SEGF32(true, false); }
+    else { if (wide) TRS_SEGF32(false, true); else TRS_SEGF32(false, false); }
+#undef TRS_SEGF32
+    TRS_CUDA(cudaGetLastError());
+  } else {
+    TRS_CUDA(cudaMemsetAsync(c, 0, (size_t)v.n_rows * k * (f16 ? 2 : 4), stream));
+  }
+  if (p->info.tc_tiles + p->info.sptc_tiles + p->info.promoted_tiles > 0) {
+    if (f16) tile_f32_kernel<true><<<v.n_windows, kThreads, 0, stream>>>(v, b, k, c, route_mask);
+    else tile_f32_kernel<false><<<v.n_windows, kThreads, 0, stream>>>(v, b, k, c, route_mask);
+    TRS_CUDA(cudaGetLastError());
+  }
+  return TR_OK;
+}
+
+int launch_sddmm_f32(const int32_t* indptr, const int32_t* indices, int32_t m, int64_t nnz,
+                     const float* x, const float* y, int32_t k, float* out, cudaStream_t stream) {
+  if (m == 0 || nnz == 0) return TR_OK;
+  if (k == 0) {
+    TRS_CUDA(cudaMemsetAsync(out, 0, (size_t)nnz * 4, stream));
+    return TR_OK;
+  }
+  const bool vec = k % 4 == 0 && aligned16(x) && aligned16(y);
+  const int blocks = (int)std::min<int64_t>(((int64_t)m + 7) / 8, 148 * 16);
+  if (vec && k == 64) {
+    sddmm_group_kernel<16, 1, float><<<blocks, 256, 0, stream>>>(indptr, indices, m, x, y, out);
+  } else if (vec && k == 128) {
+    sddmm_group_kernel<32, 1, float><<<blocks, 256, 0, stream>>>(indptr, indices, m, x, y, out);
+  } else if (vec && k == 256) {
+    sddmm_group_kernel<32, 2, float><<<blocks, 256, 0, stream>>>(indptr, indices, m, x, y, out);
+  } else if (vec) {
+    sddmm_kernel<float><<<blocks, 256, 0, stream>>>(indptr, indices, m, x, y, k, out);
+  } else {
+    const int blocks = (int)std::min<int64_t>(m, 148 * 32);
+    sddmm_generic_kernel<float><<<blocks, 128, 0, stream>>>(indptr, indices, m, x, y, k, out);
+  }
   TRS_CUDA(cudaGetLastError());
   return TR_OK;
 }

@@ -11,10 +11,13 @@ two routed plans built once: A for the forward, A^T for the adjoint).
              (tr_adjoint_sddmm: each gathered row of dC feeds both products)
 
 The reference has no backward at all; this is the differentiation path a GNN
-built on the reference's operator would need.  Operands are FP16 on the
-tensor cores with FP32 accumulation; FP32 inputs and gradients are scaled by
-their largest magnitude before the FP16 cast (and the results scaled back),
-so their FP16 copies use the full exponent range.  When the values ``w`` are
+built on the reference's operator would need.  With features="f16" (the
+default) operands are FP16 on the tensor cores with FP32 accumulation; FP32
+inputs and gradients are scaled by their largest magnitude before the FP16
+cast (and the results scaled back), so their FP16 copies use the full
+exponent range.  With features="f32" B, dC and dB stay FP32 end to end on
+the FP32-feature route (tr_spmm_routed_f32 forward and adjoint,
+tr_sddmm_csr_f32 for the values' gradient).  When the values ``w`` are
 learnable, both plans are re-valued on the device (tr_plan_set_values)
 whenever a forward or backward runs, so the pattern is routed only once.
 """
@@ -30,10 +33,15 @@ class RoutedAdjacency:
     """Sparse A (n_rows x n_cols, CSR) with its forward and adjoint plans."""
 
     def __init__(self, indptr, indices, values, n_rows, n_cols, device="cuda",
-                 row_scale=True, promote_min=2, reorder=False, plan_cache=None, **route_kw):
+                 row_scale=True, promote_min=2, reorder=False, plan_cache=None,
+                 features="f16", **route_kw):
         """plan_cache: None builds both plans; True or a directory takes them
         from the on-disk plan cache (trspmm.plan_cache), routing once per
-        graph."""
+        graph.  features: "f16" (FP16 operands) or "f32" (FP32 features on
+        the FP32-feature route)."""
+        if features not in ("f16", "f32"):
+            raise ValueError(f"features must be 'f16' or 'f32', not {features!r}")
+        self.features = features
         indptr = np.ascontiguousarray(indptr, dtype=np.int32)
         indices = np.ascontiguousarray(indices, dtype=np.int32)
         values = np.ascontiguousarray(values, dtype=np.float32)
@@ -76,21 +84,36 @@ class RoutedSpMMFunction(torch.autograd.Function):
     def forward(ctx, w, b, adj):
         if w is not None:
             adj.set_values(w)
+        ctx.adj = adj
+        ctx.has_w = w is not None
+        ctx.b_dtype = b.dtype
+        if adj.features == "f32":
+            b32 = b.detach().to(torch.float32).contiguous()
+            ctx.save_for_backward(w if w is not None else torch.empty(0, device=b.device), b32)
+            return adj.fwd.spmm(b32, out_dtype=torch.float32)
         b16, sb = _to_half_scaled(b)
         out = adj.fwd.spmm(b16, out_dtype=torch.float32)
         if sb is not None:
             out = out * sb
-        ctx.adj = adj
-        ctx.has_w = w is not None
-        ctx.b_dtype = b.dtype
         ctx.save_for_backward(w if w is not None else torch.empty(0, device=b.device), b16,
                               sb if sb is not None else torch.empty(0, device=b.device))
         return out
 
     @staticmethod
     def backward(ctx, dc):
-        w, b16, sb = ctx.saved_tensors
         adj = ctx.adj
+        if adj.features == "f32":
+            w, b32 = ctx.saved_tensors
+            if ctx.has_w:
+                adj.set_values(w)
+            dc32 = dc.detach().to(torch.float32).contiguous()
+            db = dw = None
+            if ctx.needs_input_grad[1]:
+                db = adj.adj.spmm(dc32, out_dtype=torch.float32).to(ctx.b_dtype)
+            if ctx.has_w and ctx.needs_input_grad[0]:
+                dw = sddmm_csr(adj.indptr, adj.indices, dc32, b32)
+            return dw, db, None
+        w, b16, sb = ctx.saved_tensors
         if ctx.has_w:
             adj.set_values(w)
         dc16, sc = _to_half_scaled(dc.contiguous())

@@ -267,17 +267,19 @@ class Plan:
                                        int(values.numel()), ctypes.c_void_p(s)))
 
     def spmm(self, b, out=None, out_dtype=None, route_mask=TR_ROUTE_ALL, stream=None):
-        """C = A_plan . B for a CUDA FP16 tensor B [n_cols, K]."""
+        """C = A_plan . B for a CUDA tensor B [n_cols, K]: FP16 B on the routed
+        kernels (tensor-core tiles + CUDA-core residual), FP32 B on the
+        FP32-feature route (tr_spmm_routed_f32, CUDA cores in FP32)."""
         import torch
-        _check_b(b, self.n_cols)
+        _check_b(b, self.n_cols, fp32_ok=True)
         k = b.shape[1]
         if out is None:
             out = torch.empty((self.n_rows, k), dtype=out_dtype or torch.float32, device=b.device)
         _check_out(out, self.n_rows, k)
         s = stream if stream is not None else torch.cuda.current_stream(b.device).cuda_stream
-        check(lib().tr_spmm_routed(self._h, ctypes.c_void_p(b.data_ptr()), int(k),
-                                   ctypes.c_void_p(out.data_ptr()), _odt(out), int(route_mask),
-                                   ctypes.c_void_p(s)))
+        fn = lib().tr_spmm_routed_f32 if b.dtype == torch.float32 else lib().tr_spmm_routed
+        check(fn(self._h, ctypes.c_void_p(b.data_ptr()), int(k), ctypes.c_void_p(out.data_ptr()),
+                 _odt(out), int(route_mask), ctypes.c_void_p(s)))
         return out
 
     def adjoint_sddmm(self, a_indptr, a_indices, dc, b, db=None, dval=None, db_dtype=None,
@@ -329,10 +331,12 @@ def _odt(out):
     raise TypeError("output must be float32 or float16")
 
 
-def _check_b(b, n_cols):
+def _check_b(b, n_cols, fp32_ok=False):
     import torch
-    if not (b.is_cuda and b.dtype == torch.float16 and b.dim() == 2 and b.is_contiguous()):
-        raise RuntimeError("B must be a contiguous 2-D float16 CUDA tensor")
+    kinds = (torch.float16, torch.float32) if fp32_ok else (torch.float16,)
+    if not (b.is_cuda and b.dtype in kinds and b.dim() == 2 and b.is_contiguous()):
+        raise RuntimeError("B must be a contiguous 2-D " +
+                           ("float16 or float32" if fp32_ok else "float16") + " CUDA tensor")
     if b.shape[0] != n_cols:
         raise RuntimeError(f"B has {b.shape[0]} rows, the matrix has {n_cols} columns")
 
@@ -408,13 +412,17 @@ def host_plan_arrays(h):
 
 
 def sddmm_csr(indptr, indices, x, y, out=None, stream=None):
-    """out[e] = <x[row(e)], y[indices[e]]> (FP16 x [m, K], y [n, K], FP32 out)
-    for every entry of the CSR pattern (int32 CUDA indptr/indices)."""
+    """out[e] = <x[row(e)], y[indices[e]]> (x [m, K], y [n, K], both FP16 or
+    both FP32; FP32 out) for every entry of the CSR pattern (int32 CUDA
+    indptr/indices)."""
     import torch
     m = indptr.numel() - 1
     for t in (x, y):
-        if not (t.is_cuda and t.dtype == torch.float16 and t.dim() == 2 and t.is_contiguous()):
-            raise RuntimeError("x and y must be contiguous 2-D float16 CUDA tensors")
+        if not (t.is_cuda and t.dtype in (torch.float16, torch.float32) and t.dim() == 2
+                and t.is_contiguous()):
+            raise RuntimeError("x and y must be contiguous 2-D float16 or float32 CUDA tensors")
+    if x.dtype != y.dtype:
+        raise RuntimeError("x and y must have the same dtype")
     if x.shape[0] != m or x.shape[1] != y.shape[1]:
         raise RuntimeError("x must be [rows, K] and y [cols, K] with the same K")
     for t in (indptr, indices):
@@ -426,10 +434,11 @@ def sddmm_csr(indptr, indices, x, y, out=None, stream=None):
     if not (out.is_cuda and out.dtype == torch.float32 and out.numel() == nnz and out.is_contiguous()):
         raise RuntimeError("out must be a contiguous float32 CUDA tensor with one item per entry")
     s = stream if stream is not None else torch.cuda.current_stream(x.device).cuda_stream
-    check(lib().tr_sddmm_csr(ctypes.c_void_p(indptr.data_ptr()), ctypes.c_void_p(indices.data_ptr()),
-                             int(m), int(y.shape[0]), int(nnz), ctypes.c_void_p(x.data_ptr()),
-                             ctypes.c_void_p(y.data_ptr()), int(x.shape[1]),
-                             ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(s)))
+    fn = lib().tr_sddmm_csr_f32 if x.dtype == torch.float32 else lib().tr_sddmm_csr
+    check(fn(ctypes.c_void_p(indptr.data_ptr()), ctypes.c_void_p(indices.data_ptr()),
+             int(m), int(y.shape[0]), int(nnz), ctypes.c_void_p(x.data_ptr()),
+             ctypes.c_void_p(y.data_ptr()), int(x.shape[1]),
+             ctypes.c_void_p(out.data_ptr()), ctypes.c_void_p(s)))
     return out
 
 
