@@ -292,6 +292,9 @@ typedef struct tr_tca_stats {
   int32_t bands, rows_per_band;   /* LSH banding used */
   int64_t pairs1, clusters1;      /* candidate row pairs, row clusters */
   int64_t pairs2, clusters2;      /* candidate cluster pairs, final groups */
+  double seconds[4];              /* wall time of: column sets + signatures,
+                                     candidate pairs, Jaccard similarities,
+                                     clustering (both levels together) */
 } tr_tca_stats;
 int tr_tca_order(const int32_t* indptr, const int32_t* indices, int32_t n_rows,
                  const tr_tca_params* params, int32_t* order, tr_tca_stats* stats);

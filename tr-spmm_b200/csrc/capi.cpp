@@ -302,6 +302,7 @@ int tr_tca_order(const int32_t* indptr, const int32_t* indices, int32_t n_rows,
     stats->clusters1 = st.clusters1;
     stats->pairs2 = st.pairs2;
     stats->clusters2 = st.clusters2;
+    for (int i = 0; i < 4; ++i) stats->seconds[i] = st.seconds[i];
   }
   return TR_OK;
 }

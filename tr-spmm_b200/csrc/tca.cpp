@@ -22,6 +22,7 @@
 // Rows without columns are never candidates (in the reference they only meet
 // each other, and are skipped when queried).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -107,23 +108,36 @@ int32_t intersect_count(const int32_t* x, int64_t nx, const int32_t* y, int64_t 
     for (int64_t i = 0; i < nx; ++i) c += std::binary_search(y, y + ny, x[i]) ? 1 : 0;
     return c;
   }
-  for (int64_t i = 0, j = 0; i < nx && j < ny;) {
-    if (x[i] < y[j]) ++i;
-    else if (y[j] < x[i]) ++j;
-    else { ++c; ++i; ++j; }
+  for (int64_t i = 0, j = 0; i < nx && j < ny;) {     // branch-free merge
+    const int32_t a = x[i], b = y[j];
+    c += a == b;
+    i += a <= b;
+    j += b <= a;
   }
   return c;
 }
 
+// |set(pa[k]) & set(pb[k])| for pairs sorted by pa: per run of equal pa the
+// thread stamps pa's columns into its own column-indexed array, then counts
+// each partner's columns that carry the stamp (|pb| direct lookups, no merge).
 void intersections_host(const std::vector<int64_t>& ptr, const std::vector<int32_t>& col,
                         const std::vector<int32_t>& pa, const std::vector<int32_t>& pb,
                         std::vector<int32_t>& inter) {
   inter.resize(pa.size());
+  int32_t n_cols = 0;
+  for (int32_t c : col) n_cols = std::max(n_cols, c + 1);
   parallel_for((int64_t)pa.size(), 4096, [&](int64_t lo, int64_t hi) {
+    std::vector<int32_t> stamp(n_cols, -1);
+    int32_t cur = -1;
     for (int64_t k = lo; k < hi; ++k) {
       const int32_t i = pa[k], j = pb[k];
-      inter[k] = intersect_count(col.data() + ptr[i], ptr[i + 1] - ptr[i], col.data() + ptr[j],
-                                 ptr[j + 1] - ptr[j]);
+      if (i != cur) {
+        for (int64_t e = ptr[i]; e < ptr[i + 1]; ++e) stamp[col[e]] = i;
+        cur = i;
+      }
+      int32_t c = 0;
+      for (int64_t e = ptr[j]; e < ptr[j + 1]; ++e) c += stamp[col[e]] == i;
+      inter[k] = c;
     }
   });
 }
@@ -198,13 +212,51 @@ int candidate_pairs(const std::vector<uint64_t>& dig, int bands, const std::vect
 // Capped union-find clustering of m items over the queued pairs (sorted
 // unique keys i * m + j with their similarities); `rejac(r1, r2)` is the
 // similarity a re-queued pair of roots gets.  Returns each item's root.
+// Pop order of the queued pairs: similarity descending, then queue order
+// (the key index).  Records are sorted in parallel chunks and merged.
+struct PopRec {
+  double s;
+  int64_t i;         // index of the pair among the sorted keys
+  int32_t p1, p2;    // the pair (p1 < p2)
+};
+inline bool pop_before(const PopRec& x, const PopRec& y) { return x.s != y.s ? x.s > y.s : x.i < y.i; }
+
+std::vector<PopRec> pop_order(const std::vector<uint64_t>& keys, const std::vector<double>& simi,
+                              int64_t m) {
+  const int64_t P = (int64_t)simi.size();
+  std::vector<PopRec> rec(P);
+  parallel_for(P, 65536, [&](int64_t lo, int64_t hi) {
+    for (int64_t x = lo; x < hi; ++x)
+      rec[x] = {simi[x], x, (int32_t)(keys[x] / m), (int32_t)(keys[x] % m)};
+  });
+  int t = (int)std::max(1u, std::thread::hardware_concurrency());
+  t = (int)std::min<int64_t>(t, std::max<int64_t>(1, P / 65536));
+  std::vector<int64_t> cut(t + 1);
+  for (int k = 0; k <= t; ++k) cut[k] = P * k / t;
+  parallel_for(t, 1, [&](int64_t lo, int64_t hi) {
+    for (int64_t k = lo; k < hi; ++k) std::sort(rec.begin() + cut[k], rec.begin() + cut[k + 1], pop_before);
+  });
+  for (int w = 1; w < t; w *= 2) {                   // pairwise merges of sorted runs
+    std::vector<std::pair<int64_t, int64_t>> jobs;
+    for (int k = 0; k + w < t; k += 2 * w) jobs.push_back({k, std::min(k + 2 * w, t)});
+    parallel_for((int64_t)jobs.size(), 1, [&](int64_t lo, int64_t hi) {
+      for (int64_t q = lo; q < hi; ++q)
+        std::inplace_merge(rec.begin() + cut[jobs[q].first], rec.begin() + cut[jobs[q].first + w],
+                           rec.begin() + cut[jobs[q].second], pop_before);
+    });
+  }
+  return rec;
+}
+
 template <class Rejac>
 std::vector<int32_t> cluster(int64_t m, const std::vector<uint64_t>& keys,
                              const std::vector<double>& simi, int32_t cap, Rejac rejac) {
   const int64_t P = (int64_t)keys.size();
-  std::vector<int64_t> ord(P);
-  std::iota(ord.begin(), ord.end(), 0);
-  std::stable_sort(ord.begin(), ord.end(), [&](int64_t x, int64_t y) { return simi[x] > simi[y]; });
+  const std::vector<PopRec> ord = pop_order(keys, simi, m);
+  // where each item's pairs (i, .) start among the sorted keys
+  std::vector<int64_t> kstart(m + 1, 0);
+  for (int64_t x = 0; x < P; ++x) kstart[keys[x] / m + 1]++;
+  for (int64_t i = 0; i < m; ++i) kstart[i + 1] += kstart[i];
   std::vector<uint8_t> popped(P, 0);
   struct Re {
     double s;
@@ -230,17 +282,19 @@ std::vector<int32_t> cluster(int64_t m, const std::vector<uint64_t>& keys,
     return a < b ? (uint64_t)a * m + b : (uint64_t)b * m + a;
   };
   auto queued = [&](uint64_t k) {
-    const auto it = std::lower_bound(keys.begin(), keys.end(), k);
-    if (it != keys.end() && *it == k && !popped[it - keys.begin()]) return true;
+    const int64_t i = (int64_t)(k / m);
+    const auto b = keys.begin() + kstart[i], e = keys.begin() + kstart[i + 1];
+    const auto it = std::lower_bound(b, e, k);
+    if (it != e && *it == k && !popped[it - keys.begin()]) return true;
     return queued_re.count(k) > 0;
   };
   while (ncl > 0 && (pos < P || !heap.empty())) {
     int32_t p1, p2;
-    if (pos < P && (heap.empty() || simi[ord[pos]] >= heap.top().s)) {
-      const int64_t x = ord[pos++];
-      popped[x] = 1;
-      p1 = (int32_t)(keys[x] / m);
-      p2 = (int32_t)(keys[x] % m);
+    if (pos < P && (heap.empty() || ord[pos].s >= heap.top().s)) {
+      const PopRec& q = ord[pos++];
+      popped[q.i] = 1;
+      p1 = q.p1;
+      p2 = q.p2;
     } else {
       const Re t = heap.top();
       heap.pop();
@@ -279,10 +333,12 @@ int pair_similarities(const std::vector<int64_t>& ptr, const std::vector<int32_t
                       std::string& err) {
   const int64_t m = (int64_t)ptr.size() - 1;
   std::vector<int32_t> pa(keys.size()), pb(keys.size()), inter;
-  for (size_t k = 0; k < keys.size(); ++k) {
-    pa[k] = (int32_t)(keys[k] / m);
-    pb[k] = (int32_t)(keys[k] % m);
-  }
+  parallel_for((int64_t)keys.size(), 65536, [&](int64_t lo, int64_t hi) {
+    for (int64_t k = lo; k < hi; ++k) {
+      pa[k] = (int32_t)(keys[k] / m);
+      pb[k] = (int32_t)(keys[k] % m);
+    }
+  });
   if (device) {
     const int rc = tca_intersections_gpu(ptr, col, pa, pb, inter, err);
     if (rc) return rc;
@@ -290,8 +346,10 @@ int pair_similarities(const std::vector<int64_t>& ptr, const std::vector<int32_t
     intersections_host(ptr, col, pa, pb, inter);
   }
   simi.resize(keys.size());
-  for (size_t k = 0; k < keys.size(); ++k)
-    simi[k] = jaccard(ptr[pa[k] + 1] - ptr[pa[k]], ptr[pb[k] + 1] - ptr[pb[k]], inter[k]);
+  parallel_for((int64_t)keys.size(), 65536, [&](int64_t lo, int64_t hi) {
+    for (int64_t k = lo; k < hi; ++k)
+      simi[k] = jaccard(ptr[pa[k] + 1] - ptr[pa[k]], ptr[pb[k] + 1] - ptr[pb[k]], inter[k]);
+  });
   return TR_OK;
 }
 
@@ -349,6 +407,12 @@ int tca_order(const int32_t* indptr, const int32_t* indices, int32_t n_rows, con
   tca_lsh_params(p.lsh_threshold, kTcaPerm, bands, rows);
   st.bands = bands;
   st.rows_per_band = rows;
+  auto t_last = std::chrono::steady_clock::now();
+  auto lap = [&](int stage) {          // adds the time since the last lap to a stage
+    const auto now = std::chrono::steady_clock::now();
+    st.seconds[stage] += std::chrono::duration<double>(now - t_last).count();
+    t_last = now;
+  };
 
   // ---- level 1: rows ----------------------------------------------------------
   std::vector<int64_t> ptr;
@@ -359,13 +423,16 @@ int tca_order(const int32_t* indptr, const int32_t* indices, int32_t n_rows, con
   int rc = p.device ? tca_signatures_gpu(ptr, col, p.seed, bands, rows, sig, dig, err)
                     : (signatures_host(ptr, col, p.seed, bands, rows, sig, dig), TR_OK);
   if (rc) return rc;
+  lap(0);
   std::vector<uint64_t> keys;
   rc = candidate_pairs(dig, bands, ptr, p.max_pairs, keys, err);
   if (rc) return rc;
   std::vector<uint64_t>().swap(dig);
+  lap(1);
   std::vector<double> simi;
   rc = pair_similarities(ptr, col, keys, p.device, simi, err);
   if (rc) return rc;
+  lap(2);
   st.pairs1 = (int64_t)keys.size();
   const int64_t n = n_rows;
   std::vector<int32_t> root1 = cluster(n, keys, simi, p.thres, [&](int32_t a, int32_t b) {
@@ -374,6 +441,7 @@ int tca_order(const int32_t* indptr, const int32_t* indices, int32_t n_rows, con
   });
   std::vector<uint64_t>().swap(keys);
   std::vector<double>().swap(simi);
+  lap(3);
 
   // level-1 clusters in order of first appearance, members ascending
   std::vector<int32_t> cl_of_root(n, -1), cl_start, cl_rows;
@@ -424,10 +492,13 @@ int tca_order(const int32_t* indptr, const int32_t* indices, int32_t n_rows, con
     std::copy(cols_of[c].begin(), cols_of[c].end(), ccol.begin() + cptr[c]);
     std::vector<int32_t>().swap(cols_of[c]);
   }
+  lap(0);
   rc = candidate_pairs(cdig, bands, cptr, p.max_pairs, keys, err);
   if (rc) return rc;
+  lap(1);
   rc = pair_similarities(cptr, ccol, keys, p.device, simi, err);
   if (rc) return rc;
+  lap(2);
   st.pairs2 = (int64_t)keys.size();
   std::vector<int32_t> root2 = cluster(nc, keys, simi, p.cluster_thres, [&](int32_t a, int32_t b) {
     const int64_t la = cptr[a + 1] - cptr[a], lb = cptr[b + 1] - cptr[b];
@@ -450,6 +521,7 @@ int tca_order(const int32_t* indptr, const int32_t* indices, int32_t n_rows, con
   for (const auto& g : members)
     for (int32_t c : g)
       for (int32_t k = cl_start[c]; k < cl_start[c + 1]; ++k) order.push_back(cl_rows[k]);
+  lap(3);
   return TR_OK;
 }
 

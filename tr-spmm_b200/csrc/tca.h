@@ -64,6 +64,7 @@ struct TcaParams {
 struct TcaStats {
   int32_t bands = 0, rows_per_band = 0;
   int64_t pairs1 = 0, clusters1 = 0, pairs2 = 0, clusters2 = 0;
+  double seconds[4] = {0, 0, 0, 0};   // sets + signatures, candidates, Jaccard, clustering
 };
 
 // LSH banding (b bands of r rows, b * r <= num_perm) minimising the equally

@@ -93,7 +93,8 @@ class TcaStats(ctypes.Structure):
     """tr_tca_stats (include/trspmm.h)."""
     _fields_ = [("bands", ctypes.c_int32), ("rows_per_band", ctypes.c_int32),
                 ("pairs1", ctypes.c_int64), ("clusters1", ctypes.c_int64),
-                ("pairs2", ctypes.c_int64), ("clusters2", ctypes.c_int64)]
+                ("pairs2", ctypes.c_int64), ("clusters2", ctypes.c_int64),
+                ("seconds", ctypes.c_double * 4)]
 
 
 _TABLE_FIELDS = ["t_row_offset", "t_block_offset", "t_column", "t_value", "t_window_row",

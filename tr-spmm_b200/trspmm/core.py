@@ -457,7 +457,27 @@ def tca_order(indptr, indices, n_rows=None, thres=16, cluster_thres=128, lsh_thr
     order = np.empty(max(n, 0), dtype=np.int32)
     st = TcaStats()
     check(lib().tr_tca_order(_vp(rp), _vp(ci), n, ctypes.byref(prm), _vp(order), ctypes.byref(st)))
-    return order, {name: getattr(st, name) for name, _ in TcaStats._fields_}
+    out = {name: getattr(st, name) for name, _ in TcaStats._fields_ if name != "seconds"}
+    return order, out
+
+
+def tca_order_timed(indptr, indices, n_rows=None, **kw):
+    """tca_order plus the wall time of its stages: (order, stats, seconds)
+    with seconds = {"signatures", "candidates", "jaccard", "cluster"}."""
+    rp = np.ascontiguousarray(indptr, dtype=np.int32)
+    ci = np.ascontiguousarray(indices, dtype=np.int32)
+    n = int(rp.shape[0] - 1) if n_rows is None else int(n_rows)
+    d = dict(thres=16, cluster_thres=128, lsh_threshold=0.2, seed=1, max_pairs=1 << 25,
+             device=False)
+    d.update(kw)
+    prm = TcaParams(int(d["thres"]), int(d["cluster_thres"]), float(d["lsh_threshold"]),
+                    int(d["seed"]), int(d["max_pairs"]), int(bool(d["device"])))
+    order = np.empty(max(n, 0), dtype=np.int32)
+    st = TcaStats()
+    check(lib().tr_tca_order(_vp(rp), _vp(ci), n, ctypes.byref(prm), _vp(order), ctypes.byref(st)))
+    stats = {name: getattr(st, name) for name, _ in TcaStats._fields_ if name != "seconds"}
+    secs = dict(zip(("signatures", "candidates", "jaccard", "cluster"), list(st.seconds)))
+    return order, stats, secs
 
 
 def lsh_params(threshold=0.2, num_perm=128):
