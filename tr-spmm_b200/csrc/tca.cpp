@@ -195,13 +195,23 @@ int candidate_pairs(const std::vector<uint64_t>& dig, int bands, const std::vect
       err = e;
       return TR_ERR_UNSUPPORTED;
     }
-  keys.clear();
-  for (auto& v : acc) {
-    std::vector<uint64_t> merged;
-    std::set_union(keys.begin(), keys.end(), v.begin(), v.end(), std::back_inserter(merged));
-    keys.swap(merged);
-    std::vector<uint64_t>().swap(v);
+  // union of the threads' sorted sets, merged pairwise in parallel
+  for (int w = 1; w < t; w *= 2) {
+    std::vector<int> left;
+    for (int k = 0; k + w < t; k += 2 * w) left.push_back(k);
+    parallel_for((int64_t)left.size(), 1, [&](int64_t lo, int64_t hi) {
+      for (int64_t q = lo; q < hi; ++q) {
+        std::vector<uint64_t>& a = acc[left[q]];
+        std::vector<uint64_t>& b = acc[left[q] + w];
+        std::vector<uint64_t> merged;
+        merged.reserve(a.size() + b.size());
+        std::set_union(a.begin(), a.end(), b.begin(), b.end(), std::back_inserter(merged));
+        a.swap(merged);
+        std::vector<uint64_t>().swap(b);
+      }
+    });
   }
+  keys.swap(acc[0]);
   if ((int64_t)keys.size() > max_pairs) {
     err = "TCA: more than max_pairs LSH candidate pairs";
     return TR_ERR_UNSUPPORTED;
@@ -257,7 +267,12 @@ std::vector<int32_t> cluster(int64_t m, const std::vector<uint64_t>& keys,
   std::vector<int64_t> kstart(m + 1, 0);
   for (int64_t x = 0; x < P; ++x) kstart[keys[x] / m + 1]++;
   for (int64_t i = 0; i < m; ++i) kstart[i + 1] += kstart[i];
-  std::vector<uint8_t> popped(P, 0);
+  // rank[x] = position of key x in the pop order: an initial pair is still
+  // queued while the pop position has not passed its rank
+  std::vector<int64_t> rank(P);
+  parallel_for(P, 65536, [&](int64_t lo, int64_t hi) {
+    for (int64_t q = lo; q < hi; ++q) rank[ord[q].i] = q;
+  });
   struct Re {
     double s;
     uint64_t seq;
@@ -285,14 +300,13 @@ std::vector<int32_t> cluster(int64_t m, const std::vector<uint64_t>& keys,
     const int64_t i = (int64_t)(k / m);
     const auto b = keys.begin() + kstart[i], e = keys.begin() + kstart[i + 1];
     const auto it = std::lower_bound(b, e, k);
-    if (it != e && *it == k && !popped[it - keys.begin()]) return true;
+    if (it != e && *it == k && rank[it - keys.begin()] >= pos) return true;
     return queued_re.count(k) > 0;
   };
   while (ncl > 0 && (pos < P || !heap.empty())) {
     int32_t p1, p2;
     if (pos < P && (heap.empty() || ord[pos].s >= heap.top().s)) {
       const PopRec& q = ord[pos++];
-      popped[q.i] = 1;
       p1 = q.p1;
       p2 = q.p2;
     } else {
