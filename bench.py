@@ -438,11 +438,19 @@ def main():
     plain_ms = float(np.mean(timed(plain_step, n_side, 3)))
     plain_fwd_ms = float(np.mean(timed(lambda: trspmm.spmm_csr(ip, ix, iv, bd, g.n_rows, out=c2),
                                        n_side, 3)))
+    # the same forward with the features in FP32 (FP32-feature route, same plan)
+    b32 = bd.float()
+    c3 = torch.empty_like(cd)
+    f32_ms = float(np.mean(timed(lambda: pf.spmm(b32, out=c3), n_side, 3)))
     routed_step()
     plain_step()
+    pf.spmm(b32, out=c3)
     torch.cuda.synchronize()
     rel = lambda a_, b_: float((a_ - b_).abs().max().item() / max(b_.abs().max().item(), 1e-30))
     err = {"C": rel(cd, c2), "dB": rel(dbd, db2), "dval": rel(dvd, dv2)}
+    fp32_route = {"ms": f32_ms, "tflops": 2.0 * g.nnz * k / (f32_ms * 1e-3) / 1e12,
+                  "max_rel_diff_vs_fp16_features": rel(c3, cd)}
+    del b32, c3
 
     # ---- end to end through the public API with host buffers -------------------
     # Every step uploads its B and dC from pinned host memory and downloads C,
@@ -600,6 +608,7 @@ def main():
                           "algorithmic_bytes": res_bytes,
                           "traffic": _profile_traffic("seg_residual_pass_large_routed.txt")},
                       "plain_csr_step_ms": plain_ms, "plain_csr_forward_ms": plain_fwd_ms,
+                      "fp32_features_forward": fp32_route,
                       "routed_vs_plain_step": plain_ms / ms,
                       "routed_vs_plain_forward": plain_fwd_ms / fwd_ms,
                       "max_rel_diff_vs_plain": err,
