@@ -265,8 +265,10 @@ __global__ void __launch_bounds__(kThreads, 4) seg_block_kernel(
     const __half* __restrict__ values, int M, const TB* __restrict__ B, int K, void* C,
     const int32_t* __restrict__ row_out, const float* __restrict__ row_scale,
     const int32_t* __restrict__ order) {
-  constexpr int U = kSegU;
   constexpr int NPL = SegFeat<TB>::kPer, PASS = 32 * NPL;   // features per lane / per pass
+  // entries per lane group and batch: FP32 features hold half the
+  // accumulators, which leaves room for twice the gathers in flight
+  constexpr int U = NPL == 4 ? 2 * kSegU : kSegU;
   __shared__ __align__(16) float racc[kBlockRows * kSegStrideW];
   __shared__ __align__(16) int2 sent[kStage + 2];
   __shared__ int rp[kBlockRows + 1];
