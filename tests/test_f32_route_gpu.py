@@ -11,7 +11,6 @@ significand), dw within 1e-5 (FP32 SDDMM, no rounded operand).
 """
 import numpy as np
 import pytest
-import scipy.sparse as sp
 import torch
 
 import oracle

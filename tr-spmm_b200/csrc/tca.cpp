@@ -24,7 +24,6 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
-#include <cstring>
 #include <map>
 #include <mutex>
 #include <numeric>

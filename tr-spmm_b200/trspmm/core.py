@@ -447,6 +447,16 @@ def tca_order(indptr, indices, n_rows=None, thres=16, cluster_thres=128, lsh_thr
     """TCA row order of a host CSR (tr_tca_order): (order int32 [n_rows],
     new position -> old row; stats dict).  ``device=True`` computes the
     MinHash signatures and the Jaccard similarities on the current GPU."""
+    order, stats, _ = tca_order_timed(indptr, indices, n_rows, thres=thres,
+                                      cluster_thres=cluster_thres, lsh_threshold=lsh_threshold,
+                                      seed=seed, max_pairs=max_pairs, device=device)
+    return order, stats
+
+
+def tca_order_timed(indptr, indices, n_rows=None, thres=16, cluster_thres=128,
+                    lsh_threshold=0.2, seed=1, max_pairs=1 << 25, device=False):
+    """tca_order plus the wall time of its stages: (order, stats, seconds)
+    with seconds = {"signatures", "candidates", "jaccard", "cluster"}."""
     rp = np.ascontiguousarray(indptr, dtype=np.int32)
     ci = np.ascontiguousarray(indices, dtype=np.int32)
     n = int(rp.shape[0] - 1) if n_rows is None else int(n_rows)
@@ -454,24 +464,6 @@ def tca_order(indptr, indices, n_rows=None, thres=16, cluster_thres=128, lsh_thr
         raise ValueError("indptr shorter than n_rows + 1")
     prm = TcaParams(int(thres), int(cluster_thres), float(lsh_threshold), int(seed),
                     int(max_pairs), int(bool(device)))
-    order = np.empty(max(n, 0), dtype=np.int32)
-    st = TcaStats()
-    check(lib().tr_tca_order(_vp(rp), _vp(ci), n, ctypes.byref(prm), _vp(order), ctypes.byref(st)))
-    out = {name: getattr(st, name) for name, _ in TcaStats._fields_ if name != "seconds"}
-    return order, out
-
-
-def tca_order_timed(indptr, indices, n_rows=None, **kw):
-    """tca_order plus the wall time of its stages: (order, stats, seconds)
-    with seconds = {"signatures", "candidates", "jaccard", "cluster"}."""
-    rp = np.ascontiguousarray(indptr, dtype=np.int32)
-    ci = np.ascontiguousarray(indices, dtype=np.int32)
-    n = int(rp.shape[0] - 1) if n_rows is None else int(n_rows)
-    d = dict(thres=16, cluster_thres=128, lsh_threshold=0.2, seed=1, max_pairs=1 << 25,
-             device=False)
-    d.update(kw)
-    prm = TcaParams(int(d["thres"]), int(d["cluster_thres"]), float(d["lsh_threshold"]),
-                    int(d["seed"]), int(d["max_pairs"]), int(bool(d["device"])))
     order = np.empty(max(n, 0), dtype=np.int32)
     st = TcaStats()
     check(lib().tr_tca_order(_vp(rp), _vp(ci), n, ctypes.byref(prm), _vp(order), ctypes.byref(st)))
