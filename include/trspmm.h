@@ -396,6 +396,12 @@ int tr_sddmm_csr(const int32_t* indptr, const int32_t* indices, int32_t m, int32
  * anything else a scalar kernel. */
 int tr_spmm_routed_f32(const tr_plan* p, const float* b, int32_t k, void* c, int c_dtype,
                        int route_mask, void* stream);
+/* tr_adjoint_sddmm with FP32 dc [a_rows, K] and b [n_cols, K]: one pass over
+ * the adjoint plan for 16 < K <= 128 (K % 4 == 0) when the plan keeps every
+ * entry in its residual; otherwise tr_spmm_routed_f32 then tr_sddmm_csr_f32. */
+int tr_adjoint_sddmm_f32(const tr_plan* adj, const int32_t* a_indptr, const int32_t* a_indices,
+                         int32_t a_rows, int64_t nnz, const float* dc, const float* b, int32_t k,
+                         void* db, int db_dtype, float* dval, void* stream);
 /* tr_sddmm_csr with FP32 x [m, k] and y [n_cols, k]. */
 int tr_sddmm_csr_f32(const int32_t* indptr, const int32_t* indices, int32_t m, int32_t n_cols,
                      int64_t nnz, const float* x, const float* y, int32_t k, float* out,

@@ -160,3 +160,27 @@ def test_autograd_f32_vs_torch_sparse(dev, name):
     assert rel_err(wt.grad.cpu().numpy(), w64.grad.numpy()) <= TOL_F32
     with pytest.raises(ValueError, match="features"):
         RoutedAdjacency(g.indptr, g.indices, w, g.n_rows, g.n_cols, features="tf32")
+
+
+@pytest.mark.parametrize("name,k,opts", [
+    ("chung_lu", 128, dict(row_scale=True, demote_below=1000)),     # fused, 32-lane groups
+    ("sbm", 64, dict(row_scale=True, demote_below=1000)),           # fused, 16-lane groups
+    ("ragged", 20, dict()),                                          # fused, 8-lane groups, 5 active
+    ("sbm", 256, dict(demote_below=1000)),                           # K > 128: two launches
+    ("route_mix", 64, dict()),                                       # tiles: two launches
+])
+def test_adjoint_sddmm_f32(dev, name, k, opts):
+    g = _graph(name)
+    plan = trspmm.Plan.build(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, transpose=True,
+                             **opts)
+    rng = np.random.default_rng(k)
+    dc = rng.standard_normal((g.n_rows, k)).astype(np.float32)
+    b = rng.standard_normal((g.n_cols, k)).astype(np.float32)
+    ip = torch.from_numpy(g.indptr).to(dev)
+    ix = torch.from_numpy(g.indices).to(dev)
+    db, dval = plan.adjoint_sddmm(ip, ix, torch.from_numpy(dc).to(dev), torch.from_numpy(b).to(dev))
+    torch.cuda.synchronize()
+    AT = _decoded(g, dict(transpose=True, **opts))["all"]
+    assert rel_err(db.cpu().numpy(), AT @ dc.astype(np.float64)) <= TOL_F32
+    ref = oracle.sddmm_f64(g.indptr, g.indices, dc.astype(np.float64), b.astype(np.float64))
+    assert rel_err(dval.cpu().numpy(), ref) <= TOL_F32

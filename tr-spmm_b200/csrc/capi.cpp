@@ -473,6 +473,19 @@ int tr_adjoint_sddmm(const tr_plan* adj, const int32_t* a_indptr, const int32_t*
                               (cudaStream_t)stream);
 }
 
+int tr_adjoint_sddmm_f32(const tr_plan* adj, const int32_t* a_indptr, const int32_t* a_indices,
+                         int32_t a_rows, int64_t nnz, const float* dc, const float* b, int32_t k,
+                         void* db, int db_dtype, float* dval, void* stream) {
+  if (!adj) return fail(TR_ERR_ARG, "null plan");
+  if (a_rows < 0 || nnz < 0 || k < 0) return fail(TR_ERR_ARG, "negative size");
+  if (db_dtype != TR_OUT_F32 && db_dtype != TR_OUT_F16) return fail(TR_ERR_ARG, "bad output dtype");
+  if (a_rows != adj->view.n_cols) return fail(TR_ERR_ARG, "a_rows must equal the adjoint plan's column count");
+  if (k > 0 && (!dc || !b || !db || (nnz > 0 && (!a_indptr || !a_indices || !dval))))
+    return fail(TR_ERR_ARG, "null device pointer");
+  return launch_adjoint_sddmm_f32(adj, a_indptr, a_indices, a_rows, nnz, dc, b, k, db, db_dtype,
+                                  dval, (cudaStream_t)stream);
+}
+
 int tr_sddmm_csr(const int32_t* indptr, const int32_t* indices, int32_t m, int32_t n_cols,
                  int64_t nnz, const uint16_t* x, const uint16_t* y, int32_t k, float* out,
                  void* stream) {

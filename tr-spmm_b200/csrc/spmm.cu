@@ -1009,16 +1009,17 @@ __device__ __forceinline__ float group_reduce_scatter8(float (&d)[8], int li) {
 // dval for the batch's entry u.  K <= 256 in one pass (lane groups of 8,
 // 16 or 32 lanes).  Four CTAs per SM (64 registers, a few bytes of spill)
 // beat three without spill.
-template <bool F16OUT, int L, bool WIDE>
+template <bool F16OUT, int L, bool WIDE, class TB = __half>
 __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
     const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
     const __half* __restrict__ values, const int32_t* __restrict__ edges, int M,
-    const __half* __restrict__ G, int K, void* C, const int32_t* __restrict__ row_out,
-    const float* __restrict__ row_scale, const __half* __restrict__ H, float* __restrict__ dval,
+    const TB* __restrict__ G, int K, void* C, const int32_t* __restrict__ row_out,
+    const float* __restrict__ row_scale, const TB* __restrict__ H, float* __restrict__ dval,
     const int32_t* __restrict__ order) {
   constexpr int U = 8;
+  constexpr int NPL = SegFeat<TB>::kPer;                   // features per lane
   constexpr int Gn = 32 / L, groups = kWarps * Gn;
-  constexpr int S = L == 32 ? kSegStrideW : kSegStride;   // padded shared row (floats)
+  constexpr int S = L * NPL > kChunk ? kSegStrideW : kSegStride;   // padded shared row (floats)
   __shared__ __align__(16) float racc[kBlockRows * S];
   __shared__ __align__(16) int4 sent[kStage + 1];
   __shared__ int rp[kBlockRows + 1];
@@ -1037,14 +1038,14 @@ __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
   const int e_begin = rp[0], e_end = rp[kBlockRows];
   const uint32_t uK = (uint32_t)K;
   const int li = lane % L, q = warp * Gn + lane / L;
-  const bool active = li * 8 < K;
+  const bool active = li * NPL < K;
   if (tid < kBlockRows) s_own[tid] = seg_owned(rp[tid], rp[tid + 1], e_begin, e_end, groups);
   {
     float4* z = reinterpret_cast<float4*>(racc);
     for (int i = tid; i < kBlockRows * S / 4; i += kThreads) z[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
-  const __half* Gf = G + (active ? li * 8 : 0);
-  float* dst = racc + seg_slot_w<S>(0, active ? li * 8 : 0);
+  const TB* Gf = G + (active ? li * NPL : 0);
+  float* dst = racc + seg_slot_w<S>(0, active ? li * NPL : 0);
   const uint16_t* v16 = reinterpret_cast<const uint16_t*>(values);
   for (int c0 = e_begin; c0 < e_end; c0 += kStage) {
     const int n = min(kStage, e_end - c0);
@@ -1061,20 +1062,20 @@ __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
     // row j of B for the dot products of row r's entries
     auto load_h = [&]() {
       const int o = s_out[r];
-      return (active && o >= 0) ? __ldg(reinterpret_cast<const uint4*>(H + (int64_t)o * K + li * 8))
+      return (active && o >= 0) ? __ldg(reinterpret_cast<const uint4*>(H + (int64_t)o * K + li * NPL))
                                 : make_uint4(0u, 0u, 0u, 0u);
     };
     uint4 hv = load_h();
-    float acc[8];
+    float acc[NPL];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) acc[i] = 0.f;
+    for (int i = 0; i < NPL; ++i) acc[i] = 0.f;
     auto flush = [&]() {
       if (!active) return;
       if (rp[r] >= c0 + lo && rp[r + 1] <= c0 + hi) {
-        if (s_out[r] >= 0) store_vec<F16OUT, 8>(C, K, s_out[r], li * 8, acc, s_scale[r]);
+        if (s_out[r] >= 0) store_vec<F16OUT, NPL>(C, K, s_out[r], li * NPL, acc, s_scale[r]);
       } else {
 #pragma unroll
-        for (int i = 0; i < 8; ++i) atomicAdd(dst + r * S + i, acc[i]);
+        for (int i = 0; i < NPL; ++i) atomicAdd(dst + r * S + i, acc[i]);
       }
     };
 #pragma unroll 1
@@ -1100,8 +1101,8 @@ __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
       if (__all_sync(0xffffffffu, t + U <= nb && t + U <= hi)) {   // no boundary, full
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-          fma8h(acc, (uint16_t)(v[u / 2] >> (16 * (u & 1))), b[u]);
-          d[u] = dot8h(hv, b[u]);
+          seg_fma(acc, (uint16_t)(v[u / 2] >> (16 * (u & 1))), b[u]);
+          d[u] = dot_chunk(hv, b[u], TB());
         }
       } else {
 #pragma unroll
@@ -1112,13 +1113,13 @@ __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
             if (j >= nb) {                     // row r ends before entry j
               flush();
 #pragma unroll
-              for (int i = 0; i < 8; ++i) acc[i] = 0.f;
+              for (int i = 0; i < NPL; ++i) acc[i] = 0.f;
               do ++r; while (rp[r + 1] - c0 <= j);
               nb = rp[r + 1] - c0;
               hv = load_h();
             }
-            fma8h(acc, (uint16_t)(v[u / 2] >> (16 * (u & 1))), b[u]);
-            d[u] = dot8h(hv, b[u]);
+            seg_fma(acc, (uint16_t)(v[u / 2] >> (16 * (u & 1))), b[u]);
+            d[u] = dot_chunk(hv, b[u], TB());
           }
         }
         __syncwarp();                          // reconverge the lane groups
@@ -1423,6 +1424,45 @@ int launch_adjoint_sddmm(const tr_plan* p, const int32_t* a_indptr, const int32_
     else { if (f16) TRS_SEGADJ(true, 8, false); else TRS_SEGADJ(false, 8, false); }
   }
 #undef TRS_SEGADJ
+  TRS_CUDA(cudaGetLastError());
+  return TR_OK;
+}
+
+// The same with FP32 dC and B (FP32-feature route): fused for 16 < K <= 128
+// (K % 4 == 0, lane groups of 8, 16 or 32 lanes of 4 features), otherwise the
+// FP32 routed adjoint and the FP32 SDDMM one after the other.
+int launch_adjoint_sddmm_f32(const tr_plan* p, const int32_t* a_indptr, const int32_t* a_indices,
+                             int32_t a_rows, int64_t nnz, const float* dc, const float* b,
+                             int32_t k, void* db, int db_dtype, float* dval, cudaStream_t stream) {
+  const PlanView& v = p->view;
+  const bool f16 = db_dtype == TR_OUT_F16;
+  const bool tiles = p->info.tc_tiles + p->info.sptc_tiles + p->info.promoted_tiles > 0;
+  const bool fused = !tiles && k > 16 && k <= kChunk && k % 4 == 0 && aligned16(dc) &&
+                     aligned16(b) && aligned16(db) && p->n_edges == nnz &&
+                     p->info.residual_nnz == nnz && v.n_rows > 0;
+  if (!fused) {
+    int rc = launch_routed_f32(p, dc, k, db, db_dtype, TR_ROUTE_ALL, stream);
+    if (rc) return rc;
+    return launch_sddmm_f32(a_indptr, a_indices, a_rows, nnz, dc, b, k, dval, stream);
+  }
+  const int rows = v.n_windows * kBlockRows;
+  const __half* rv = reinterpret_cast<const __half*>(v.res_val);
+#define TRS_SEGADJ32(F16, L, W)                                                             \
+  seg_adjoint_sddmm_kernel<F16, L, W, float><<<v.n_windows, kThreads, 0, stream>>>(          \
+      v.res_ptr, v.res_col, rv, v.res_edge, rows, dc, k, db, v.row_out, v.row_scale, b, dval,   \
+      v.win_order)
+  const bool wide = (int64_t)v.n_cols * k >= ((int64_t)1 << 31);
+  if (k > 64) {
+    if (wide) { if (f16) TRS_SEGADJ32(true, 32, true); else TRS_SEGADJ32(false, 32, true); }
+    else { if (f16) TRS_SEGADJ32(true, 32, false); else TRS_SEGADJ32(false, 32, false); }
+  } else if (k > 32) {
+    if (wide) { if (f16) TRS_SEGADJ32(true, 16, true); else TRS_SEGADJ32(false, 16, true); }
+    else { if (f16) TRS_SEGADJ32(true, 16, false); else TRS_SEGADJ32(false, 16, false); }
+  } else {
+    if (wide) { if (f16) TRS_SEGADJ32(true, 8, true); else TRS_SEGADJ32(false, 8, true); }
+    else { if (f16) TRS_SEGADJ32(true, 8, false); else TRS_SEGADJ32(false, 8, false); }
+  }
+#undef TRS_SEGADJ32
   TRS_CUDA(cudaGetLastError());
   return TR_OK;
 }

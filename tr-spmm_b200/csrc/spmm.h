@@ -24,6 +24,9 @@ int launch_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c
                   int route_mask, cudaStream_t stream);
 int launch_routed_f32(const tr_plan* p, const float* b, int32_t k, void* c, int c_dtype,
                       int route_mask, cudaStream_t stream);
+int launch_adjoint_sddmm_f32(const tr_plan* p, const int32_t* a_indptr, const int32_t* a_indices,
+                             int32_t a_rows, int64_t nnz, const float* dc, const float* b,
+                             int32_t k, void* db, int db_dtype, float* dval, cudaStream_t stream);
 int launch_sddmm_f32(const int32_t* indptr, const int32_t* indices, int32_t m, int64_t nnz,
                      const float* x, const float* y, int32_t k, float* out, cudaStream_t stream);
 

@@ -30,6 +30,7 @@ EXPORTED = [
     "tr_forward_fp16_tcu_cuda_sptc_mma_parallel_online", "tr_forward_fp16_sptc_online",
     "tr_forward_fp16_sptc_mma_online", "tr_forward_fp16_sptc_mma_packed_online",
     "tr_tca_order", "tr_lsh_params", "tr_spmm_routed_f32", "tr_sddmm_csr_f32",
+    "tr_adjoint_sddmm_f32",
 ]
 
 
@@ -154,6 +155,7 @@ def lib():
     L.tr_spmm_routed.argtypes = [P, P, I32, P, ctypes.c_int, ctypes.c_int, P]
     L.tr_spmm_routed_f32.argtypes = [P, P, I32, P, ctypes.c_int, ctypes.c_int, P]
     L.tr_sddmm_csr_f32.argtypes = [P, P, I32, I32, I64, P, P, I32, P, P]
+    L.tr_adjoint_sddmm_f32.argtypes = [P, P, P, I32, I64, P, P, I32, P, ctypes.c_int, P, P]
     pairs29 = [P, I64] * 27 + [P, I64]
     L.tr_forward_fp16_tcu_cuda_sptc_mma_parallel_online.argtypes = (
         [P, I64] * 27 + [I32] * 9 + [P, P])

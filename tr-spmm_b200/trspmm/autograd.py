@@ -16,8 +16,8 @@ default) operands are FP16 on the tensor cores with FP32 accumulation; FP32
 inputs and gradients are scaled by their largest magnitude before the FP16
 cast (and the results scaled back), so their FP16 copies use the full
 exponent range.  With features="f32" B, dC and dB stay FP32 end to end on
-the FP32-feature route (tr_spmm_routed_f32 forward and adjoint,
-tr_sddmm_csr_f32 for the values' gradient).  When the values ``w`` are
+the FP32-feature route (tr_spmm_routed_f32 forward; tr_adjoint_sddmm_f32
+for dB and the values' gradient together).  When the values ``w`` are
 learnable, both plans are re-valued on the device (tr_plan_set_values)
 whenever a forward or backward runs, so the pattern is routed only once.
 """
@@ -108,6 +108,10 @@ class RoutedSpMMFunction(torch.autograd.Function):
                 adj.set_values(w)
             dc32 = dc.detach().to(torch.float32).contiguous()
             db = dw = None
+            if ctx.needs_input_grad[1] and ctx.has_w and ctx.needs_input_grad[0]:
+                # both gradients in one pass over A^T (tr_adjoint_sddmm_f32)
+                db, dw = adj.adj.adjoint_sddmm(adj.indptr, adj.indices, dc32, b32)
+                return dw, db.to(ctx.b_dtype), None
             if ctx.needs_input_grad[1]:
                 db = adj.adj.spmm(dc32, out_dtype=torch.float32).to(ctx.b_dtype)
             if ctx.has_w and ctx.needs_input_grad[0]:

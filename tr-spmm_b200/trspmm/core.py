@@ -286,12 +286,13 @@ class Plan:
                       stream=None):
         """For an adjoint plan (built with transpose=True): dB = A^T . dC and
         dval = SDDMM(dC, B) on A's pattern, fused into one pass where the plan
-        allows (tr_adjoint_sddmm).  dc [A rows, K], b [A cols, K] FP16 CUDA."""
+        allows (tr_adjoint_sddmm).  dc [A rows, K], b [A cols, K] CUDA, both
+        FP16 or both FP32 (tr_adjoint_sddmm_f32)."""
         import torch
-        _check_b(dc, self.n_cols)
-        if not (b.is_cuda and b.dtype == torch.float16 and b.is_contiguous() and b.dim() == 2
+        _check_b(dc, self.n_cols, fp32_ok=True)
+        if not (b.is_cuda and b.dtype == dc.dtype and b.is_contiguous() and b.dim() == 2
                 and b.shape == (self.n_rows, dc.shape[1])):
-            raise RuntimeError("b must be a contiguous float16 CUDA tensor [A cols, K]")
+            raise RuntimeError("b must be a contiguous CUDA tensor [A cols, K] of dc's dtype")
         k = dc.shape[1]
         nnz = a_indices.numel()
         if db is None:
@@ -302,12 +303,13 @@ class Plan:
         if not (dval.is_cuda and dval.dtype == torch.float32 and dval.numel() == nnz):
             raise RuntimeError("dval must be a float32 CUDA tensor with one item per entry")
         s = stream if stream is not None else torch.cuda.current_stream(dc.device).cuda_stream
-        check(lib().tr_adjoint_sddmm(self._h, ctypes.c_void_p(a_indptr.data_ptr()),
-                                     ctypes.c_void_p(a_indices.data_ptr()), int(self.n_cols),
-                                     int(nnz), ctypes.c_void_p(dc.data_ptr()),
-                                     ctypes.c_void_p(b.data_ptr()), int(k),
-                                     ctypes.c_void_p(db.data_ptr()), _odt(db),
-                                     ctypes.c_void_p(dval.data_ptr()), ctypes.c_void_p(s)))
+        fn = lib().tr_adjoint_sddmm_f32 if dc.dtype == torch.float32 else lib().tr_adjoint_sddmm
+        check(fn(self._h, ctypes.c_void_p(a_indptr.data_ptr()),
+                 ctypes.c_void_p(a_indices.data_ptr()), int(self.n_cols),
+                 int(nnz), ctypes.c_void_p(dc.data_ptr()),
+                 ctypes.c_void_p(b.data_ptr()), int(k),
+                 ctypes.c_void_p(db.data_ptr()), _odt(db),
+                 ctypes.c_void_p(dval.data_ptr()), ctypes.c_void_p(s)))
         return db, dval
 
     def close(self):
