@@ -279,6 +279,22 @@ def dist_setup():
     return world, rank, local
 
 
+def max_over_ranks(ms, world, device):
+    """The largest of the ranks' per-step times (every rank calls this, in the
+    same order; world 1 returns ms)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_tflops(flops_per_step, world, ms_max):
+    """Whole-job throughput: every rank processes one step's units in ms_max."""
+    return flops_per_step * world / (ms_max * 1e-3) / 1e12
+
+
 def workload(name=WORKLOAD):
     from trspmm import graphs
     g, b = graphs.make_workload(name)
@@ -419,12 +435,9 @@ def main():
     if world > 1:
         dist.barrier()
     ms = float(np.mean(times))
-    ms_t = torch.tensor([ms], device=dev)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    ms_max = max_over_ranks(ms, world, dev)
     flops = 3 * 2.0 * g.nnz * k
-    value = flops * world / (ms_max * 1e-3) / 1e12
+    value = whole_job_tflops(flops, world, ms_max)
 
     # per-pass times and the plain single-route comparison (outside the timed region)
     n_side = min(args.steps, 100)
@@ -518,10 +531,8 @@ def main():
     e_ev.record(stream)
     torch.cuda.synchronize()
     e2e_ms = s_ev.elapsed_time(e_ev) / e2e_steps
-    e2e_t = torch.tensor([e2e_ms], device=dev)
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_val = flops * world / (float(e2e_t.item()) * 1e-3) / 1e12
+    e2e_max = max_over_ranks(e2e_ms, world, dev)
+    e2e_val = whole_job_tflops(flops, world, e2e_max)
     # the same through the public API without the pipelining (one step after
     # another on one stream), for reference
     def serial_step():
@@ -620,7 +631,7 @@ def main():
                                    for r in tune_report.get("results", [])],
                       "batched_512": batched,
                       "plan_forward": pf.info, "plan_adjoint": pa.info,
-                      "e2e_ms_per_step": float(e2e_t.item())},
+                      "e2e_ms_per_step": e2e_max},
         }
         print(json.dumps(line), flush=True)
     if world > 1:
