@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstring>
 #include <numeric>
+#include <thread>
 
 #include "common.cuh"
 #include "router.h"
@@ -34,6 +35,20 @@ namespace trs {
 namespace {
 
 inline int a_index(int n, int k) { return (n / 8) * 128 + (k / 8) * 64 + (n % 8) * 8 + (k % 8); }
+
+// f(begin, end) over [0, n) on the host's threads (windows are independent).
+template <class F>
+void parallel_windows(int64_t n, F f) {
+  int t = (int)std::max(1u, std::thread::hardware_concurrency());
+  t = (int)std::min<int64_t>(t, std::max<int64_t>(1, n / 64));
+  if (t <= 1) {
+    f((int64_t)0, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int k = 0; k < t; ++k) pool.emplace_back([&, k] { f(n * k / t, n * (k + 1) / t); });
+  for (auto& th : pool) th.join();
+}
 
 inline uint16_t f2h(float f) {
   _Float16 h = (_Float16)f;
@@ -88,7 +103,10 @@ inline int elem_row(int i) { return (i / 128) * 8 + (i % 64) / 8; }
 // are dropped.
 void demote(Staging& st, int W, int min_rows) {
   if (min_rows <= 1) return;
-  for (int w = 0; w < W; ++w) {
+  // each window's demoted entries, appended to the residual in window order
+  std::vector<std::vector<ResEntry>> moved(W);
+  parallel_windows(W, [&](int64_t w0, int64_t w1) {
+  for (int w = (int)w0; w < (int)w1; ++w) {
     WinTiles& wt = st.sp[w];
     WinTiles kept;
     for (int t = 0; t < wt.n; ++t) {
@@ -100,10 +118,10 @@ void demote(Staging& st, int W, int min_rows) {
       for (int k = 0; k < 16; ++k) {
         if (wt.col[cb + k] < 0) continue;
         if (cnt[k] >= min_rows) { any = true; continue; }
-        for (int i = 0; i < 256; ++i) {
-          if (((i % 128) / 64) * 8 + (i % 8) != k) continue;
+        for (int n = 0; n < 16; ++n) {              // column k's slots, rows ascending
+          const int i = a_index(n, k);
           if (wt.a[ab + i] == 0.f && wt.edge[ab + i] < 0) continue;
-          st.res.push_back({w * 16 + elem_row(i), wt.col[cb + k], wt.a[ab + i], wt.edge[ab + i]});
+          moved[w].push_back({w * 16 + elem_row(i), wt.col[cb + k], wt.a[ab + i], wt.edge[ab + i]});
           wt.a[ab + i] = 0.f;
           wt.edge[ab + i] = -1;
         }
@@ -116,6 +134,14 @@ void demote(Staging& st, int W, int min_rows) {
       kept.n++;
     }
     wt = std::move(kept);
+  }
+  });
+  size_t total = st.res.size();
+  for (const auto& m : moved) total += m.size();
+  st.res.reserve(total);
+  for (auto& m : moved) {
+    st.res.insert(st.res.end(), m.begin(), m.end());
+    std::vector<ResEntry>().swap(m);
   }
 }
 
@@ -189,17 +215,29 @@ void flatten(HostPlan& hp, Staging& st, const PlanOptions& opt, int64_t n_edges)
   hp.win_tile.assign(1, 0);
   hp.win_split.resize(W);
   hp.win_prom.resize(W);
-  hp.tile_col.clear();
-  hp.tile_a.clear();
   hp.val_slot.assign(n_edges, -1);
   hp.edge_row.assign(n_edges, -1);
-  auto put_tiles = [&](int w, WinTiles& wt) {
+  // window offsets first, then every window's tiles filled in parallel (each
+  // CSR entry lives in one tile slot, so the entry maps are written once)
+  hp.win_tile.resize((size_t)W + 1);
+  hp.win_tile[0] = 0;
+  for (int w = 0; w < W; ++w) {
+    hp.win_split[w] = hp.win_tile[w] + st.tc[w].n;
+    hp.win_prom[w] = hp.win_split[w] + st.sp[w].n;
+    hp.win_tile[w + 1] = hp.win_prom[w] + st.pr[w].n;
+    hp.tc_tiles += st.tc[w].n;
+    hp.sptc_tiles += st.sp[w].n;
+    hp.prom_tiles += st.pr[w].n;
+  }
+  hp.tile_col.resize((size_t)hp.win_tile[W] * 16);
+  hp.tile_a.resize((size_t)hp.win_tile[W] * 256);
+  auto put_tiles = [&](int w, const WinTiles& wt, int64_t first) {
     for (int t = 0; t < wt.n; ++t) {
-      const int64_t tile = (int64_t)hp.tile_col.size() / 16;
-      hp.tile_col.insert(hp.tile_col.end(), wt.col.begin() + t * 16, wt.col.begin() + t * 16 + 16);
+      const int64_t tile = first + t;
+      std::copy(wt.col.begin() + t * 16, wt.col.begin() + t * 16 + 16, hp.tile_col.begin() + tile * 16);
       for (int i = 0; i < 256; ++i) {
         const int64_t r = (int64_t)w * 16 + elem_row(i);
-        hp.tile_a.push_back(f2h(wt.a[(size_t)t * 256 + i] / hp.row_scale[r]));
+        hp.tile_a[(size_t)tile * 256 + i] = f2h(wt.a[(size_t)t * 256 + i] / hp.row_scale[r]);
         const int32_t e = wt.edge[(size_t)t * 256 + i];
         if (e >= 0 && e < n_edges) {
           hp.val_slot[e] = (int32_t)(tile * 256 + i);
@@ -208,17 +246,13 @@ void flatten(HostPlan& hp, Staging& st, const PlanOptions& opt, int64_t n_edges)
       }
     }
   };
-  for (int w = 0; w < W; ++w) {
-    put_tiles(w, st.tc[w]);
-    hp.win_split[w] = hp.win_tile.back() + st.tc[w].n;
-    put_tiles(w, st.sp[w]);
-    hp.win_prom[w] = hp.win_split[w] + st.sp[w].n;
-    put_tiles(w, st.pr[w]);
-    hp.win_tile.push_back(hp.win_prom[w] + st.pr[w].n);
-    hp.tc_tiles += st.tc[w].n;
-    hp.sptc_tiles += st.sp[w].n;
-    hp.prom_tiles += st.pr[w].n;
-  }
+  parallel_windows(W, [&](int64_t w0, int64_t w1) {
+    for (int w = (int)w0; w < (int)w1; ++w) {
+      put_tiles(w, st.tc[w], hp.win_tile[w]);
+      put_tiles(w, st.sp[w], hp.win_split[w]);
+      put_tiles(w, st.pr[w], hp.win_prom[w]);
+    }
+  });
   const int64_t T = (int64_t)hp.tile_col.size() / 16;
   // ---- residual CSR over padded rows, entries of a row in table order -------
   hp.res_ptr.assign(rows + 1, 0);
