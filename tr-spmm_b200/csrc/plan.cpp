@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -403,59 +404,79 @@ int add_groups(const int32_t* s_column, const float* s_value, const int8_t* s_po
                const int32_t* s_edge, int64_t groups, const std::vector<int32_t>& gwin,
                int32_t n_rows, int32_t n_cols, int W, Staging& st, std::string& err,
                bool to_residual = false) {
+  std::atomic<bool> bad_col{false};
   if (to_residual) {
-    for (int64_t g = 0; g < groups; ++g) {
-      const int w = gwin[g];
-      if (!in_range(w, 0, W)) continue;                     // beyond the matrix
-      int32_t c[4];
-      for (int p = 0; p < 4; ++p) {
-        c[p] = s_column[g * 4 + p];
-        if (c[p] < -1 || c[p] >= n_cols) { err = "s_column out of range"; return TR_ERR_ARG; }
-      }
-      for (int lr = 0; lr < 16; ++lr) {
-        if ((int64_t)w * 16 + lr >= n_rows) continue;
-        const int64_t at0 = (g * 16 + lr) * 2;
-        for (int s = 0; s < 2; ++s) {
-          const int64_t at = at0 + s;
-          const int pos = s_pos[at];
-          if (pos < 0 || pos > 3 || c[pos] < 0) continue;
-          if (s == 0 && s_pos[at0 + 1] == pos) continue;    // the later slot wins, as in a tile
-          const float v = s_value[at];
-          const int32_t e = s_edge ? s_edge[at] : -1;
-          if (v != 0.f || e >= 0) st.res.push_back({w * 16 + lr, c[pos], v, e});
+    // contiguous ranges of groups on the host threads, concatenated in range
+    // order: the residual keeps the groups' order
+    const int chunks = 64;
+    std::vector<std::vector<ResEntry>> part(chunks);
+    parallel_windows(chunks, [&](int64_t q0, int64_t q1) {
+      for (int64_t q = q0; q < q1; ++q)
+        for (int64_t g = groups * q / chunks; g < groups * (q + 1) / chunks; ++g) {
+          const int w = gwin[g];
+          if (!in_range(w, 0, W)) continue;                 // beyond the matrix
+          int32_t c[4];
+          for (int p = 0; p < 4; ++p) {
+            c[p] = s_column[g * 4 + p];
+            if (c[p] < -1 || c[p] >= n_cols) { bad_col = true; c[p] = -1; }
+          }
+          for (int lr = 0; lr < 16; ++lr) {
+            if ((int64_t)w * 16 + lr >= n_rows) continue;
+            const int64_t at0 = (g * 16 + lr) * 2;
+            for (int s = 0; s < 2; ++s) {
+              const int64_t at = at0 + s;
+              const int pos = s_pos[at];
+              if (pos < 0 || pos > 3 || c[pos] < 0) continue;
+              if (s == 0 && s_pos[at0 + 1] == pos) continue;  // the later slot wins, as in a tile
+              const float v = s_value[at];
+              const int32_t e = s_edge ? s_edge[at] : -1;
+              if (v != 0.f || e >= 0) part[q].push_back({w * 16 + lr, c[pos], v, e});
+            }
+          }
         }
-      }
-    }
+    });
+    if (bad_col) { err = "s_column out of range"; return TR_ERR_ARG; }
+    size_t total = st.res.size();
+    for (const auto& v : part) total += v.size();
+    st.res.reserve(total);
+    for (auto& v : part) st.res.insert(st.res.end(), v.begin(), v.end());
     return TR_OK;
   }
   std::vector<std::vector<int64_t>> wg(W);
   for (int64_t g = 0; g < groups; ++g)
     if (in_range(gwin[g], 0, W)) wg[gwin[g]].push_back(g);   // others lie beyond the matrix
-  for (int w = 0; w < W; ++w) {
-    for (size_t i = 0; i < wg[w].size(); i += 4) {
+  parallel_windows(W, [&](int64_t w0, int64_t w1) {
+    for (int w = (int)w0; w < (int)w1; ++w) {
       WinTiles& wt = st.sp[w];
-      const size_t cbase = wt.col.size(), abase = wt.a.size();
-      wt.add_empty();
-      for (int ch = 0; ch < 4 && i + ch < wg[w].size(); ++ch) {
-        const int64_t g = wg[w][i + ch];
-        for (int p = 0; p < 4; ++p) {
-          const int32_t c = s_column[g * 4 + p];
-          if (c < -1 || c >= n_cols) { err = "s_column out of range"; return TR_ERR_ARG; }
-          wt.col[cbase + ch * 4 + p] = c;
-        }
-        for (int lr = 0; lr < 16; ++lr) {
-          if ((int64_t)w * 16 + lr >= n_rows) continue;
-          for (int s = 0; s < 2; ++s) {
-            const int64_t at = (g * 16 + lr) * 2 + s;
-            const int pos = s_pos[at];
-            if (pos < 0 || pos > 3 || wt.col[cbase + ch * 4 + pos] < 0) continue;   // kernel skips
-            wt.a[abase + a_index(lr, ch * 4 + pos)] = s_value[at];
-            wt.edge[abase + a_index(lr, ch * 4 + pos)] = s_edge ? s_edge[at] : -1;
+      const size_t nt = (wg[w].size() + 3) / 4;
+      wt.col.reserve(wt.col.size() + nt * 16);
+      wt.a.reserve(wt.a.size() + nt * 256);
+      wt.edge.reserve(wt.edge.size() + nt * 256);
+      for (size_t i = 0; i < wg[w].size(); i += 4) {
+        const size_t cbase = wt.col.size(), abase = wt.a.size();
+        wt.add_empty();
+        for (int ch = 0; ch < 4 && i + ch < wg[w].size(); ++ch) {
+          const int64_t g = wg[w][i + ch];
+          for (int p = 0; p < 4; ++p) {
+            int32_t c = s_column[g * 4 + p];
+            if (c < -1 || c >= n_cols) { bad_col = true; c = -1; }
+            wt.col[cbase + ch * 4 + p] = c;
+          }
+          for (int lr = 0; lr < 16; ++lr) {
+            if ((int64_t)w * 16 + lr >= n_rows) continue;
+            for (int s = 0; s < 2; ++s) {
+              const int64_t at = (g * 16 + lr) * 2 + s;
+              const int pos = s_pos[at];
+              if (pos < 0 || pos > 3 || wt.col[cbase + ch * 4 + pos] < 0) continue;   // kernel skips
+              wt.a[abase + a_index(lr, ch * 4 + pos)] = s_value[at];
+              wt.edge[abase + a_index(lr, ch * 4 + pos)] = s_edge ? s_edge[at] : -1;
+            }
           }
         }
       }
     }
-  }
+  });
+  if (bad_col) { err = "s_column out of range"; return TR_ERR_ARG; }
   return TR_OK;
 }
 
