@@ -84,27 +84,33 @@ struct Vote {
   float w;
 };
 
+// Per-label vote sums of one row (label-indexed, all zero between calls)
+// and the labels that received votes.
+struct VoteAcc {
+  std::vector<float> w;
+  std::vector<int32_t> touched;
+};
+
 // Label with the largest summed vote among those with room (size < cap),
-// the current label winning ties; `votes` is sorted in place.
-int32_t best_label(std::vector<Vote>& votes, int32_t cur, const std::vector<int32_t>& size,
-                   int32_t cap) {
-  std::sort(votes.begin(), votes.end(), [](const Vote& x, const Vote& y) { return x.label < y.label; });
-  float cur_w = 0.f;
-  for (const Vote& v : votes)
-    if (v.label == cur) cur_w += v.w;
-  int32_t best = cur;
-  float best_w = cur_w;
-  for (size_t i = 0; i < votes.size();) {
-    size_t j = i;
-    float w = 0.f;
-    while (j < votes.size() && votes[j].label == votes[i].label) w += votes[j++].w;
-    const int32_t l = votes[i].label;
-    if (l != cur && size[l] < cap && w > best_w) {
-      best = l;
-      best_w = w;
-    }
-    i = j;
+// the current label winning ties and otherwise the smallest label among
+// equal sums.  Vote weights are positive, so a zero sum marks a label that
+// has not been touched yet.
+int32_t best_label(const std::vector<Vote>& votes, int32_t cur, const std::vector<int32_t>& size,
+                   int32_t cap, VoteAcc& a) {
+  for (const Vote& v : votes) {
+    if (a.w[v.label] == 0.f) a.touched.push_back(v.label);
+    a.w[v.label] += v.w;
   }
+  std::sort(a.touched.begin(), a.touched.end());
+  int32_t best = cur;
+  float best_w = cur >= 0 ? a.w[cur] : 0.f;
+  for (int32_t l : a.touched)
+    if (l != cur && size[l] < cap && a.w[l] > best_w) {
+      best = l;
+      best_w = a.w[l];
+    }
+  for (int32_t l : a.touched) a.w[l] = 0.f;
+  a.touched.clear();
   return best;
 }
 
@@ -155,12 +161,14 @@ void cluster_rows(const Csr& a, std::vector<int32_t>& perm, int sweeps, int32_t 
   });
   std::vector<Vote> votes;
   const std::vector<int32_t> no_size(R, 0);
+  VoteAcc acc;
+  acc.w.assign(R, 0.f);
   for (int s = 0; s < sweeps; ++s) {
     if (!square) {
       for (int32_t c = 0; c < C; ++c) {
         votes.clear();
         for (int32_t e = cptr[c]; e < cptr[c + 1]; ++e) votes.push_back({rlab[crow[e]], rinv[crow[e]]});
-        clab[c] = votes.empty() ? -1 : best_label(votes, -1, no_size, INT32_MAX);
+        clab[c] = votes.empty() ? -1 : best_label(votes, -1, no_size, INT32_MAX, acc);
       }
     }
     int64_t changed = 0;
@@ -178,7 +186,7 @@ void cluster_rows(const Csr& a, std::vector<int32_t>& perm, int sweeps, int32_t 
         for (int32_t e = cptr[r]; e < cptr[r + 1]; ++e)
           if (crow[e] != r) votes.push_back({rlab[crow[e]], rinv[crow[e]]});
       const int32_t cur = rlab[r];
-      const int32_t l = best_label(votes, cur, rsize, cap);
+      const int32_t l = best_label(votes, cur, rsize, cap, acc);
       if (l != cur) {
         rsize[cur]--;
         rsize[l]++;
