@@ -79,40 +79,36 @@ inline uint32_t mix32(uint32_t x) {
   return x;
 }
 
-struct Vote {
-  int32_t label;
-  float w;
-};
-
-// Per-label vote sums of one row (label-indexed, all zero between calls)
-// and the labels that received votes.
+// Per-label vote sums of one row: label-indexed sums (all zero between rows)
+// and the labels that received votes.  Vote weights are positive, so a zero
+// sum marks a label that has not been touched yet.
 struct VoteAcc {
   std::vector<float> w;
   std::vector<int32_t> touched;
-};
 
-// Label with the largest summed vote among those with room (size < cap),
-// the current label winning ties and otherwise the smallest label among
-// equal sums.  Vote weights are positive, so a zero sum marks a label that
-// has not been touched yet.
-int32_t best_label(const std::vector<Vote>& votes, int32_t cur, const std::vector<int32_t>& size,
-                   int32_t cap, VoteAcc& a) {
-  for (const Vote& v : votes) {
-    if (a.w[v.label] == 0.f) a.touched.push_back(v.label);
-    a.w[v.label] += v.w;
+  void add(int32_t label, float v) {
+    if (w[label] == 0.f) touched.push_back(label);
+    w[label] += v;
   }
-  std::sort(a.touched.begin(), a.touched.end());
-  int32_t best = cur;
-  float best_w = cur >= 0 ? a.w[cur] : 0.f;
-  for (int32_t l : a.touched)
-    if (l != cur && size[l] < cap && a.w[l] > best_w) {
-      best = l;
-      best_w = a.w[l];
-    }
-  for (int32_t l : a.touched) a.w[l] = 0.f;
-  a.touched.clear();
-  return best;
-}
+  bool empty() const { return touched.empty(); }
+
+  // Label with the largest summed vote among those with room (size < cap),
+  // the current label winning ties and otherwise the smallest label among
+  // equal sums; clears the sums for the next row.
+  int32_t pick(int32_t cur, const std::vector<int32_t>& size, int32_t cap) {
+    std::sort(touched.begin(), touched.end());
+    int32_t best = cur;
+    float best_w = cur >= 0 ? w[cur] : 0.f;
+    for (int32_t l : touched)
+      if (l != cur && size[l] < cap && w[l] > best_w) {
+        best = l;
+        best_w = w[l];
+      }
+    for (int32_t l : touched) w[l] = 0.f;
+    touched.clear();
+    return best;
+  }
+};
 
 }  // namespace
 
@@ -159,34 +155,31 @@ void cluster_rows(const Csr& a, std::vector<int32_t>& perm, int sweeps, int32_t 
     const uint32_t hx = mix32((uint32_t)x * 2654435761u), hy = mix32((uint32_t)y * 2654435761u);
     return hx != hy ? hx < hy : x < y;
   });
-  std::vector<Vote> votes;
   const std::vector<int32_t> no_size(R, 0);
   VoteAcc acc;
   acc.w.assign(R, 0.f);
   for (int s = 0; s < sweeps; ++s) {
     if (!square) {
       for (int32_t c = 0; c < C; ++c) {
-        votes.clear();
-        for (int32_t e = cptr[c]; e < cptr[c + 1]; ++e) votes.push_back({rlab[crow[e]], rinv[crow[e]]});
-        clab[c] = votes.empty() ? -1 : best_label(votes, -1, no_size, INT32_MAX, acc);
+        for (int32_t e = cptr[c]; e < cptr[c + 1]; ++e) acc.add(rlab[crow[e]], rinv[crow[e]]);
+        clab[c] = acc.empty() ? -1 : acc.pick(-1, no_size, INT32_MAX);
       }
     }
     int64_t changed = 0;
     for (int32_t r : order) {
-      votes.clear();
       for (int32_t e = a.ptr[r]; e < a.ptr[r + 1]; ++e) {
         const int32_t c = a.idx[e];
         if (square) {
-          if (c != r) votes.push_back({rlab[c], rinv[c]});
+          if (c != r) acc.add(rlab[c], rinv[c]);
         } else if (clab[c] >= 0) {
-          votes.push_back({clab[c], cinv[c]});
+          acc.add(clab[c], cinv[c]);
         }
       }
       if (square)
         for (int32_t e = cptr[r]; e < cptr[r + 1]; ++e)
-          if (crow[e] != r) votes.push_back({rlab[crow[e]], rinv[crow[e]]});
+          if (crow[e] != r) acc.add(rlab[crow[e]], rinv[crow[e]]);
       const int32_t cur = rlab[r];
-      const int32_t l = best_label(votes, cur, rsize, cap, acc);
+      const int32_t l = acc.pick(cur, rsize, cap);
       if (l != cur) {
         rsize[cur]--;
         rsize[l]++;
