@@ -80,6 +80,10 @@ typedef struct tr_route_params {
   int32_t skip_tc;         /* LIBRA_SKIP_TC (0) */
   int32_t mode;            /* TR_ROUTE_COMPAT / TR_ROUTE_EXACT */
   int32_t threads;         /* host threads, <= 0 = all */
+  int32_t skip_sptc;       /* 1: no 2:4 groups; every column outside the dense-TC
+                              funnel goes to the CUDA parts (0; the plan builder
+                              sets it when demote_below > 16, where every 2:4
+                              column would be demoted) */
 } tr_route_params;
 
 typedef struct tr_route tr_route;

@@ -196,3 +196,20 @@ def test_empty_matrix_plan():
     P = trspmm.host_plan(np.zeros(4, np.int32), np.zeros(0, np.int32), np.zeros(0, np.float32),
                          3, 5, transpose=True, reorder=True)
     assert oracle.decode_plan(P)["all"].nnz == 0
+
+
+def test_skip_sptc_routes_every_non_tc_column_to_cuda():
+    """skip_sptc (set by the builder when demote_below > 16): no 2:4 groups,
+    the dense-TC funnel unchanged, the CUDA parts hold every other entry."""
+    g = graphs.route_mix(n=2048, target_nnz=100_000, seed=5)
+    full = trspmm.route(g.indptr, g.indices, g.values, mode="exact")
+    skip = trspmm.route(g.indptr, g.indices, g.values, mode="exact", skip_sptc=True)
+    names = trspmm.TABLE_NAMES
+    assert skip[names.index("s_column")].size == 0
+    for t in ("t_column", "t_binary", "t_value"):
+        assert np.array_equal(full[names.index(t)], skip[names.index(t)]), t
+    dec = oracle.decode_tables(skip, g.n_rows, g.n_cols)
+    A = sp.csr_matrix((np.asarray(g.values, np.float64), g.indices, g.indptr),
+                      shape=(g.n_rows, g.n_cols))
+    assert abs(dec["all"] - A).max() <= 1e-3 * abs(A).max()     # FP16 TC values
+    assert dec["sptc"].nnz == 0

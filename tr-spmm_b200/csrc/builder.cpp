@@ -265,7 +265,11 @@ int build_plan(const int32_t* indptr, const int32_t* indices, const float* value
     a = std::move(p);
   }
   RouteTables T;
-  rc = build_route(a.ptr.data(), a.idx.data(), a.val.data(), a.n_rows, params, T, err);
+  // every 2:4 column would be demoted: form no 2:4 groups at all (the same
+  // tiles and matrix; the residual keeps each row's entries in CSR order)
+  tr_route_params rp = params;
+  if (opts.demote_below > 16) rp.skip_sptc = 1;
+  rc = build_route(a.ptr.data(), a.idx.data(), a.val.data(), a.n_rows, rp, T, err);
   if (rc) return rc;
   PlanOptions po;
   po.row_scale = opts.row_scale != 0;

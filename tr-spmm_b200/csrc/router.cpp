@@ -213,9 +213,11 @@ void route_window(const int32_t* indptr, const int32_t* indices, const float* va
   }
 
   // ---- stage 2a: units (block_online.cpp:267-328) -------------------------
+  // (skip_sptc: no candidates, so no units, pairs or groups; the columns
+  // outside the TC funnel keep route 0 and go to the CUDA parts)
   S.tmp.clear();
   uint32_t any_odd = 0;
-  for (int i = 0; i < np; ++i)
+  for (int i = 0; i < np && !p.skip_sptc; ++i)
     if (prof[i].route != 1) { S.tmp.push_back(i); any_odd |= prof[i].vec & kOddBits; }
   order_by_count(prof, S.tmp, S.cand);
   S.units.clear();

@@ -62,7 +62,8 @@ class RouteParams(ctypes.Structure):
                                                  "window", "wide")] + [
         ("tc_min_util", ctypes.c_float), ("sptc_min_util", ctypes.c_float),
         ("sptc_threshold", ctypes.c_int32), ("unit_min_nnz", ctypes.c_int32),
-        ("skip_tc", ctypes.c_int32), ("mode", ctypes.c_int32), ("threads", ctypes.c_int32)]
+        ("skip_tc", ctypes.c_int32), ("mode", ctypes.c_int32), ("threads", ctypes.c_int32),
+        ("skip_sptc", ctypes.c_int32)]
 
 
 class PlanInfo(ctypes.Structure):

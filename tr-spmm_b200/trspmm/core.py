@@ -70,7 +70,7 @@ def plan_opts(row_scale=False, promote_min=0, transpose=False, reorder=False, de
 
 def _params(partsize_t=32, partsize_c=32, shortsize=3, density=8, window=16, wide=16,
             tc_min_util=0.0, sptc_min_util=0.5, sptc_threshold=12, unit_min_nnz=None,
-            skip_tc=None, mode="compat", threads=0):
+            skip_tc=None, mode="compat", threads=0, skip_sptc=False):
     if unit_min_nnz is None:
         unit_min_nnz = int(os.environ.get("LIBRA_SPTC_UNIT_MIN_NNZ", "2"))
     if skip_tc is None:
@@ -78,21 +78,24 @@ def _params(partsize_t=32, partsize_c=32, shortsize=3, density=8, window=16, wid
     m = {"compat": TR_ROUTE_COMPAT, "exact": TR_ROUTE_EXACT}[mode]
     return RouteParams(int(partsize_t), int(partsize_c), int(shortsize), int(density), int(window),
                        int(wide), float(tc_min_util), float(sptc_min_util), int(sptc_threshold),
-                       int(unit_min_nnz), int(bool(skip_tc)), m, int(threads))
+                       int(unit_min_nnz), int(bool(skip_tc)), m, int(threads),
+                       int(bool(skip_sptc)))
 
 
 def route(indptr, indices, values, partsize_t=32, partsize_c=32, shortsize=3, density=8,
           window=16, wide=16, tc_min_util=0.0, sptc_min_util=0.5, sptc_threshold=12,
-          mode="compat", unit_min_nnz=None, skip_tc=None, threads=0):
+          mode="compat", unit_min_nnz=None, skip_tc=None, threads=0, skip_sptc=False):
     """Route a CSR matrix; returns the 30 tables of block_sptc_2to4_online
     (TR-source/Block/block_online.cpp:844-870) as numpy arrays, the last being
-    the routing time in seconds (float32)."""
+    the routing time in seconds (float32).  skip_sptc: no 2:4 groups (every
+    column outside the dense-TC funnel goes to the CUDA parts)."""
     L = lib()
     rp = np.ascontiguousarray(indptr, dtype=np.int32)
     ci = np.ascontiguousarray(indices, dtype=np.int32)
     vv = np.ascontiguousarray(values, dtype=np.float32)
     prm = _params(partsize_t, partsize_c, shortsize, density, window, wide, tc_min_util,
-                  sptc_min_util, sptc_threshold, unit_min_nnz, skip_tc, mode, threads)
+                  sptc_min_util, sptc_threshold, unit_min_nnz, skip_tc, mode, threads,
+                  skip_sptc)
     h = ctypes.c_void_p()
     check(L.tr_route_build(_vp(rp), _vp(ci), _vp(vv), rp.shape[0] - 1, ctypes.byref(prm),
                            ctypes.byref(h)))
