@@ -20,6 +20,7 @@
 #include <cstring>
 #include <numeric>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/trspmm.h"
@@ -52,24 +53,62 @@ int validate_csr(const int32_t* indptr, const int32_t* indices, int32_t n_rows, 
 
 namespace {
 
+// A^T as CSR, entries of each row of A^T in A's row order (a stable counting
+// sort by column).  Host threads take contiguous ranges of A's rows, count
+// their entries per column, and scatter from per-(column, thread) offsets, so
+// the result is the sequential one.
 void transpose(const Csr& a, Csr& t) {
   t.n_rows = a.n_cols;
   t.n_cols = a.n_rows;
   const int64_t nnz = (int64_t)a.idx.size();
-  t.ptr.assign((size_t)t.n_rows + 1, 0);
-  for (int32_t c : a.idx) t.ptr[c + 1]++;
-  for (int32_t r = 0; r < t.n_rows; ++r) t.ptr[r + 1] += t.ptr[r];
+  const int32_t C = a.n_cols, R = a.n_rows;
+  t.ptr.assign((size_t)C + 1, 0);
   t.idx.resize(nnz);
   t.val.resize(nnz);
   t.src.resize(nnz);
-  std::vector<int32_t> fill(t.ptr.begin(), t.ptr.end() - 1);
-  for (int32_t r = 0; r < a.n_rows; ++r)
-    for (int32_t e = a.ptr[r]; e < a.ptr[r + 1]; ++e) {
-      const int32_t at = fill[a.idx[e]]++;
-      t.idx[at] = r;
-      t.val[at] = a.val[e];
-      t.src[at] = a.src[e];
+  int T = (int)std::max(1u, std::thread::hardware_concurrency());
+  T = (int)std::min<int64_t>(T, std::max<int64_t>(1, nnz / 65536));
+  while (T > 1 && (int64_t)T * C > ((int64_t)1 << 26)) --T;      // per-thread counts fit
+  std::vector<int32_t> r_at(T + 1);
+  {
+    int32_t r = 0;                          // row ranges of about nnz / T entries
+    for (int k = 0; k <= T; ++k) {
+      const int64_t want = nnz * k / T;
+      while (r < R && a.ptr[r] < want) ++r;
+      r_at[k] = k == T ? R : r;
     }
+  }
+  std::vector<std::vector<int32_t>> off(T, std::vector<int32_t>((size_t)C, 0));
+  auto run = [&](auto body) {
+    std::vector<std::thread> pool;
+    for (int k = 1; k < T; ++k) pool.emplace_back(body, k);
+    body(0);
+    for (auto& th : pool) th.join();
+  };
+  run([&](int k) {
+    for (int32_t r = r_at[k]; r < r_at[k + 1]; ++r)
+      for (int32_t e = a.ptr[r]; e < a.ptr[r + 1]; ++e) off[k][a.idx[e]]++;
+  });
+  int32_t base = 0;
+  for (int32_t c = 0; c < C; ++c) {
+    t.ptr[c] = base;
+    for (int k = 0; k < T; ++k) {
+      const int32_t n = off[k][c];
+      off[k][c] = base;
+      base += n;
+    }
+  }
+  t.ptr[C] = base;
+  run([&](int k) {
+    std::vector<int32_t>& fill = off[k];
+    for (int32_t r = r_at[k]; r < r_at[k + 1]; ++r)
+      for (int32_t e = a.ptr[r]; e < a.ptr[r + 1]; ++e) {
+        const int32_t at = fill[a.idx[e]]++;
+        t.idx[at] = r;
+        t.val[at] = a.val[e];
+        t.src[at] = a.src[e];
+      }
+  });
 }
 
 inline uint32_t mix32(uint32_t x) {
