@@ -182,3 +182,12 @@ def test_loader_reorders_rows_when_asked(monkeypatch):
     monkeypatch.setenv("LIBRA_TCA_REORDER", "0")
     d0 = DS.from_csr(g.indptr, g.indices, g.n_cols, 16)
     assert d0.reorder_id is None and np.array_equal(d0.row_pointers.numpy()[:g.n_rows + 1], g.indptr)
+
+
+def test_device_stages_without_a_gpu_raise():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("checks the error path of a machine without a CUDA device")
+    g = _graph("dup_300x200")
+    with pytest.raises(trspmm.TrError, match="TCA signatures"):
+        core.tca_order(g.indptr, g.indices, device=True)
