@@ -25,6 +25,7 @@
 //  * windows are processed in parallel chunks and concatenated in window
 //    order.
 #include <algorithm>
+#include <functional>
 #include <array>
 #include <atomic>
 #include <chrono>
@@ -524,6 +525,22 @@ void prefix_append(std::vector<int32_t>& dst, const std::vector<int32_t>& counts
   for (int32_t c : counts) { b += c; dst.push_back((int32_t)b); }
 }
 
+// dst += the field `get` of every chunk, in chunk order: sized once, then
+// copied (each chunk's field is released after its copy).
+template <typename T, typename Get>
+void concat(std::vector<T>& dst, std::vector<Chunk>& chunks, Get get) {
+  size_t total = dst.size();
+  for (auto& ck : chunks) total += get(ck).size();
+  size_t at = dst.size();
+  dst.resize(total);
+  for (auto& ck : chunks) {
+    std::vector<T>& v = get(ck);
+    std::copy(v.begin(), v.end(), dst.begin() + at);
+    at += v.size();
+    std::vector<T>().swap(v);
+  }
+}
+
 }  // namespace
 
 int build_route(const int32_t* indptr, const int32_t* indices, const float* values,
@@ -577,46 +594,41 @@ int build_route(const int32_t* indptr, const int32_t* indices, const float* valu
   RouteTables& T = out;
   T = RouteTables();
   T.window = p.window;
+  // offsets and counts in chunk order (small), then the large tables, each
+  // concatenated on its own host thread (the same arrays as appending chunk
+  // by chunk)
   int64_t group_base = 0;
   for (auto& ck : chunks) {
     prefix_append(T.t_row_offset, ck.t_parts);
     prefix_append(T.t_block_offset, ck.t_subcounts);
-    append(T.t_column, ck.t_column);
-    append(T.t_value, ck.t_value);
-    append(T.t_window_row, ck.t_window_row);
-    append(T.t_atomic, ck.t_atomic);
-    append(T.t_binary, ck.t_binary);
-    append(T.t_edge, ck.t_edge);
-    append(T.c_edge, ck.c_edge);
-    append(T.s_edge, ck.s_edge);
     prefix_append(T.c_row_offset, ck.c_counts);
-    append(T.c_row, ck.c_row);
-    append(T.c_atomic, ck.c_atomic);
-    append(T.c_column, ck.c_column);
-    append(T.c_value, ck.c_value);
-    append(T.s_column, ck.s_column);
-    append(T.s_mask, ck.s_mask);
-    append(T.s_value, ck.s_value);
-    append(T.s_pos, ck.s_pos);
-    append(T.s_window, ck.s_window);
     prefix_append(T.s_offsets, ck.s_groups_per_window);
-    append(T.s_tile_window, ck.s_tile_window);
-    for (int32_t g : ck.s_tile_group_local) T.s_tile_group.push_back((int32_t)(g + group_base));
-    append(T.s_tile_column, ck.s_tile_column);
-    append(T.s_packed_a, ck.s_packed_a);
-    append(T.s_packed_meta, ck.s_packed_meta);
     prefix_append(T.s_window_tile_offset, ck.s_tiles_per_window);
+    for (int32_t g : ck.s_tile_group_local) T.s_tile_group.push_back((int32_t)(g + group_base));
     group_base += (int64_t)ck.s_window.size();
     T.dropped += ck.lost;
   }
   // the short residual parts follow all long ones (block_online.cpp:770-778)
-  for (auto& ck : chunks) {
-    prefix_append(T.cs_row_offset, ck.cs_counts);
-    append(T.cs_row, ck.cs_row);
-    append(T.cs_atomic, ck.cs_atomic);
-    append(T.cs_column, ck.cs_column);
-    append(T.cs_value, ck.cs_value);
-    append(T.cs_edge, ck.cs_edge);
+  for (auto& ck : chunks) prefix_append(T.cs_row_offset, ck.cs_counts);
+#define TRS_CAT(F) [&] { concat(T.F, chunks, [](Chunk& c) -> decltype(c.F)& { return c.F; }); }
+  std::vector<std::function<void()>> tasks = {
+      TRS_CAT(t_column),   TRS_CAT(t_value),      TRS_CAT(t_window_row), TRS_CAT(t_atomic),
+      TRS_CAT(t_binary),   TRS_CAT(t_edge),       TRS_CAT(c_edge),       TRS_CAT(s_edge),
+      TRS_CAT(c_row),      TRS_CAT(c_atomic),     TRS_CAT(c_column),     TRS_CAT(c_value),
+      TRS_CAT(s_column),   TRS_CAT(s_mask),       TRS_CAT(s_value),      TRS_CAT(s_pos),
+      TRS_CAT(s_window),   TRS_CAT(s_tile_window), TRS_CAT(s_tile_column), TRS_CAT(s_packed_a),
+      TRS_CAT(s_packed_meta), TRS_CAT(cs_row),    TRS_CAT(cs_atomic),    TRS_CAT(cs_column),
+      TRS_CAT(cs_value),   TRS_CAT(cs_edge)};
+#undef TRS_CAT
+  {
+    std::atomic<size_t> next_task{0};
+    auto run = [&]() {
+      for (size_t i; (i = next_task.fetch_add(1)) < tasks.size();) tasks[i]();
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(run);
+    run();
+    for (auto& th : pool) th.join();
   }
   if (p.mode == TR_ROUTE_EXACT) T.dropped = 0;
   T.seconds = std::chrono::duration<double>(std::chrono::high_resolution_clock::now() - t0).count();
