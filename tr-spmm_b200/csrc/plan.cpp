@@ -256,23 +256,52 @@ void flatten(HostPlan& hp, Staging& st, const PlanOptions& opt, int64_t n_edges)
   });
   const int64_t T = (int64_t)hp.tile_col.size() / 16;
   // ---- residual CSR over padded rows, entries of a row in table order -------
+  // (a stable counting sort by row: host threads take contiguous ranges of
+  // the entries, count per row, and scatter from per-(row, thread) offsets)
+  const int64_t NR = (int64_t)st.res.size();
+  int nt = (int)std::max(1u, std::thread::hardware_concurrency());
+  nt = (int)std::min<int64_t>(nt, std::max<int64_t>(1, NR / 65536));
+  while (nt > 1 && (int64_t)nt * rows > ((int64_t)1 << 26)) --nt;
+  std::vector<std::vector<int32_t>> off(nt, std::vector<int32_t>((size_t)rows, 0));
+  auto on_ranges = [&](auto body) {
+    std::vector<std::thread> pool;
+    for (int k = 1; k < nt; ++k) pool.emplace_back(body, k);
+    body(0);
+    for (auto& th : pool) th.join();
+  };
+  on_ranges([&](int k) {
+    for (int64_t i = NR * k / nt; i < NR * (k + 1) / nt; ++i) off[k][st.res[i].row]++;
+  });
   hp.res_ptr.assign(rows + 1, 0);
-  for (auto& e : st.res) hp.res_ptr[e.row + 1]++;
-  for (int64_t i = 0; i < rows; ++i) hp.res_ptr[i + 1] += hp.res_ptr[i];
+  {
+    int32_t base = 0;
+    for (int64_t r = 0; r < rows; ++r) {
+      hp.res_ptr[r] = base;
+      for (int k = 0; k < nt; ++k) {
+        const int32_t c = off[k][r];
+        off[k][r] = base;
+        base += c;
+      }
+    }
+    hp.res_ptr[rows] = base;
+  }
   hp.res_col.resize(hp.res_ptr[rows]);
   hp.res_val.resize(hp.res_ptr[rows]);
   hp.res_edge.assign(hp.res_ptr[rows], -1);
-  std::vector<int32_t> fill(hp.res_ptr.begin(), hp.res_ptr.end() - 1);
-  for (auto& e : st.res) {
-    const int32_t at = fill[e.row]++;
-    hp.res_col[at] = e.col;
-    hp.res_val[at] = f2h(e.val / hp.row_scale[e.row]);
-    if (e.edge >= 0 && e.edge < n_edges) {
-      hp.res_edge[at] = e.edge;
-      hp.val_slot[e.edge] = (int32_t)(T * 256 + at);
-      hp.edge_row[e.edge] = e.row;
+  on_ranges([&](int k) {
+    std::vector<int32_t>& fill = off[k];
+    for (int64_t i = NR * k / nt; i < NR * (k + 1) / nt; ++i) {
+      const ResEntry& e = st.res[i];
+      const int32_t at = fill[e.row]++;
+      hp.res_col[at] = e.col;
+      hp.res_val[at] = f2h(e.val / hp.row_scale[e.row]);
+      if (e.edge >= 0 && e.edge < n_edges) {
+        hp.res_edge[at] = e.edge;
+        hp.val_slot[e.edge] = (int32_t)(T * 256 + at);
+        hp.edge_row[e.edge] = e.row;
+      }
     }
-  }
+  });
   // ---- launch order: heaviest windows first (cost ~ gathered rows) -----------
   std::vector<int64_t> cost(W);
   for (int w = 0; w < W; ++w)
