@@ -24,6 +24,8 @@ CASES = {
     "sbm_3000": lambda: graphs.sbm_powerlaw(n=3000, avg_degree=20, communities=30, seed=4),
     "ragged_500x300": lambda: graphs.random_csr(500, 300, 0.05, seed=2, empty_rows=0.4),
     "dup_300x200": lambda: graphs.random_csr(300, 200, 0.08, seed=7, dup=True),
+    "batched_24": lambda: graphs.batched(num_graphs=24, seed=11),
+    "rect_400x900": lambda: graphs.random_csr(400, 900, 0.02, seed=13, empty_rows=0.1),
 }
 _built = {}
 
