@@ -14,8 +14,9 @@ Everything else -- candidate queueing, Jaccard, both clustering levels, the
 final order, the rebuilt column array -- is the reference's code.  The
 reference's rebuilt row pointers are recorded only by their last value: its
 loop leaves every row empty (row_ptr all zeros), a defect the library does
-not reproduce.  Run from the repository root:
-    python tests/golden/make_tca_golden.py
+not reproduce.  Run from the repository root with the reference checkout's
+root directory as the argument (or in TR_REFERENCE_ROOT):
+    python tests/golden/make_tca_golden.py <reference root>
 """
 import contextlib
 import hashlib
@@ -39,7 +40,7 @@ sys.path.insert(0, os.path.join(ROOT, "tr-spmm_b200"))
 from oracle import tca as otca           # noqa: E402  (hash family of the stand-in)
 from trspmm import graphs                # noqa: E402
 
-REF = "/root/reference/spmm/tr_csr_fp16/tr_tca_reorder.py"
+REF_FILE = os.path.join("spmm", "tr_csr_fp16", "tr_tca_reorder.py")
 
 
 class _MinHash:
@@ -130,9 +131,13 @@ def checksum(g):
 
 
 def main():
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TR_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_tca_golden.py <reference root> (or set TR_REFERENCE_ROOT)")
+    ref = os.path.join(root, REF_FILE)
     sys.modules["datasketch"] = types.SimpleNamespace(MinHash=_MinHash, MinHashLSH=_MinHashLSH)
     queue.PriorityQueue = _StablePQ
-    spec = importlib.util.spec_from_file_location("tr_tca_reorder_ref", REF)
+    spec = importlib.util.spec_from_file_location("tr_tca_reorder_ref", ref)
     mod = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mod)
     out = {"source": "spmm/tr_csr_fp16/tr_tca_reorder.py apply_tca_reorder(thres=16)",

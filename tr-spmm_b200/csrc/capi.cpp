@@ -4,8 +4,11 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/trspmm.h"
@@ -40,6 +43,19 @@ int fail(int code, const std::string& msg) {
 int cuda_fail(cudaError_t e, const char* what) {
   g_error = std::string(what) + ": " + cudaGetErrorString(e);
   return TR_ERR_CUDA;
+}
+
+int kernel_smem_limit(const void* kernel, int bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, int> set_to;
+  int dev = 0;
+  TRS_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lock(mu);
+  int& have = set_to[std::make_pair(dev, kernel)];
+  if (have >= bytes) return TR_OK;
+  TRS_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  have = bytes;
+  return TR_OK;
 }
 
 namespace {
@@ -200,6 +216,7 @@ int tr_route_tc_device(const int32_t* d_indptr, const int32_t* d_indices, const 
                        int32_t n_rows, const tr_route_params* params, tr_route** out) {
   if (!d_indptr || !params || !out) return fail(TR_ERR_ARG, "null argument");
   if (n_rows < 0) return fail(TR_ERR_ARG, "negative row count");
+  if (n_rows > 0 && (!d_indices || !d_values)) return fail(TR_ERR_ARG, "null indices or values");
   if (params->window != 16) return fail(TR_ERR_UNSUPPORTED, "the device router uses 16-row windows");
   RouteGpuParams gp;
   gp.window = 16;
@@ -232,6 +249,7 @@ int tr_route_tc_device_noalloc(const int32_t* d_indptr, const int32_t* d_indices
                                int64_t cap_sub, int64_t cap_val, int64_t* n_sub_out,
                                int64_t* n_val_out, void* stream) {
   if (!d_indptr || !params) return fail(TR_ERR_ARG, "null argument");
+  if (n_rows > 0 && (!d_indices || !d_values)) return fail(TR_ERR_ARG, "null indices or values");
   if (params->window != 16) return fail(TR_ERR_UNSUPPORTED, "the device router uses 16-row windows");
   if (cap_sub > 0 && (!t_column || !t_binary || !t_block_offset))
     return fail(TR_ERR_ARG, "null table buffer with a non-zero sub-block capacity");

@@ -13,6 +13,10 @@ namespace trs {
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
+// Raises a kernel's dynamic shared-memory limit to `bytes` on the current
+// device.  The attribute belongs to (device, kernel), so it is set once per
+// pair; thread-safe.
+int kernel_smem_limit(const void* kernel, int bytes);
 
 #define TRS_CUDA(call)                                           \
   do {                                                           \

@@ -442,12 +442,8 @@ int make_b_map(CUtensorMap* map, const void* b, int32_t n_cols, int32_t k) {
 template <bool F16OUT, int NCH, int TPS, bool ACC>
 int launch_pipe_t(const tr_plan* p, const __half* b, int32_t k, void* c, cudaStream_t stream) {
   using Cfg = PipeCfg<NCH, TPS>;
-  static bool attr = false;
-  if (!attr) {
-    TRS_CUDA(cudaFuncSetAttribute(pipe_kernel<F16OUT, NCH, TPS, ACC>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::kSmem));
-    attr = true;
-  }
+  if (int rc = kernel_smem_limit((const void*)pipe_kernel<F16OUT, NCH, TPS, ACC>, Cfg::kSmem))
+    return rc;
   CUtensorMap map;
   int rc = make_b_map(&map, b, p->view.n_cols, k);
   if (rc) return rc;

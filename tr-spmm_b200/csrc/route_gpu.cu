@@ -29,6 +29,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -217,7 +218,7 @@ constexpr int kSmemRoute = 64 * 4;        // s_int scratch after the storage
 // FILL == false: sub-blocks and values per window into n_sub / n_val.
 // FILL == true:  the tables at sub_off / val_off.
 // NOALLOC (the entry point that allocates nothing): windows beyond shared
-// memory are refused (status[0] |= 1, no output), nothing is written when
+// memory are refused (status[0] |= 1), nothing is written when any window was refused or when
 // the scanned totals exceed the caller's capacities (status[0] |= 2), and
 // each sub-block's value count goes to sub_nval[sb + s] for the caller's
 // t_block_offset (sub_nval = t_block_offset + 1).
@@ -243,7 +244,7 @@ __global__ void __launch_bounds__(kRThreads) tc_funnel_kernel(
       }
       return;
     }
-    if (FILL && (status[0] & 2)) return;
+    if (FILL && status[0]) return;
   }
   if (n <= kSmemKeys) bind_storage(w, smem_route, kSmemKeys);
   else bind_storage(w, big_scratch + big_off[wi], next_pow2((uint32_t)n));
@@ -339,12 +340,9 @@ int route_tc_gpu(const int32_t* d_indptr, const int32_t* d_indices, const float*
     return rc;
   TRS_CUDA(cudaMemcpy(d_big_off.p, big_off.data(), W * 8, cudaMemcpyHostToDevice));
   const int smem = (int)storage_bytes(kSmemKeys) + kSmemRoute;
-  static bool attr = false;
-  if (!attr) {
-    TRS_CUDA(cudaFuncSetAttribute(tc_funnel_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    TRS_CUDA(cudaFuncSetAttribute(tc_funnel_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    attr = true;
-  }
+  if ((rc = kernel_smem_limit((const void*)tc_funnel_kernel<false>, smem)) ||
+      (rc = kernel_smem_limit((const void*)tc_funnel_kernel<true>, smem)))
+    return rc;
   tc_funnel_kernel<false><<<W, kRThreads, smem>>>(d_indptr, d_indices, d_values, n_rows, p,
                                                   d_big_off.p, d_big.p, d_nsub.p, d_nval.p, nullptr,
                                                   nullptr, nullptr, nullptr, nullptr, nullptr,
@@ -503,9 +501,11 @@ __global__ void noalloc_block_offsets_kernel(int32_t* a, const int* status) {
 // shared-memory limit, once per device.
 int noalloc_setup(int** scratch) {
   static int* addr[128] = {nullptr};
+  static std::mutex mu;
   int dev = 0;
   TRS_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 128) return fail(TR_ERR_UNSUPPORTED, "device ordinal beyond 127");
+  std::lock_guard<std::mutex> lock(mu);
   if (!addr[dev]) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);

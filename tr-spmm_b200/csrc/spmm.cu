@@ -1219,12 +1219,9 @@ int launch_residual(const PlanView& v, const __half* bh, int32_t k, void* c, boo
 template <bool ACC>
 int launch_per_window(const PlanView& v, const __half* bh, int32_t k, void* c, bool f16,
                       int route_mask, cudaStream_t stream) {
-  static bool attr[2] = {false, false};
-  if (!attr[f16]) {
-    if (f16) TRS_CUDA(cudaFuncSetAttribute(routed_kernel<true, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemRouted));
-    else TRS_CUDA(cudaFuncSetAttribute(routed_kernel<false, ACC>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemRouted));
-    attr[f16] = true;
-  }
+  if (int rc = kernel_smem_limit(f16 ? (const void*)routed_kernel<true, ACC>
+                                     : (const void*)routed_kernel<false, ACC>, kSmemRouted))
+    return rc;
   if (f16) routed_kernel<true, ACC><<<v.n_windows, kThreads, kSmemRouted, stream>>>(v, bh, k, c, route_mask);
   else routed_kernel<false, ACC><<<v.n_windows, kThreads, kSmemRouted, stream>>>(v, bh, k, c, route_mask);
   TRS_CUDA(cudaGetLastError());

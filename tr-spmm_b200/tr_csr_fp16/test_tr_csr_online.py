@@ -13,18 +13,19 @@ import Libra6SpMMOnline
 from tr_csr_fp16.mdataset2_online import GCN_dataset_tcu_sptc_cuda_online
 
 
+# The nine SPTC tensors of the parallel operator, in argument order; the
+# offset tables keep their length when the route is switched off (every
+# window then owns no group and no tile), the others become empty.
+_SPTC_NAMES = ("s_columnTensor", "s_valueTensor", "s_posTensor", "s_offsetTensor",
+               "s_tile_windowTensor", "s_tile_columnTensor", "s_packed_aTensor",
+               "s_packed_metaTensor", "s_window_tile_offsetTensor")
+_SPTC_OFFSETS = {"s_offsetTensor", "s_window_tile_offsetTensor"}
+
+
 def _zero_sptc_like(inputInfo):
-    groups = inputInfo.s_columnTensor[:0].contiguous()
-    values = inputInfo.s_valueTensor[:0].contiguous()
-    pos = inputInfo.s_posTensor[:0].contiguous()
-    offsets = torch.zeros_like(inputInfo.s_offsetTensor)
-    tile_window = inputInfo.s_tile_windowTensor[:0].contiguous()
-    tile_column = inputInfo.s_tile_columnTensor[:0].contiguous()
-    packed_a = inputInfo.s_packed_aTensor[:0].contiguous()
-    packed_meta = inputInfo.s_packed_metaTensor[:0].contiguous()
-    window_tile_offset = torch.zeros_like(inputInfo.s_window_tile_offsetTensor)
-    return (groups, values, pos, offsets, tile_window, tile_column, packed_a, packed_meta,
-            window_tile_offset)
+    """The SPTC arguments of a run without the SPTC route."""
+    return tuple(torch.zeros_like(t) if n in _SPTC_OFFSETS else t.new_empty((0,) + tuple(t.shape[1:]))
+                 for n, t in ((n, getattr(inputInfo, n)) for n in _SPTC_NAMES))
 
 
 def _parallel_call(inputInfo, epoches, sptc):
@@ -48,10 +49,7 @@ def _parallel_call(inputInfo, epoches, sptc):
 
 
 def _full_sptc(inputInfo):
-    return (inputInfo.s_columnTensor, inputInfo.s_valueTensor, inputInfo.s_posTensor,
-            inputInfo.s_offsetTensor, inputInfo.s_tile_windowTensor,
-            inputInfo.s_tile_columnTensor, inputInfo.s_packed_aTensor,
-            inputInfo.s_packed_metaTensor, inputInfo.s_window_tile_offsetTensor)
+    return tuple(getattr(inputInfo, n) for n in _SPTC_NAMES)
 
 
 def _base_tcu_cuda_profile_online(inputInfo, epoches):
