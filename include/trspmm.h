@@ -211,6 +211,9 @@ typedef struct tr_plan_info {
   int64_t promoted_tiles;  /* 16x16 tiles holding residual columns moved onto the tensor cores */
   int32_t row_scaled;      /* 1 if values are stored as FP16(v / row scale) */
   int32_t reordered;       /* 1 if the plan's rows were clustered before routing */
+  int32_t engine;          /* TR_ENGINE_WINDOW or TR_ENGINE_BLOCK */
+  int32_t n_blocks;        /* 128-row blocks (block engine) */
+  int64_t chunks;          /* 16-column chunks = tensor-core MMAs per product (block engine) */
 } tr_plan_info;
 
 /* Host route tables (pointer + element count each), in the reference's
@@ -264,7 +267,26 @@ typedef struct tr_plan_opts {
   const int32_t* row_order;  /* TR_REORDER_GIVEN: host array [rows of the
                               (transposed) matrix], plan row i = row_order[i],
                               a permutation (e.g. from tr_tca_order) */
+  int32_t engine;          /* TR_ENGINE_WINDOW (0): the reference's three routes
+                              over 16-row windows; TR_ENGINE_BLOCK: every entry
+                              on the tensor cores over 128-row blocks, each
+                              distinct column of a block gathered once (route
+                              parameters, promote_min and demote_below do not
+                              apply) */
 } tr_plan_opts;
+
+/* Plan engines (tr_plan_opts.engine).
+ *   TR_ENGINE_WINDOW  the routed layout: dense-TC and 2:4 tiles of 16-row
+ *                     windows on the tensor cores, the residual on CUDA cores
+ *   TR_ENGINE_BLOCK   128-row blocks: the distinct columns of a block are
+ *                     the K slots of 16-column chunks, one tcgen05.mma
+ *                     (M = 128 rows, N = K features) per chunk with FP32
+ *                     accumulation in TMEM; each row of B is gathered once
+ *                     per block and each output row written once (bitwise
+ *                     repeatable).  Pays off when rows that share columns
+ *                     sit in the same block (reorder = TR_REORDER_LABEL on
+ *                     community-structured graphs). */
+enum { TR_ENGINE_WINDOW = 0, TR_ENGINE_BLOCK = 1 };
 
 /* Row orders of tr_plan_opts.reorder:
  *   TR_REORDER_NONE     natural order
@@ -319,8 +341,9 @@ int tr_plan_build(const int32_t* indptr, const int32_t* indices, const float* va
  * (for inspection and host-side tests; no device needed).  Arrays by index:
  * 0 win_tile, 1 win_split, 2 win_prom, 3 tile_col, 4 tile_a (FP16 bits),
  * 5 res_ptr, 6 res_col, 7 res_val (FP16 bits), 8 win_order, 9 row_scale
- * (FP32), 10 row_out, 11 val_slot, 12 edge_row, 13 res_edge; `count` is in
- * elements. */
+ * (FP32), 10 row_out, 11 val_slot, 12 edge_row, 13 res_edge; block layout:
+ * 14 blk_chunk, 15 chunk_col, 16 chunk_ent, 17 ent_pos (uint16), 18 ent_val
+ * (FP16 bits), 19 ent_src, 20 blk_order; `count` is in elements. */
 typedef struct tr_host_plan tr_host_plan;
 int tr_plan_build_host(const int32_t* indptr, const int32_t* indices, const float* values,
                        int32_t n_rows, int32_t n_cols, const tr_route_params* params,

@@ -305,6 +305,8 @@ def decode_plan(P):
     matrices {'tc', 'sptc', 'prom' (tile parts), 'res', 'all'} in the output
     row space, values as the kernels see them (FP16 x FP32 scale)."""
     n_rows, n_cols = int(P["n_rows"]), int(P["n_cols"])
+    if len(P.get("blk_order", ())):
+        return decode_block_plan(P)
     wt, split, prom = P["win_tile"], P["win_split"], P["win_prom"]
     W = len(wt) - 1
     a = P["tile_a"].view(np.float16).astype(np.float64)
@@ -349,9 +351,46 @@ def decode_plan(P):
             "all": total}
 
 
+def decode_block_plan(P):
+    """The matrix a block-layout plan multiplies (layout in
+    tr-spmm_b200/csrc/plan.h): chunk c of block b multiplies B[chunk_col[16c
+    + k]] into plan row 128b + m for every entry at byte offset
+    (m//8)*256 + (k//8)*128 + (m%8)*16 + (k%8)*2 of its A tile; plan row r is
+    scaled by row_scale[r] and lands in output row row_out[r].  Also checks
+    that no two entries of a chunk share a tile position and that every
+    entry's slot holds a column.  Returns {'block', 'all'} (CSR float64)."""
+    n_rows, n_cols = int(P["n_rows"]), int(P["n_cols"])
+    bc, cc, ce = P["blk_chunk"], P["chunk_col"], P["chunk_ent"]
+    pos = P["ent_pos"].astype(np.int64)
+    m = (pos >> 8) * 8 + ((pos >> 4) & 7)
+    k = ((pos >> 7) & 1) * 8 + ((pos >> 1) & 7)
+    assert ((pos & 1) == 0).all() and (pos < 4096).all(), "entry outside its A tile"
+    n_chunks = len(ce) - 1
+    chunk_of = np.repeat(np.arange(n_chunks), np.diff(ce))
+    blk_of_chunk = np.repeat(np.arange(len(bc) - 1), np.diff(bc))
+    blk = blk_of_chunk[chunk_of]
+    cols = cc[chunk_of * 16 + k]
+    assert (cols >= 0).all(), "entry in an empty column slot"
+    key = chunk_of * 4096 + pos
+    assert np.unique(key).size == key.size, "two entries at one tile position"
+    prow = blk * 128 + m
+    out = P["row_out"]
+    assert (out[prow] >= 0).all(), "entry in a padding row"
+    vv = P["ent_val"].view(np.float16).astype(np.float64) * P["row_scale"].astype(np.float64)[prow]
+    mat = sp.csr_matrix((vv, (out[prow], cols)), shape=(n_rows, n_cols))
+    return {"block": mat, "all": mat}
+
+
 def plan_value_of_entries(P):
     """Value the plan holds for each CSR entry of A (via val_slot), FP16 x
     row scale, NaN where an entry has no slot."""
+    if len(P.get("blk_order", ())):
+        slot = P["val_slot"].astype(np.int64)
+        v = np.full(slot.shape, np.nan)
+        has = slot >= 0
+        v[has] = P["ent_val"].view(np.float16).astype(np.float64)[slot[has]]
+        v[has] *= P["row_scale"][P["edge_row"][has]]
+        return v
     T = len(P["tile_col"]) // 16
     slot = P["val_slot"].astype(np.int64)
     a = P["tile_a"].view(np.float16).astype(np.float64)

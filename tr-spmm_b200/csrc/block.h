@@ -1,0 +1,21 @@
+// Block engine launchers (block.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "plan.h"
+
+namespace trs {
+
+// K and B alignment the tensor-core block kernel takes (64 <= K <= 256,
+// K % 64 == 0, 16-byte aligned B); other shapes run the CUDA-core kernel.
+bool block_mma_supported(int32_t k, const void* b);
+// C = A_plan . B over a block plan, FP16 features; every output row written.
+int launch_block(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_dtype,
+                 bool force_generic, cudaStream_t stream);
+// The same with FP32 features (CUDA cores, FP32 arithmetic).
+int launch_block_f32(const tr_plan* p, const float* b, int32_t k, void* c, int c_dtype,
+                     cudaStream_t stream);
+
+}  // namespace trs

@@ -31,13 +31,6 @@
 
 namespace trs {
 
-struct Csr {
-  int32_t n_rows = 0, n_cols = 0;
-  std::vector<int32_t> ptr, idx;
-  std::vector<float> val;
-  std::vector<int32_t> src;      // entry of the caller's A behind each entry
-};
-
 int validate_csr(const int32_t* indptr, const int32_t* indices, int32_t n_rows, int32_t n_cols,
                  std::string& err) {
   if (n_rows < 0 || n_cols < 0) { err = "negative matrix shape"; return TR_ERR_ARG; }
@@ -258,7 +251,12 @@ int build_plan(const int32_t* indptr, const int32_t* indices, const float* value
                HostPlan& hp, std::string& err) {
   int rc = validate_csr(indptr, indices, n_rows, n_cols, err);
   if (rc) return rc;
-  if (params.window != 16) { err = "routed plans need window == 16"; return TR_ERR_UNSUPPORTED; }
+  if (opts.engine != TR_ENGINE_WINDOW && opts.engine != TR_ENGINE_BLOCK) {
+    err = "unknown plan engine " + std::to_string(opts.engine);
+    return TR_ERR_ARG;
+  }
+  const bool blocks = opts.engine == TR_ENGINE_BLOCK;
+  if (!blocks && params.window != 16) { err = "routed plans need window == 16"; return TR_ERR_UNSUPPORTED; }
   if (opts.promote_min < 0) { err = "promote_min must be >= 0"; return TR_ERR_ARG; }
   if (opts.demote_below < 0) { err = "demote_below must be >= 0"; return TR_ERR_ARG; }
   const int64_t nnz = indptr[n_rows];
@@ -302,6 +300,14 @@ int build_plan(const int32_t* indptr, const int32_t* indices, const float* value
     Csr p;
     permute_rows(a, perm, p);
     a = std::move(p);
+  }
+  if (blocks) {
+    rc = plan_blocks(a, opts.row_scale != 0, nnz, hp, err);
+    if (rc) return rc;
+    if (opts.reorder)
+      for (size_t r = 0; r < perm.size(); ++r) hp.row_out[r] = perm[r];
+    hp.reordered = opts.reorder != 0;
+    return TR_OK;
   }
   RouteTables T;
   // every 2:4 column would be demoted: form no 2:4 groups at all (the same

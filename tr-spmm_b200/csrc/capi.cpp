@@ -13,6 +13,7 @@
 
 #include "../../include/trspmm.h"
 #include "common.cuh"
+#include "block.h"
 #include "plan.h"
 #include "route_gpu.h"
 #include "router.h"
@@ -404,7 +405,8 @@ int tr_host_plan_array(const tr_host_plan* h, int idx, const void** data, int64_
     TRS_A(0, win_tile) TRS_A(1, win_split) TRS_A(2, win_prom) TRS_A(3, tile_col)
     TRS_A(4, tile_a) TRS_A(5, res_ptr) TRS_A(6, res_col) TRS_A(7, res_val) TRS_A(8, win_order)
     TRS_A(9, row_scale) TRS_A(10, row_out) TRS_A(11, val_slot) TRS_A(12, edge_row)
-    TRS_A(13, res_edge)
+    TRS_A(13, res_edge) TRS_A(14, blk_chunk) TRS_A(15, chunk_col) TRS_A(16, chunk_ent)
+    TRS_A(17, ent_pos) TRS_A(18, ent_val) TRS_A(19, ent_src) TRS_A(20, blk_order)
     default: return fail(TR_ERR_ARG, "plan array index out of range");
   }
 #undef TRS_A
@@ -445,6 +447,16 @@ int tr_spmm_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int 
   if (k < 0) return fail(TR_ERR_ARG, "negative K");
   if (c_dtype != TR_OUT_F32 && c_dtype != TR_OUT_F16) return fail(TR_ERR_ARG, "bad output dtype");
   if (p->view.n_rows > 0 && k > 0 && (!b || !c)) return fail(TR_ERR_ARG, "null device pointer");
+  if (p->blocked) {
+    if ((route_mask & TR_ROUTE_ALL) == 0) {
+      if (p->view.n_rows > 0 && k > 0)
+        TRS_CUDA(cudaMemsetAsync(c, 0, (size_t)p->view.n_rows * k * (c_dtype == TR_OUT_F16 ? 2 : 4),
+                                 (cudaStream_t)stream));
+      return TR_OK;
+    }
+    return launch_block(p, b, k, c, c_dtype, (route_mask & TR_ROUTE_PER_WINDOW) != 0,
+                        (cudaStream_t)stream);
+  }
   return launch_routed(p, b, k, c, c_dtype,
                        route_mask & (TR_ROUTE_ALL | TR_ROUTE_PER_WINDOW | TR_ROUTE_PIPELINED |
                                      TR_ROUTE_RESIDUAL_PASS),
@@ -457,6 +469,15 @@ int tr_spmm_routed_f32(const tr_plan* p, const float* b, int32_t k, void* c, int
   if (k < 0) return fail(TR_ERR_ARG, "negative K");
   if (c_dtype != TR_OUT_F32 && c_dtype != TR_OUT_F16) return fail(TR_ERR_ARG, "bad output dtype");
   if (p->view.n_rows > 0 && k > 0 && (!b || !c)) return fail(TR_ERR_ARG, "null device pointer");
+  if (p->blocked) {
+    if ((route_mask & TR_ROUTE_ALL) == 0) {
+      if (p->view.n_rows > 0 && k > 0)
+        TRS_CUDA(cudaMemsetAsync(c, 0, (size_t)p->view.n_rows * k * (c_dtype == TR_OUT_F16 ? 2 : 4),
+                                 (cudaStream_t)stream));
+      return TR_OK;
+    }
+    return launch_block_f32(p, b, k, c, c_dtype, (cudaStream_t)stream);
+  }
   return launch_routed_f32(p, b, k, c, c_dtype, route_mask & TR_ROUTE_ALL, (cudaStream_t)stream);
 }
 
@@ -487,6 +508,11 @@ int tr_adjoint_sddmm(const tr_plan* adj, const int32_t* a_indptr, const int32_t*
   if (a_rows != adj->view.n_cols) return fail(TR_ERR_ARG, "a_rows must equal the adjoint plan's column count");
   if (k > 0 && (!dc || !b || !db || (nnz > 0 && (!a_indptr || !a_indices || !dval))))
     return fail(TR_ERR_ARG, "null device pointer");
+  if (adj->blocked) {
+    int rc = launch_block(adj, dc, k, db, db_dtype, false, (cudaStream_t)stream);
+    if (rc) return rc;
+    return launch_sddmm(a_indptr, a_indices, a_rows, nnz, dc, b, k, dval, (cudaStream_t)stream);
+  }
   return launch_adjoint_sddmm(adj, a_indptr, a_indices, a_rows, nnz, dc, b, k, db, db_dtype, dval,
                               (cudaStream_t)stream);
 }
@@ -500,6 +526,11 @@ int tr_adjoint_sddmm_f32(const tr_plan* adj, const int32_t* a_indptr, const int3
   if (a_rows != adj->view.n_cols) return fail(TR_ERR_ARG, "a_rows must equal the adjoint plan's column count");
   if (k > 0 && (!dc || !b || !db || (nnz > 0 && (!a_indptr || !a_indices || !dval))))
     return fail(TR_ERR_ARG, "null device pointer");
+  if (adj->blocked) {
+    int rc = launch_block_f32(adj, dc, k, db, db_dtype, (cudaStream_t)stream);
+    if (rc) return rc;
+    return launch_sddmm_f32(a_indptr, a_indices, a_rows, nnz, dc, b, k, dval, (cudaStream_t)stream);
+  }
   return launch_adjoint_sddmm_f32(adj, a_indptr, a_indices, a_rows, nnz, dc, b, k, db, db_dtype,
                                   dval, (cudaStream_t)stream);
 }

@@ -645,6 +645,13 @@ int plan_upload(const HostPlan& hp, tr_plan** out) {
       {hp.edge_row.data(), n_edges * 4, 0},
       {hp.res_edge.data(), (int64_t)hp.res_edge.size() * 4, 0},
       {nullptr, 0, 256},                       // error words
+      {hp.blk_chunk.data(), (int64_t)hp.blk_chunk.size() * 4, 0},
+      {hp.chunk_col.data(), (int64_t)hp.chunk_col.size() * 4, 0},
+      {hp.chunk_ent.data(), (int64_t)hp.chunk_ent.size() * 4, 0},
+      {hp.ent_pos.data(), (int64_t)hp.ent_pos.size() * 2, 0},
+      {hp.ent_val.data(), (int64_t)hp.ent_val.size() * 2, 0},
+      {hp.ent_src.data(), (int64_t)hp.ent_src.size() * 4, 0},
+      {hp.blk_order.data(), (int64_t)hp.blk_order.size() * 4, 0},
   };
   constexpr int kSecs = sizeof(secs) / sizeof(secs[0]);
   int64_t total = 0;
@@ -666,7 +673,7 @@ int plan_upload(const HostPlan& hp, tr_plan** out) {
     if (e != cudaSuccess) break;
     off += secs[i].size;
   }
-  if (e == cudaSuccess) e = cudaMemset(at[kSecs - 1], 0, 256);
+  if (e == cudaSuccess) e = cudaMemset(at[14], 0, 256);
   if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) { cudaFree(p->block); delete p; return cuda_fail(e, "plan upload"); }
   PlanView& v = p->view;
@@ -686,13 +693,24 @@ int plan_upload(const HostPlan& hp, tr_plan** out) {
   v.row_out = (const int32_t*)at[10];
   v.res_edge = (const int32_t*)at[13];
   v.err = (int*)at[14];
-  p->tile_a = (uint16_t*)at[4];
+  v.n_blocks = hp.block ? (int32_t)hp.blk_order.size() : 0;
+  v.blk_chunk = (const int32_t*)at[15];
+  v.chunk_col = (const int32_t*)at[16];
+  v.chunk_ent = (const int32_t*)at[17];
+  v.ent_pos = (const uint16_t*)at[18];
+  v.ent_val = (const uint16_t*)at[19];
+  v.ent_src = (const int32_t*)at[20];
+  v.blk_order = (const int32_t*)at[21];
+  p->blocked = hp.block;
+  // re-valuing writes tile values below n_tile_vals: the block layout's
+  // values take that place
+  p->tile_a = hp.block ? (uint16_t*)at[19] : (uint16_t*)at[4];
   p->res_val = (uint16_t*)at[7];
   p->row_scale = (float*)at[9];
   p->val_slot = (int32_t*)at[11];
   p->edge_row = (int32_t*)at[12];
   p->n_edges = n_edges;
-  p->n_tile_vals = T * 256;
+  p->n_tile_vals = hp.block ? (int64_t)hp.ent_val.size() : T * 256;
   p->row_scaled = hp.row_scaled;
   p->info.n_rows = hp.n_rows;
   p->info.n_cols = hp.n_cols;
@@ -705,6 +723,10 @@ int plan_upload(const HostPlan& hp, tr_plan** out) {
   p->info.promoted_tiles = hp.prom_tiles;
   p->info.row_scaled = hp.row_scaled ? 1 : 0;
   p->info.reordered = hp.reordered ? 1 : 0;
+  p->info.engine = hp.block ? TR_ENGINE_BLOCK : TR_ENGINE_WINDOW;
+  p->info.n_blocks = v.n_blocks;
+  p->info.chunks = hp.block ? (int64_t)hp.blk_chunk.back() : 0;
+  if (hp.block) p->info.residual_nnz = 0;
   *out = p;
   return TR_OK;
 }

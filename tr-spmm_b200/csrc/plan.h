@@ -25,6 +25,23 @@
 //                    the entry is not multiplied (compat-mode truncation)
 //   edge_row[E]      plan row of each CSR entry (row scale of learnable values)
 //   err[4]           device error flags (bounded-wait timeouts)
+//
+// Block layout (the block engine, opts.engine == TR_ENGINE_BLOCK): the plan's
+// rows in blocks of 128 (eight windows); every distinct column a block
+// touches is one K slot of a 16-column chunk, so each feature row of B is
+// gathered once per block and multiplied by the tensor cores against all 128
+// rows at once (tcgen05.mma M = 128 rows, N = K features, K = 16 slots):
+//   blk_chunk[NB+1]  chunks of block b: [blk_chunk[b], blk_chunk[b+1])
+//   chunk_col[NC*16] row of B gathered into each slot of a chunk (-1: none)
+//   chunk_ent[NC+1]  entries of chunk c: [chunk_ent[c], chunk_ent[c+1])
+//   ent_pos[E]       byte offset of the entry in the chunk's 128x16 FP16 A
+//                    tile (tcgen05 K-major, no swizzle: row m, slot k at
+//                    (m/8)*256 + (k/8)*128 + (m%8)*16 + (k%8)*2)
+//   ent_val[E]       FP16 value (FP16(v / row_scale) when row-scaled)
+//   ent_src[E]       CSR entry of the caller's A behind the entry
+//   blk_order[NB]    blocks in decreasing chunk count (launch order)
+// row_scale / row_out cover NB*128 rows (n_windows = NB*8); the window
+// sections are empty, and val_slot indexes ent_val.
 #pragma once
 #include <cstdint>
 #include <string>
@@ -49,6 +66,15 @@ struct PlanView {
   const float* row_scale;
   const int32_t* row_out;
   int* err;
+  // block layout (n_blocks == 0 for window plans)
+  int32_t n_blocks;
+  const int32_t* blk_chunk;
+  const int32_t* chunk_col;
+  const int32_t* chunk_ent;
+  const uint16_t* ent_pos;
+  const uint16_t* ent_val;
+  const int32_t* ent_src;
+  const int32_t* blk_order;
 };
 
 struct HostPlan {
@@ -64,6 +90,23 @@ struct HostPlan {
   std::vector<int32_t> val_slot, edge_row;
   bool row_scaled = false, reordered = false;
   int64_t tc_tiles = 0, sptc_tiles = 0, prom_tiles = 0, nnz = 0;
+  // block layout
+  bool block = false;
+  std::vector<int32_t> blk_chunk, chunk_col, chunk_ent, ent_src, blk_order;
+  std::vector<uint16_t> ent_pos, ent_val;
+};
+
+// Rows per block of the block layout and K slots per chunk.
+constexpr int kBlkRows = 128;
+constexpr int kChunkCols = 16;
+
+// A CSR matrix on its way through the builder; src[e] is the entry of the
+// caller's A behind entry e.
+struct Csr {
+  int32_t n_rows = 0, n_cols = 0;
+  std::vector<int32_t> ptr, idx;
+  std::vector<float> val;
+  std::vector<int32_t> src;
 };
 
 }  // namespace trs
@@ -81,6 +124,7 @@ struct tr_plan {
   uint16_t* res_val = nullptr;
   int64_t n_tile_vals = 0;      // T*256
   bool row_scaled = false;
+  bool blocked = false;         // block layout (the block engine)
   tr_plan_info info{};
 };
 
@@ -111,6 +155,10 @@ int plan_from_groups(const int32_t* s_column, const float* s_value, const int8_t
                      int64_t n_offsets, int32_t window, int32_t n_rows, int32_t n_cols,
                      HostPlan& hp, std::string& err);
 int plan_upload(const HostPlan& hp, tr_plan** out);
+// Block layout of a (transposed / reordered) CSR: fills hp's block arrays,
+// row_scale / row_out (identity; the caller maps reordered rows), val_slot /
+// edge_row over n_edges entries of the caller's A.
+int plan_blocks(const Csr& a, bool row_scale, int64_t n_edges, HostPlan& hp, std::string& err);
 // Native builder (builder.cpp): validate, transpose / reorder as asked, route, lay out.
 int validate_csr(const int32_t* indptr, const int32_t* indices, int32_t n_rows, int32_t n_cols,
                  std::string& err);

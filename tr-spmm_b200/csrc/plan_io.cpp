@@ -5,6 +5,9 @@
 // Format (little-endian): the 8-byte tag "TRSPLAN1", a u32 version, the
 // scalar fields, then each array as (u64 element count, raw elements) in a
 // fixed order, then a 64-bit FNV-1a checksum of every preceding byte.
+// Version 2 adds a block-layout flag after the scalar flags and the seven
+// block arrays after the window arrays; version-1 files (window plans) still
+// load.
 // Loading checks the tag, the version, every count against the bytes left
 // and the checksum, and refuses the file (with the reason) on any mismatch.
 #include <cstdint>
@@ -20,7 +23,7 @@ namespace trs {
 namespace {
 
 constexpr char kTag[8] = {'T', 'R', 'S', 'P', 'L', 'A', 'N', '1'};
-constexpr uint32_t kVersion = 1;
+constexpr uint32_t kVersion = 2;
 
 struct Fnv {
   uint64_t h = 1469598103934665603ull;
@@ -99,10 +102,40 @@ bool contents_valid(const HostPlan& h) {
   const int64_t slots = T * 256 + (int64_t)h.res_col.size();
   for (int32_t e : h.res_edge)
     if (e < -1 || e >= n_edges) return false;
+  const int64_t ents = (int64_t)h.ent_pos.size();
   for (int64_t e = 0; e < n_edges; ++e)
-    if (h.val_slot[e] < -1 || h.val_slot[e] >= slots || h.edge_row[e] < -1 ||
+    if (h.val_slot[e] < -1 || h.val_slot[e] >= (h.block ? ents : slots) || h.edge_row[e] < -1 ||
         h.edge_row[e] >= rows)
       return false;
+  if (!h.block)
+    return h.blk_chunk.empty() && h.chunk_col.empty() && h.chunk_ent.empty() && ents == 0 &&
+           h.ent_val.empty() && h.ent_src.empty() && h.blk_order.empty();
+  // block layout: every offset monotone and in range, every position inside
+  // a 128x16 FP16 tile, the launch order a permutation of the blocks
+  const int64_t NB = (int64_t)h.blk_order.size();
+  if (T != 0 || !h.res_col.empty() || W != NB * 8 || (int64_t)h.blk_chunk.size() != NB + 1 ||
+      h.blk_chunk[0] != 0)
+    return false;
+  for (int64_t b = 0; b < NB; ++b)
+    if (h.blk_chunk[b] > h.blk_chunk[b + 1]) return false;
+  const int64_t NC = h.blk_chunk[NB];
+  if ((int64_t)h.chunk_col.size() != NC * kChunkCols || (int64_t)h.chunk_ent.size() != NC + 1 ||
+      h.chunk_ent[0] != 0 || h.chunk_ent[NC] != ents || (int64_t)h.ent_val.size() != ents ||
+      (int64_t)h.ent_src.size() != ents)
+    return false;
+  for (int64_t c = 0; c < NC; ++c)
+    if (h.chunk_ent[c] > h.chunk_ent[c + 1]) return false;
+  for (int32_t c : h.chunk_col)
+    if (c < -1 || c >= h.n_cols) return false;
+  for (uint16_t p : h.ent_pos)
+    if ((p & 1) || p >= 4096) return false;
+  for (int32_t e : h.ent_src)
+    if (e < -1 || e >= n_edges) return false;
+  std::vector<char> bseen(NB, 0);
+  for (int32_t b : h.blk_order) {
+    if (b < 0 || b >= NB || bseen[b]) return false;
+    bseen[b] = 1;
+  }
   return true;
 }
 
@@ -117,6 +150,7 @@ int save_host_plan(const HostPlan& hp, const char* path, std::string& err) {
   w.put<int32_t>(hp.n_windows);
   w.put<uint8_t>(hp.row_scaled ? 1 : 0);
   w.put<uint8_t>(hp.reordered ? 1 : 0);
+  w.put<uint8_t>(hp.block ? 1 : 0);
   w.put<int64_t>(hp.tc_tiles);
   w.put<int64_t>(hp.sptc_tiles);
   w.put<int64_t>(hp.prom_tiles);
@@ -135,6 +169,13 @@ int save_host_plan(const HostPlan& hp, const char* path, std::string& err) {
   w.vec(hp.row_out);
   w.vec(hp.val_slot);
   w.vec(hp.edge_row);
+  w.vec(hp.blk_chunk);
+  w.vec(hp.chunk_col);
+  w.vec(hp.chunk_ent);
+  w.vec(hp.ent_pos);
+  w.vec(hp.ent_val);
+  w.vec(hp.ent_src);
+  w.vec(hp.blk_order);
   Fnv f;
   f.add(w.buf.data(), w.buf.size());
   w.put<uint64_t>(f.h);
@@ -184,7 +225,7 @@ int load_host_plan(const char* path, HostPlan& hp, std::string& err) {
   }
   Reader r{buf.data() + sizeof(kTag), buf.size() - sizeof(kTag) - 8};
   const uint32_t version = r.get<uint32_t>();
-  if (version != kVersion) {
+  if (version != kVersion && version != 1) {
     err = "plan file version " + std::to_string(version) + " (this library reads version " +
           std::to_string(kVersion) + ")";
     return TR_ERR_UNSUPPORTED;
@@ -195,6 +236,7 @@ int load_host_plan(const char* path, HostPlan& hp, std::string& err) {
   h.n_windows = r.get<int32_t>();
   h.row_scaled = r.get<uint8_t>() != 0;
   h.reordered = r.get<uint8_t>() != 0;
+  if (version >= 2) h.block = r.get<uint8_t>() != 0;
   h.tc_tiles = r.get<int64_t>();
   h.sptc_tiles = r.get<int64_t>();
   h.prom_tiles = r.get<int64_t>();
@@ -213,6 +255,15 @@ int load_host_plan(const char* path, HostPlan& hp, std::string& err) {
   r.vec(h.row_out);
   r.vec(h.val_slot);
   r.vec(h.edge_row);
+  if (version >= 2) {
+    r.vec(h.blk_chunk);
+    r.vec(h.chunk_col);
+    r.vec(h.chunk_ent);
+    r.vec(h.ent_pos);
+    r.vec(h.ent_val);
+    r.vec(h.ent_src);
+    r.vec(h.blk_order);
+  }
   const int64_t W = h.n_windows;
   const bool shapes = r.ok && r.left == 0 && W >= 0 && h.win_tile.size() == (size_t)W + 1 &&
                       h.win_split.size() == (size_t)W && h.win_prom.size() == (size_t)W &&

@@ -72,16 +72,19 @@ class PlanInfo(ctypes.Structure):
                 ("tc_tiles", ctypes.c_int64), ("sptc_tiles", ctypes.c_int64),
                 ("residual_nnz", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
                 ("promoted_tiles", ctypes.c_int64), ("row_scaled", ctypes.c_int32),
-                ("reordered", ctypes.c_int32)]
+                ("reordered", ctypes.c_int32), ("engine", ctypes.c_int32),
+                ("n_blocks", ctypes.c_int32), ("chunks", ctypes.c_int64)]
 
 
 class PlanOpts(ctypes.Structure):
     _fields_ = [("row_scale", ctypes.c_int32), ("promote_min", ctypes.c_int32),
                 ("transpose", ctypes.c_int32), ("reorder", ctypes.c_int32),
-                ("demote_below", ctypes.c_int32), ("row_order", ctypes.c_void_p)]
+                ("demote_below", ctypes.c_int32), ("row_order", ctypes.c_void_p),
+                ("engine", ctypes.c_int32)]
 
 
 TR_REORDER_NONE, TR_REORDER_LABEL, TR_REORDER_TCA, TR_REORDER_GIVEN = 0, 1, 2, 3
+TR_ENGINE_WINDOW, TR_ENGINE_BLOCK = 0, 1
 
 
 class TcaParams(ctypes.Structure):

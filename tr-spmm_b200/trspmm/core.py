@@ -21,6 +21,7 @@ import numpy as np
 from . import _lib
 from ._lib import (TR_MATCH_BUCKET, TR_MATCH_HASH, TR_MATCH_ONLINE, TR_MATCH_SLIDING, TR_OUT_F16,
                    TR_OUT_F32,
+                   TR_ENGINE_BLOCK, TR_ENGINE_WINDOW,
                    TR_REORDER_GIVEN, TR_REORDER_LABEL, TR_REORDER_NONE, TR_REORDER_TCA,
                    TR_ROUTE_ALL, TR_ROUTE_COMPAT, TR_ROUTE_EXACT, MatchStats, PlanInfo, PlanOpts,
                    RouteParams, Tables, TcaParams, TcaStats, check, lib)
@@ -49,12 +50,19 @@ REORDER_MODES = {False: TR_REORDER_NONE, None: TR_REORDER_NONE, "none": TR_REORD
                  True: TR_REORDER_LABEL, "label": TR_REORDER_LABEL, "tca": TR_REORDER_TCA}
 
 
-def plan_opts(row_scale=False, promote_min=0, transpose=False, reorder=False, demote_below=0):
+ENGINES = {"window": TR_ENGINE_WINDOW, "block": TR_ENGINE_BLOCK}
+
+
+def plan_opts(row_scale=False, promote_min=0, transpose=False, reorder=False, demote_below=0,
+              engine="window"):
     """(tr_plan_opts, keep-alive array).  ``reorder``: False / "none", True /
     "label" (label propagation), "tca" (TCA clustering, tr_tca_order's
     defaults) or an int array, the caller's row permutation (plan row i is row
     reorder[i] of the matrix the plan is built for: A, or A^T when
-    transpose)."""
+    transpose).  ``engine``: "window" (the three routes over 16-row windows)
+    or "block" (every entry on the tensor cores over 128-row blocks)."""
+    if engine not in ENGINES:
+        raise ValueError(f"unknown plan engine {engine!r}")
     order = None
     if isinstance(reorder, (str, bool)) or reorder is None:
         if reorder not in REORDER_MODES:
@@ -64,7 +72,8 @@ def plan_opts(row_scale=False, promote_min=0, transpose=False, reorder=False, de
         order = np.ascontiguousarray(reorder, dtype=np.int32)
         mode = TR_REORDER_GIVEN
     opts = PlanOpts(int(bool(row_scale)), int(promote_min), int(bool(transpose)), int(mode),
-                    int(demote_below), _vp(order) if order is not None else ctypes.c_void_p(0))
+                    int(demote_below), _vp(order) if order is not None else ctypes.c_void_p(0),
+                    ENGINES[engine])
     return opts, order
 
 
@@ -245,15 +254,17 @@ class Plan:
 
     @classmethod
     def build(cls, indptr, indices, values, n_rows, n_cols, row_scale=False, promote_min=0,
-              transpose=False, reorder=False, demote_below=0, mode="exact", **route_kw):
+              transpose=False, reorder=False, demote_below=0, mode="exact", engine="window",
+              **route_kw):
         """Native builder (tr_plan_build): route A (or A^T when transpose) and
         lay it out; the plan keeps, for every CSR entry of A, where its value
-        lives (set_values).  For a transposed plan n_rows/n_cols are A's."""
+        lives (set_values).  For a transposed plan n_rows/n_cols are A's.
+        ``engine="block"`` lays the matrix out for the block engine."""
         rp = np.ascontiguousarray(indptr, dtype=np.int32)
         ci = np.ascontiguousarray(indices, dtype=np.int32)
         vv = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
         prm = _params(mode=mode, **route_kw)
-        opts, keep = plan_opts(row_scale, promote_min, transpose, reorder, demote_below)
+        opts, keep = plan_opts(row_scale, promote_min, transpose, reorder, demote_below, engine)
         h = ctypes.c_void_p()
         check(lib().tr_plan_build(_vp(rp), _vp(ci), _vp(vv), int(n_rows), int(n_cols),
                                   ctypes.byref(prm), ctypes.byref(opts), ctypes.byref(h)))
@@ -375,18 +386,21 @@ HOST_PLAN_ARRAYS = [("win_tile", np.int32), ("win_split", np.int32), ("win_prom"
                     ("tile_col", np.int32), ("tile_a", np.uint16), ("res_ptr", np.int32),
                     ("res_col", np.int32), ("res_val", np.uint16), ("win_order", np.int32),
                     ("row_scale", np.float32), ("row_out", np.int32), ("val_slot", np.int32),
-                    ("edge_row", np.int32), ("res_edge", np.int32)]
+                    ("edge_row", np.int32), ("res_edge", np.int32), ("blk_chunk", np.int32),
+                    ("chunk_col", np.int32), ("chunk_ent", np.int32), ("ent_pos", np.uint16),
+                    ("ent_val", np.uint16), ("ent_src", np.int32), ("blk_order", np.int32)]
 
 
 def host_plan(indptr, indices, values, n_rows, n_cols, row_scale=False, promote_min=0,
-              transpose=False, reorder=False, demote_below=0, mode="exact", **route_kw):
+              transpose=False, reorder=False, demote_below=0, mode="exact", engine="window",
+              **route_kw):
     """The native builder's plan as host arrays (tr_plan_build_host), without
     a device: a dict name -> numpy array (layout in csrc/plan.h)."""
     rp = np.ascontiguousarray(indptr, dtype=np.int32)
     ci = np.ascontiguousarray(indices, dtype=np.int32)
     vv = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
     prm = _params(mode=mode, **route_kw)
-    opts, keep = plan_opts(row_scale, promote_min, transpose, reorder, demote_below)
+    opts, keep = plan_opts(row_scale, promote_min, transpose, reorder, demote_below, engine)
     L = lib()
     h = ctypes.c_void_p()
     check(L.tr_plan_build_host(_vp(rp), _vp(ci), _vp(vv), int(n_rows), int(n_cols),

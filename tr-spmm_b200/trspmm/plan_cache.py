@@ -33,7 +33,7 @@ def default_dir():
 
 
 def _options(row_scale=False, promote_min=0, transpose=False, reorder=False, demote_below=0,
-             mode="exact", **route_kw):
+             mode="exact", engine="window", **route_kw):
     if not (isinstance(reorder, (str, bool)) or reorder is None):
         raise ValueError("the plan cache takes named reorder modes (False, True / 'label', 'tca')")
     if reorder not in core.REORDER_MODES:
@@ -43,6 +43,10 @@ def _options(row_scale=False, promote_min=0, transpose=False, reorder=False, dem
     opts = {"row_scale": bool(row_scale), "promote_min": int(promote_min),
             "transpose": bool(transpose), "reorder": reorder,
             "demote_below": int(demote_below), "mode": mode}
+    if engine != "window":              # keys of window plans stay as they were
+        if engine not in core.ENGINES:
+            raise ValueError(f"unknown plan engine {engine!r}")
+        opts["engine"] = engine
     return opts, route_kw
 
 
@@ -70,7 +74,7 @@ def _build_host(indptr, indices, values, n_rows, n_cols, **plan_kw):
     vv = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
     prm = core._params(mode=opts["mode"], **route_kw)
     po, _ = core.plan_opts(opts["row_scale"], opts["promote_min"], opts["transpose"],
-                           opts["reorder"], opts["demote_below"])
+                           opts["reorder"], opts["demote_below"], opts.get("engine", "window"))
     h = ctypes.c_void_p()
     check(lib().tr_plan_build_host(core._vp(rp), core._vp(ci), core._vp(vv), int(n_rows),
                                    int(n_cols), ctypes.byref(prm), ctypes.byref(po),
