@@ -9,25 +9,37 @@
 // is written once, by one thread, in a fixed summation order: results are
 // bitwise repeatable and no atomics are involved.
 //
-// One persistent CTA per SM walks its share of the blocks (round robin over
-// the plan's cost order) as one continuous stream of chunks:
+// One persistent CTA per SM takes its blocks from the plan's schedule
+// (longest-processing-time assignment made at upload) as one stream of
+// chunks.  Every block holds a whole number of groups of four chunks (the
+// layout pads it with chunks that have no entries); the four stage slots of
+// a group share one full and one empty barrier.  Roles:
 //
-//   producer warps 4-7 (chunk q taken by warp 4 + q % 4)
-//       wait until the chunk's stage slot is free (empty barrier), clear the
-//       entries the slot's previous chunk wrote into its A tile, write this
-//       chunk's FP16 values at their packed byte offsets (the tile is zero
-//       elsewhere), and gather the 16 feature rows with 16-byte cp.async
-//       copies straight into the 128-byte-swizzled MN-major operand layout
-//       (absent slots zero-filled).  Each warp keeps up to four chunks of
-//       copies in flight (cp.async groups); once a chunk's group completed it
-//       fences its shared-memory writes for the async proxy and arrives on
-//       the chunk's full barrier;
-//   MMA warp 8 (one elected thread)
-//       per chunk: wait full, one tcgen05.mma (M = 128, N = K, K = 16) into
-//       the block's accumulator, commit to the slot's empty barrier; after a
-//       block's last chunk commit to the accumulator's full barrier; two TMEM
-//       accumulators alternate so a block's MMAs overlap the previous
-//       block's epilogue;
+//   producer warps (kProd of them, two stage slots each; chunk q of the
+//   stream taken by warp q % kProd)
+//       per chunk: wait until the slot is free, clear from its A tile the
+//       positions the slot's previous chunk set and write this chunk's
+//       values (packed entries value << 16 | tile byte offset, loaded into
+//       registers two chunks ahead), issue the 16-byte cp.async copies of
+//       the chunk's 16 feature rows straight into the 128-byte-swizzled
+//       MN-major operand layout (absent slots zero-filled) and arrive on
+//       the group's full barrier: each lane's copies arrive by themselves
+//       when they land (cp.async.mbarrier.arrive.noinc), the warp once for
+//       the A tile.  A producer never waits for its own copies.  Column
+//       lists and entry ranges come from a per-warp ring in shared memory
+//       filled eight chunks ahead.  Many producer warps keep enough gathers in
+//       flight: a warp's cp.async issue, not the memory system, sets the rate
+//       of one warp;
+//   MMA warp (one elected thread)
+//       per group: wait full, one proxy fence (the operands were written
+//       through the generic proxy; the tensor core reads them through the
+//       async proxy), four tcgen05.mma (M = 128, N = K, K = 16) into the
+//       block's accumulator, one commit to the group's empty barrier; after
+//       a block's last group a commit to the accumulator's full barrier.
+//       The loop is straight-line per group (stage descriptors are base +
+//       stage * stride): the issuing thread's own instruction latency would
+//       otherwise set the MMA rate.  Two TMEM accumulators alternate, so a
+//       block's MMAs overlap the previous block's epilogue;
 //   epilogue warps 0-3 (thread t <-> block row t <-> TMEM lane t)
 //       wait for the accumulator, tcgen05.ld the row's K values 32 at a
 //       time, apply the row scale and store the row to its output position
@@ -43,6 +55,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <type_traits>
 
 #include "block.h"
 #include "common.cuh"
@@ -51,37 +64,44 @@
 namespace trs {
 namespace {
 
-constexpr int kStages = 16;             // chunk stage slots in shared memory
-constexpr int kProdWarps = 4;
-constexpr int kDepth = 3;               // copy groups a producer retires late
+constexpr int kGroup = kChunkGroup;     // chunks per barrier group
 constexpr int kEpiWarps = 4;
-constexpr int kProdWarp0 = kEpiWarps;   // warps 4..7
-constexpr int kMmaWarp = kProdWarp0 + kProdWarps;  // warp 8
-constexpr int kBlkThreads = (kMmaWarp + 1) * 32;
+constexpr int kProdWarp0 = kEpiWarps;
 constexpr int kATile = 4096;            // 128 rows x 16 slots, FP16
-static_assert(kStages % kProdWarps == 0, "a stage slot always returns to the same producer warp");
-static_assert(kDepth < kStages / kProdWarps, "a chunk is released before its slot is reused");
+constexpr int kEntReg = 2;              // entry words per lane held in registers
+constexpr int kMaxBlk = 512;            // blocks per CTA (staged list)
+constexpr int kMetaRing = 8;            // chunks of metadata staged ahead, per warp
+// copy groups a producer leaves in flight: its range of chunk n + 2 was
+// copied kMetaRing chunks back, so waiting for all but the newest
+// kMetaRing - 3 groups suffices and never waits for recent gathers
+constexpr int kMetaWait = kMetaRing - 3;
+constexpr int kMetaInts = 18;           // a chunk's 16 columns and entry range
+constexpr uint32_t kNoEntry = 0xFFFFFFFFu;   // empty register slot (offset past the tile)
 
 template <int NA>
 struct BlkCfg {
   static constexpr int kN = 64 * NA;               // features = MMA N
   static constexpr int kBTile = 2048 * NA;         // 16 slots x kN features, FP16
   static constexpr int kStage = kBTile + kATile;   // a multiple of 1024
+  // as many stage slots as shared memory holds; two per producer warp
+  static constexpr int kStages = NA == 1 ? 32 : (NA == 2 ? 24 : (NA == 3 ? 20 : 16));
+  static constexpr int kProd = kStages / 2;
+  static constexpr int kGroups = kStages / kGroup;
+  static constexpr int kMmaWarp = kProdWarp0 + kProd;
+  static constexpr int kThreads = (kMmaWarp + 1) * 32;
   static constexpr int kBarOff = kStages * kStage;
-  // full[S], empty[S], acc_full[2], acc_empty[2], done; then tmem slot, abort flag
-  static constexpr int kSmem = 1024 + kBarOff + (2 * kStages + 5) * 8 + 16;
+  // full[G], empty[G], acc_full[2], acc_empty[2], done; tmem slot, abort flag
+  static constexpr int kBlkOff = kBarOff + (2 * kGroups + 5) * 8 + 16;
+  static constexpr int kMetaOff = kBlkOff + 3 * kMaxBlk * 4;
+  static constexpr int kSmem = 1024 + kMetaOff + kProd * kMetaRing * kMetaInts * 4;
   static constexpr uint32_t kTmemCols = 2 * kN <= 128 ? 128 : (2 * kN <= 256 ? 256 : 512);
+  // arrivals that complete a group: 32 lanes and one warp arrival per chunk
+  static constexpr uint32_t kFullCount = kGroup * 33;
+  static_assert(kStages % kGroup == 0 && kGroups >= 2, "whole groups of stage slots");
   static_assert(kStage % 1024 == 0, "B tiles keep the 1024-byte swizzle alignment");
   static_assert(kSmem <= 227 * 1024, "shared memory budget");
+  static_assert(kThreads <= 1024, "one CTA");
 };
-
-int sm_count() {
-  int dev = 0, sms = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
-    return 0;
-  return sms;
-}
 
 __device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, volatile int* abort) {
   if (mbar_try_wait(bar, parity)) return true;
@@ -120,6 +140,23 @@ __device__ __forceinline__ void tmem_ld_x32(uint32_t taddr, float (&v)[32]) {
 __device__ __forceinline__ void sts_u16(uint32_t addr, uint16_t v) {
   asm volatile("st.shared.u16 [%0], %1;\n" ::"r"(addr), "h"(v) : "memory");
 }
+__device__ __forceinline__ uint32_t lds_u32(uint32_t addr) {
+  uint32_t v;
+  asm volatile("ld.shared.u32 %0, [%1];\n" : "=r"(v) : "r"(addr) : "memory");
+  return v;
+}
+// 4-byte global->shared copy (cp.async, L1-allocating form)
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(src) : "memory");
+}
+// The i-th element of a register ring, i known only at run time.
+template <int N>
+__device__ __forceinline__ int ring_at(const int (&r)[N], int i) {
+  int v = 0;
+#pragma unroll
+  for (int t = 0; t < N; ++t) v = t == i ? r[t] : v;
+  return v;
+}
 
 // 32 consecutive features of one output row, scaled.
 template <bool F16OUT>
@@ -154,34 +191,64 @@ __device__ __forceinline__ void store_zero32(void* C, int64_t at) {
   }
 }
 
+// Arrive on `bar` once all of this thread's earlier cp.async copies have
+// landed; the arrival is counted in the barrier's expected count.
+__device__ __forceinline__ void cp_async_arrive_noinc(uint32_t bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(bar) : "memory");
+}
+
+// Position in this CTA's chunk stream: chunk id of stream index q (q only
+// grows), walking the staged block list.
+struct StreamCursor {
+  const int* c0;
+  const int* c1;
+  int nblk, i = 0, q0 = 0;
+  __device__ int chunk(int q) {
+    while (i < nblk - 1 && q >= q0 + (c1[i] - c0[i])) {
+      q0 += c1[i] - c0[i];
+      ++i;
+    }
+    return c0[i] + (q - q0);
+  }
+};
+
+__device__ __forceinline__ uint32_t ld_stream_u32(const uint32_t* p, uint64_t policy) {
+  uint32_t v;
+  asm volatile("ld.global.nc.L2::cache_hint.b32 %0, [%1], %2;\n" : "=r"(v) : "l"(p), "l"(policy));
+  return v;
+}
+
 template <bool F16OUT, int NA>
-__global__ void __launch_bounds__(kBlkThreads, 1)
+__global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
     block_mma_kernel(PlanView pv, const __half* __restrict__ B, void* C) {
   using Cfg = BlkCfg<NA>;
-  constexpr int K = Cfg::kN;
+  constexpr int K = Cfg::kN, S = Cfg::kStages, NG = Cfg::kGroups, P = Cfg::kProd;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::kBarOff);
   uint64_t* full = bars;
-  uint64_t* empty = bars + kStages;
-  uint64_t* acc_full = bars + 2 * kStages;
+  uint64_t* empty = bars + NG;
+  uint64_t* acc_full = bars + 2 * NG;
   uint64_t* acc_empty = acc_full + 2;
   uint64_t* done = acc_empty + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+  int* s_b = reinterpret_cast<int*>(smem + Cfg::kBlkOff);
+  int* s_c0 = s_b + kMaxBlk;
+  int* s_c1 = s_c0 + kMaxBlk;
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int NB = pv.n_blocks;
-  const int nblk = NB > (int)blockIdx.x ? (NB - (int)blockIdx.x + (int)gridDim.x - 1) / (int)gridDim.x : 0;
+  const int bfirst = __ldg(pv.cta_ptr + blockIdx.x);
+  const int nblk = __ldg(pv.cta_ptr + blockIdx.x + 1) - bfirst;
 
-  if (warp == kMmaWarp) {
+  if (warp == Cfg::kMmaWarp) {
     tmem_alloc(smem_u32(tmem_slot), Cfg::kTmemCols);
     tmem_relinquish();
   }
   if (tid == 0) {
-    for (int s = 0; s < kStages; ++s) {
-      mbar_init(smem_u32(&full[s]), 1);
-      mbar_init(smem_u32(&empty[s]), 1);
+    for (int g = 0; g < NG; ++g) {
+      mbar_init(smem_u32(&full[g]), Cfg::kFullCount);
+      mbar_init(smem_u32(&empty[g]), 1);
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(smem_u32(&acc_full[a]), 1);
@@ -191,105 +258,164 @@ __global__ void __launch_bounds__(kBlkThreads, 1)
     *abort_flag = 0;
     fence_mbar_init();
   }
+  // this CTA's blocks, staged once
+  for (int i = tid; i < nblk; i += Cfg::kThreads) {
+    const int b = __ldg(pv.cta_blk + bfirst + i);
+    s_b[i] = b;
+    s_c0[i] = __ldg(pv.blk_chunk + b);
+    s_c1[i] = __ldg(pv.blk_chunk + b + 1);
+  }
   // A tiles start as zeros (a chunk writes its entries, and clears them
   // again before the slot takes the next chunk); B tiles start as zeros so
   // that no stale bit pattern meets a zero of A as Inf or NaN
-  for (int s = 0; s < kStages; ++s) {
-    uint4* st = reinterpret_cast<uint4*>(smem + s * Cfg::kStage);
-    for (int i = tid; i < Cfg::kStage / 16; i += kBlkThreads) st[i] = make_uint4(0, 0, 0, 0);
-  }
+  for (int i = tid; i < S * Cfg::kStage / 16; i += Cfg::kThreads)
+    reinterpret_cast<uint4*>(smem)[i] = make_uint4(0, 0, 0, 0);
   fence_proxy_async_smem();
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp >= kProdWarp0 && warp < kMmaWarp) {
+  if (warp >= kProdWarp0 && warp < Cfg::kMmaWarp) {
     // ------------------------------------------------------------ producers
     const int p = warp - kProdWarp0;
     const uint64_t pol_keep = l2_policy_evict_last(), pol_stream = l2_policy_evict_first();
-    int prev0[kStages / kProdWarps], prev1[kStages / kProdWarps];   // entries of this warp's
-#pragma unroll                                                     // last chunks, oldest first
-    for (int i = 0; i < kStages / kProdWarps; ++i) prev0[i] = prev1[i] = 0;
-    int n = 0, q = 0;
-    bool ok = true;
-    for (int i = 0; i < nblk && ok; ++i) {
-      const int b = __ldg(pv.blk_order + blockIdx.x + i * gridDim.x);
-      const int c0 = __ldg(pv.blk_chunk + b), nc = __ldg(pv.blk_chunk + b + 1) - c0;
-      for (int j = ((p - q) % kProdWarps + kProdWarps) % kProdWarps; j < nc; j += kProdWarps, ++n) {
-        const int chunk = c0 + j, gq = q + j;          // gq == kProdWarps * n + p
-        const int s = gq % kStages, use = gq / kStages;
-        const int my_col = lane < kChunkCols ? __ldg(pv.chunk_col + (int64_t)chunk * kChunkCols + lane) : -1;
-        const int e0 = __ldg(pv.chunk_ent + chunk), e1 = __ldg(pv.chunk_ent + chunk + 1);
-        if (!wait_bar(smem_u32(&empty[s]), (use & 1) ^ 1, abort_flag)) { ok = false; break; }
-        uint8_t* st = smem + s * Cfg::kStage;
-        const uint32_t a_tile = smem_u32(st + Cfg::kBTile);
-        // clear the slot's previous chunk, then write this one
-        for (int e = prev0[0] + lane; e < prev1[0]; e += 32)
-          sts_u16(a_tile + ld_stream_u16(pv.ent_pos + e, pol_stream), 0);
-        __syncwarp();
-        for (int e = e0 + lane; e < e1; e += 32)
-          sts_u16(a_tile + ld_stream_u16(pv.ent_pos + e, pol_stream),
-                  ld_stream_u16(pv.ent_val + e, pol_stream));
+    int total = 0;
+    for (int i = lane; i < nblk; i += 32) total += s_c1[i] - s_c0[i];
 #pragma unroll
-        for (int t = 0; t + 1 < kStages / kProdWarps; ++t) {
-          prev0[t] = prev0[t + 1];
-          prev1[t] = prev1[t + 1];
-        }
-        prev0[kStages / kProdWarps - 1] = e0;
-        prev1[kStages / kProdWarps - 1] = e1;
-        // gather: 16 rows x (8 * NA) 16-byte segments, 4 * NA per lane
-        const uint32_t b_tile = smem_u32(st);
+    for (int o = 16; o > 0; o >>= 1) total += __shfl_xor_sync(0xffffffffu, total, o);
+    const int nloc = total > p ? (total - p + P - 1) / P : 0;
+    StreamCursor cur{s_c0, s_c1, nblk};
+    // columns and entry range of this warp's chunk m in ring slot m % kMetaRing
+    const uint32_t ring = smem_u32(smem + Cfg::kMetaOff) + p * kMetaRing * kMetaInts * 4;
+    auto copy_meta = [&](int m) {
+      if (m >= nloc) return;
+      const int c = cur.chunk(P * m + p);
+      const uint32_t dst = ring + (m % kMetaRing) * kMetaInts * 4 + lane * 4;
+      if (lane < kChunkCols) cp_async4(dst, pv.chunk_col + (int64_t)c * kChunkCols + lane);
+      else if (lane < kMetaInts) cp_async4(dst, pv.chunk_ent + c + (lane - kChunkCols));
+    };
+    // the first kEntReg * 32 entry words of chunk m (its range has landed)
+    auto load_ents = [&](int m, uint32_t (&w)[kEntReg]) {
+      const uint32_t slot = ring + (m % kMetaRing) * kMetaInts * 4;
+      const int e0 = m < nloc ? (int)lds_u32(slot + 64) : 0;
+      const int e1 = m < nloc ? (int)lds_u32(slot + 68) : 0;
 #pragma unroll
-        for (int t = 0; t < 4 * NA; ++t) {
-          const int idx = lane + 32 * t;
-          const int k = idx / (8 * NA), g = idx % (8 * NA);
-          const int col = __shfl_sync(0xffffffffu, my_col, k);
-          const uint32_t dst = b_tile + (k >> 3) * (NA * 1024) + (g >> 3) * 1024 + (k & 7) * 128 +
-                               (((g & 7) ^ (k & 7)) << 4);
-          const __half* src = B + (int64_t)(col >= 0 ? col : 0) * K + g * 8;
-          cp_async16_hint(dst, src, col >= 0 ? 16 : 0, pol_keep);
-        }
-        cp_async_commit();
-        if (n >= kDepth) {
-          // the chunk kDepth behind has landed: publish it to the MMA warp
-          cp_async_wait_group<kDepth>();
-          fence_proxy_async_smem();
-          __syncwarp();
-          if (lane == 0) mbar_arrive(smem_u32(&full[(kProdWarps * (n - kDepth) + p) % kStages]));
-        }
+      for (int r = 0; r < kEntReg; ++r) {
+        const int e = e0 + lane + 32 * r;
+        w[r] = e < e1 ? ld_stream_u32(pv.ent_pv + e, pol_stream) : kNoEntry;
       }
-      q += nc;
-    }
+    };
+    for (int m = 0; m < kMetaRing; ++m) copy_meta(m);
     cp_async_wait_all();
-    fence_proxy_async_smem();
     __syncwarp();
-    if (ok && lane == 0)
-      for (int m = max(0, n - kDepth); m < n; ++m)
-        mbar_arrive(smem_u32(&full[(kProdWarps * m + p) % kStages]));
-  } else if (warp == kMmaWarp) {
+    // entry words of the chunk each register set serves next (chunks n and
+    // n + 1 at the top of the loop), and of the chunk it served before
+    uint32_t ent[2][kEntReg], old[2][kEntReg];
+    int oldcnt[2] = {0, 0};
+    load_ents(0, ent[0]);
+    load_ents(1, ent[1]);
+#pragma unroll
+    for (int r = 0; r < kEntReg; ++r) old[0][r] = old[1][r] = kNoEntry;
+
+    // chunk n with register set SET (= n % 2, a compile-time index)
+    auto body = [&](auto set_tag, int n) -> bool {
+      constexpr int SET = decltype(set_tag)::value;
+      cp_async_wait_group<kMetaWait>();    // metadata of chunk n + 2 (and earlier) has landed
+      __syncwarp();
+      const uint32_t mslot = ring + (n % kMetaRing) * kMetaInts * 4;
+      const int my_col = lane < kChunkCols ? (int)lds_u32(mslot + lane * 4) : -1;
+      const int e0 = (int)lds_u32(mslot + 64), e1 = (int)lds_u32(mslot + 68);
+      const int q = P * n + p, s = q % S, gs = s / kGroup;
+      if (!wait_bar(smem_u32(&empty[gs]), ((q / S) & 1) ^ 1, abort_flag)) return false;
+      uint8_t* st = smem + s * Cfg::kStage;
+      const uint32_t b_tile = smem_u32(st), a_tile = b_tile + Cfg::kBTile;
+      // the slot's previous chunk leaves the A tile
+      if (oldcnt[SET] > kEntReg * 32) {
+        uint4* at = reinterpret_cast<uint4*>(st + Cfg::kBTile);
+        for (int i = lane; i < kATile / 16; i += 32) at[i] = make_uint4(0, 0, 0, 0);
+      } else {
+#pragma unroll
+        for (int r = 0; r < kEntReg; ++r)
+          if ((old[SET][r] & 0xFFFFu) < (uint32_t)kATile) sts_u16(a_tile + (old[SET][r] & 0xFFFFu), 0);
+      }
+      __syncwarp();
+      // this chunk's values
+#pragma unroll
+      for (int r = 0; r < kEntReg; ++r) {
+        const uint32_t w = ent[SET][r];
+        if ((w & 0xFFFFu) < (uint32_t)kATile) sts_u16(a_tile + (w & 0xFFFFu), (uint16_t)(w >> 16));
+        old[SET][r] = w;
+      }
+      for (int e = e0 + kEntReg * 32 + lane; e < e1; e += 32) {
+        const uint32_t w = __ldg(pv.ent_pv + e);
+        sts_u16(a_tile + (w & 0xFFFFu), (uint16_t)(w >> 16));
+      }
+      oldcnt[SET] = e1 - e0;
+      // gather: 16 rows x (8 * NA) 16-byte segments, 4 * NA per lane
+#pragma unroll
+      for (int t = 0; t < 4 * NA; ++t) {
+        const int idx = lane + 32 * t;
+        const int k = idx / (8 * NA), g = idx % (8 * NA);
+        const int col = __shfl_sync(0xffffffffu, my_col, k);
+        const uint32_t dst = b_tile + (k >> 3) * (NA * 1024) + (g >> 3) * 1024 + (k & 7) * 128 +
+                             (((g & 7) ^ (k & 7)) << 4);
+        const __half* src = B + (int64_t)(col >= 0 ? col : 0) * K + g * 8;
+        cp_async16_hint(dst, src, col >= 0 ? 16 : 0, pol_keep);
+      }
+      cp_async_arrive_noinc(smem_u32(&full[gs]));
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&full[gs]));
+      // the same register set serves chunk n + 2; the ring slot takes chunk
+      // n + kMetaRing
+      load_ents(n + 2, ent[SET]);
+      __syncwarp();
+      copy_meta(n + kMetaRing);
+      cp_async_commit();
+      return true;
+    };
+    bool ok = true;
+    int n = 0;
+    for (; n + 1 < nloc && ok; n += 2) {
+      ok = body(std::integral_constant<int, 0>{}, n);
+      if (ok) ok = body(std::integral_constant<int, 1>{}, n + 1);
+    }
+    if (ok && n < nloc) body(std::integral_constant<int, 0>{}, n);
+    cp_async_wait_all();
+  } else if (warp == Cfg::kMmaWarp) {
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
       constexpr uint32_t idesc = umma_idesc_f16(128, Cfg::kN, /*a MN-major*/ false, /*b MN-major*/ true);
-      int q = 0, nacc = 0;
+      // stage s's descriptors: the start-address field (address >> 4) grows by
+      // kStage >> 4 per stage
+      const uint32_t base = smem_u32(smem);
+      const uint64_t adesc0 = umma_smem_desc(base + Cfg::kBTile, 128, 256, 0);
+      const uint64_t bdesc0 = umma_smem_desc(base, 1024, NA * 1024, 2);
+      constexpr uint64_t kStep = Cfg::kStage >> 4;
+      // stage group slot gs (phase ph of its barriers) of the current group
+      int gs = 0, ph = 0, nacc = 0;
       bool ok = true;
       for (int i = 0; i < nblk && ok; ++i) {
-        const int b = __ldg(pv.blk_order + blockIdx.x + i * gridDim.x);
-        const int c0 = __ldg(pv.blk_chunk + b), c1 = __ldg(pv.blk_chunk + b + 1);
-        if (c1 == c0) continue;
-        const int a = nacc & 1, ua = nacc >> 1;
-        if (!wait_bar(smem_u32(&acc_empty[a]), (ua & 1) ^ 1, abort_flag)) { ok = false; break; }
+        const int ngb = (s_c1[i] - s_c0[i]) / kGroup;       // every block: whole groups
+        if (ngb == 0) continue;
+        const int a = nacc & 1;
+        if (!wait_bar(smem_u32(&acc_empty[a]), ((nacc >> 1) & 1) ^ 1, abort_flag)) { ok = false; break; }
         tc_fence_after();
         const uint32_t d = tmem + (uint32_t)(a * Cfg::kN);
-        for (int c = c0; c < c1; ++c, ++q) {
-          const int s = q % kStages;
-          if (!wait_bar(smem_u32(&full[s]), (q / kStages) & 1, abort_flag)) { ok = false; break; }
+        for (int t = 0; t < ngb; ++t) {
+          if (!wait_bar(smem_u32(&full[gs]), ph, abort_flag)) { ok = false; break; }
+          fence_proxy_async_smem();
           tc_fence_after();
-          const uint32_t st = smem_u32(smem + s * Cfg::kStage);
-          const uint64_t adesc = umma_smem_desc(st + Cfg::kBTile, 128, 256, 0);
-          const uint64_t bdesc = umma_smem_desc(st, 1024, NA * 1024, 2);
-          umma_f16(d, adesc, bdesc, idesc, c > c0 ? 1u : 0u);
-          umma_commit(smem_u32(&empty[s]));
+          const uint64_t off = (uint64_t)(gs * kGroup) * kStep;
+          umma_f16(d, adesc0 + off, bdesc0 + off, idesc, t > 0 ? 1u : 0u);
+          umma_f16(d, adesc0 + off + kStep, bdesc0 + off + kStep, idesc, 1u);
+          umma_f16(d, adesc0 + off + 2 * kStep, bdesc0 + off + 2 * kStep, idesc, 1u);
+          umma_f16(d, adesc0 + off + 3 * kStep, bdesc0 + off + 3 * kStep, idesc, 1u);
+          umma_commit(smem_u32(&empty[gs]));
+          if (++gs == NG) {
+            gs = 0;
+            ph ^= 1;
+          }
         }
         if (!ok) break;
         umma_commit(smem_u32(&acc_full[a]));
@@ -301,13 +427,13 @@ __global__ void __launch_bounds__(kBlkThreads, 1)
       if (!wait_bar(smem_u32(done), 0, &never)) *abort_flag = 1;
     }
     __syncwarp();
-  } else {
+  } else if (warp < kEpiWarps) {
     // ------------------------------------------------------------ epilogue
     const int w = warp;                     // TMEM lanes 32w .. 32w+31
     int nacc = 0;
     for (int i = 0; i < nblk; ++i) {
-      const int b = __ldg(pv.blk_order + blockIdx.x + i * gridDim.x);
-      const int nc = __ldg(pv.blk_chunk + b + 1) - __ldg(pv.blk_chunk + b);
+      const int b = s_b[i];
+      const int nc = s_c1[i] - s_c0[i];
       const int64_t r = (int64_t)b * kBlkRows + tid;
       const int ro = __ldg(pv.row_out + r);
       const float sc = __ldg(pv.row_scale + r);
@@ -336,7 +462,7 @@ __global__ void __launch_bounds__(kBlkThreads, 1)
   __syncthreads();
   if (tid == 0 && *abort_flag) atomicExch(pv.err, kErrMbarTimeout);
   tc_fence_after();
-  if (warp == kMmaWarp) tmem_dealloc(tmem, Cfg::kTmemCols);
+  if (warp == Cfg::kMmaWarp) tmem_dealloc(tmem, Cfg::kTmemCols);
 }
 
 // Any K, FP16 or FP32 features, on CUDA cores: one CTA per block and 64
@@ -358,11 +484,12 @@ __global__ void __launch_bounds__(256)
         if (tid < kChunkCols) cols[tid] = pv.chunk_col[(int64_t)c * kChunkCols + tid];
         __syncthreads();
         for (int e = pv.chunk_ent[c]; e < pv.chunk_ent[c + 1]; ++e) {
-          const int pos = pv.ent_pos[e];
+          const uint32_t w = pv.ent_pv[e];
+          const int pos = (int)(w & 0xFFFFu);
           const int m = ((pos >> 8) << 3) | ((pos >> 4) & 7);
           if ((m & 3) != g || !on) continue;
           const int k = (((pos >> 7) & 1) << 3) | ((pos >> 1) & 7);
-          const float v = __half2float(__ushort_as_half(pv.ent_val[e]));
+          const float v = __half2float(__ushort_as_half((uint16_t)(w >> 16)));
           float x;
           if constexpr (sizeof(TB) == 2) x = __half2float(B[(int64_t)cols[k] * K + f0 + f]);
           else x = B[(int64_t)cols[k] * K + f0 + f];
@@ -386,10 +513,8 @@ template <bool F16OUT, int NA>
 int launch_mma_t(const tr_plan* p, const __half* b, void* c, cudaStream_t stream) {
   using Cfg = BlkCfg<NA>;
   if (int rc = kernel_smem_limit((const void*)block_mma_kernel<F16OUT, NA>, Cfg::kSmem)) return rc;
-  const int sms = sm_count();
-  if (sms <= 0) return fail(TR_ERR_CUDA, "no CUDA device");
-  const int grid = std::max(1, std::min(sms, p->view.n_blocks));
-  block_mma_kernel<F16OUT, NA><<<grid, kBlkThreads, Cfg::kSmem, stream>>>(p->view, b, c);
+  block_mma_kernel<F16OUT, NA><<<std::max(1, p->view.n_sched), Cfg::kThreads, Cfg::kSmem, stream>>>(
+      p->view, b, c);
   TRS_CUDA(cudaGetLastError());
   return TR_OK;
 }
@@ -414,7 +539,9 @@ int launch_block(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_
   if (p->view.n_blocks == 0 || k == 0) return TR_OK;
   const bool f16 = c_dtype == TR_OUT_F16;
   const __half* bh = reinterpret_cast<const __half*>(b);
-  if (!force_generic && block_mma_supported(k, b) &&
+  // every CTA's block list fits the staged list
+  bool fits = p->max_sched_blocks <= kMaxBlk;
+  if (!force_generic && fits && block_mma_supported(k, b) &&
       (reinterpret_cast<uintptr_t>(c) & 15) == 0) {
     switch (k / 64) {
       case 1: return f16 ? launch_mma_t<true, 1>(p, bh, c, stream) : launch_mma_t<false, 1>(p, bh, c, stream);

@@ -73,7 +73,10 @@ void lay_out_block(const Csr& a, int32_t b, const std::vector<float>& scale, Blo
     next += layers;
     i = j;
   }
-  const int32_t n_chunks = (next + kChunkCols - 1) / kChunkCols;
+  // whole groups of kChunkGroup chunks per block (the kernel issues a
+  // group's MMAs together); padding chunks have no entries and no columns
+  const int32_t n_chunks =
+      (next + kChunkCols * kChunkGroup - 1) / (kChunkCols * kChunkGroup) * kChunkGroup;
   out.col.assign((size_t)n_chunks * kChunkCols, -1);
   for (size_t i = 0; i < n; ++i) out.col[slot[i]] = keys[i].col;
   // entries ordered by slot (so by chunk), a slot's entries by row

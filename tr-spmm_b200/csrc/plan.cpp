@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <queue>
 #include <atomic>
 #include <cmath>
 #include <cstring>
@@ -628,6 +629,46 @@ int plan_upload(const HostPlan& hp, tr_plan** out) {
   const int64_t rows = (int64_t)W * 16;
   const int64_t n_edges = (int64_t)hp.val_slot.size();
   auto al = [](int64_t b) { return (std::max<int64_t>(b, 1) + 255) / 256 * 256; };
+  // block layout on the device: each entry as one word (FP16 value bits <<
+  // 16 | tile byte offset), and val_slot naming the value's half of it
+  std::vector<uint32_t> ent_pv;
+  std::vector<int32_t> dev_slot;
+  // block schedule: longest-processing-time first over the device's SMs
+  // (each block, heaviest first, to the CTA with the fewest chunks so far)
+  std::vector<int32_t> cta_ptr, cta_blk;
+  if (hp.block) {
+    int dev = 0, sms = 1;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) {
+      cudaGetLastError();
+      sms = 1;
+    }
+    const int32_t NB = (int32_t)hp.blk_order.size();
+    const int32_t G = std::max(1, std::min(sms, NB));
+    std::vector<std::vector<int32_t>> lists(G);
+    std::priority_queue<std::pair<int64_t, int32_t>, std::vector<std::pair<int64_t, int32_t>>,
+                        std::greater<std::pair<int64_t, int32_t>>> load;
+    for (int32_t c = 0; c < G; ++c) load.push({0, c});
+    for (int32_t b : hp.blk_order) {
+      auto [l, c] = load.top();
+      load.pop();
+      lists[c].push_back(b);
+      load.push({l + hp.blk_chunk[b + 1] - hp.blk_chunk[b] + 1, c});
+    }
+    cta_ptr.assign((size_t)G + 1, 0);
+    for (int32_t c = 0; c < G; ++c) {
+      cta_ptr[c + 1] = cta_ptr[c] + (int32_t)lists[c].size();
+      cta_blk.insert(cta_blk.end(), lists[c].begin(), lists[c].end());
+    }
+  }
+  if (hp.block) {
+    ent_pv.resize(hp.ent_pos.size());
+    for (size_t e = 0; e < ent_pv.size(); ++e)
+      ent_pv[e] = (uint32_t)hp.ent_pos[e] | ((uint32_t)hp.ent_val[e] << 16);
+    dev_slot.resize(hp.val_slot.size());
+    for (size_t e = 0; e < dev_slot.size(); ++e)
+      dev_slot[e] = hp.val_slot[e] < 0 ? -1 : 2 * hp.val_slot[e] + 1;
+  }
   struct Sec { const void* src; int64_t bytes; int64_t size; };
   Sec secs[] = {
       {hp.win_tile.data(), (W + 1) * 4, 0},
@@ -641,17 +682,18 @@ int plan_upload(const HostPlan& hp, tr_plan** out) {
       {hp.win_order.data(), (int64_t)W * 4, 0},
       {hp.row_scale.data(), rows * 4, 0},
       {hp.row_out.data(), rows * 4, 0},
-      {hp.val_slot.data(), n_edges * 4, 0},
+      {hp.block ? dev_slot.data() : hp.val_slot.data(), n_edges * 4, 0},
       {hp.edge_row.data(), n_edges * 4, 0},
       {hp.res_edge.data(), (int64_t)hp.res_edge.size() * 4, 0},
       {nullptr, 0, 256},                       // error words
       {hp.blk_chunk.data(), (int64_t)hp.blk_chunk.size() * 4, 0},
       {hp.chunk_col.data(), (int64_t)hp.chunk_col.size() * 4, 0},
       {hp.chunk_ent.data(), (int64_t)hp.chunk_ent.size() * 4, 0},
-      {hp.ent_pos.data(), (int64_t)hp.ent_pos.size() * 2, 0},
-      {hp.ent_val.data(), (int64_t)hp.ent_val.size() * 2, 0},
+      {ent_pv.data(), (int64_t)ent_pv.size() * 4, 0},
       {hp.ent_src.data(), (int64_t)hp.ent_src.size() * 4, 0},
       {hp.blk_order.data(), (int64_t)hp.blk_order.size() * 4, 0},
+      {cta_ptr.data(), (int64_t)cta_ptr.size() * 4, 0},
+      {cta_blk.data(), (int64_t)cta_blk.size() * 4, 0},
   };
   constexpr int kSecs = sizeof(secs) / sizeof(secs[0]);
   int64_t total = 0;
@@ -697,20 +739,24 @@ int plan_upload(const HostPlan& hp, tr_plan** out) {
   v.blk_chunk = (const int32_t*)at[15];
   v.chunk_col = (const int32_t*)at[16];
   v.chunk_ent = (const int32_t*)at[17];
-  v.ent_pos = (const uint16_t*)at[18];
-  v.ent_val = (const uint16_t*)at[19];
-  v.ent_src = (const int32_t*)at[20];
-  v.blk_order = (const int32_t*)at[21];
+  v.ent_pv = (const uint32_t*)at[18];
+  v.ent_src = (const int32_t*)at[19];
+  v.blk_order = (const int32_t*)at[20];
+  v.n_sched = hp.block ? (int32_t)cta_ptr.size() - 1 : 0;
+  v.cta_ptr = (const int32_t*)at[21];
+  v.cta_blk = (const int32_t*)at[22];
   p->blocked = hp.block;
-  // re-valuing writes tile values below n_tile_vals: the block layout's
-  // values take that place
-  p->tile_a = hp.block ? (uint16_t*)at[19] : (uint16_t*)at[4];
+  for (size_t c = 0; c + 1 < cta_ptr.size(); ++c)
+    p->max_sched_blocks = std::max(p->max_sched_blocks, cta_ptr[c + 1] - cta_ptr[c]);
+  // re-valuing writes FP16 values at tile_a[val_slot] below n_tile_vals; in
+  // the block layout that is the value half of each entry word
+  p->tile_a = hp.block ? (uint16_t*)at[18] : (uint16_t*)at[4];
   p->res_val = (uint16_t*)at[7];
   p->row_scale = (float*)at[9];
   p->val_slot = (int32_t*)at[11];
   p->edge_row = (int32_t*)at[12];
   p->n_edges = n_edges;
-  p->n_tile_vals = hp.block ? (int64_t)hp.ent_val.size() : T * 256;
+  p->n_tile_vals = hp.block ? 2 * (int64_t)ent_pv.size() : T * 256;
   p->row_scaled = hp.row_scaled;
   p->info.n_rows = hp.n_rows;
   p->info.n_cols = hp.n_cols;

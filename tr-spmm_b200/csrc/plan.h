@@ -31,7 +31,8 @@
 // touches is one K slot of a 16-column chunk, so each feature row of B is
 // gathered once per block and multiplied by the tensor cores against all 128
 // rows at once (tcgen05.mma M = 128 rows, N = K features, K = 16 slots):
-//   blk_chunk[NB+1]  chunks of block b: [blk_chunk[b], blk_chunk[b+1])
+//   blk_chunk[NB+1]  chunks of block b: [blk_chunk[b], blk_chunk[b+1]), a
+//                    multiple of 4 (trailing chunks without entries pad it)
 //   chunk_col[NC*16] row of B gathered into each slot of a chunk (-1: none)
 //   chunk_ent[NC+1]  entries of chunk c: [chunk_ent[c], chunk_ent[c+1])
 //   ent_pos[E]       byte offset of the entry in the chunk's 128x16 FP16 A
@@ -41,7 +42,9 @@
 //   ent_src[E]       CSR entry of the caller's A behind the entry
 //   blk_order[NB]    blocks in decreasing chunk count (launch order)
 // row_scale / row_out cover NB*128 rows (n_windows = NB*8); the window
-// sections are empty, and val_slot indexes ent_val.
+// sections are empty, and val_slot indexes ent_val.  On the device each
+// entry is one 32-bit word, ent_pv[e] = ent_val[e] << 16 | ent_pos[e], and
+// the device val_slot is 2e + 1 (the value's 16-bit half of that word).
 #pragma once
 #include <cstdint>
 #include <string>
@@ -71,10 +74,14 @@ struct PlanView {
   const int32_t* blk_chunk;
   const int32_t* chunk_col;
   const int32_t* chunk_ent;
-  const uint16_t* ent_pos;
-  const uint16_t* ent_val;
+  const uint32_t* ent_pv;         // per entry: FP16 value bits << 16 | ent_pos
   const int32_t* ent_src;
   const int32_t* blk_order;
+  // launch schedule of the block kernels (device only, made at upload for the
+  // device's SM count): CTA c takes blocks cta_blk[cta_ptr[c] .. cta_ptr[c+1])
+  int32_t n_sched;
+  const int32_t* cta_ptr;
+  const int32_t* cta_blk;
 };
 
 struct HostPlan {
@@ -96,9 +103,11 @@ struct HostPlan {
   std::vector<uint16_t> ent_pos, ent_val;
 };
 
-// Rows per block of the block layout and K slots per chunk.
+// Rows per block of the block layout, K slots per chunk, and chunks per
+// group (every block holds a whole number of groups).
 constexpr int kBlkRows = 128;
 constexpr int kChunkCols = 16;
+constexpr int kChunkGroup = 4;
 
 // A CSR matrix on its way through the builder; src[e] is the entry of the
 // caller's A behind entry e.
@@ -125,6 +134,7 @@ struct tr_plan {
   int64_t n_tile_vals = 0;      // T*256
   bool row_scaled = false;
   bool blocked = false;         // block layout (the block engine)
+  int32_t max_sched_blocks = 0; // most blocks any CTA of the block schedule takes
   tr_plan_info info{};
 };
 

@@ -117,7 +117,8 @@ bool contents_valid(const HostPlan& h) {
       h.blk_chunk[0] != 0)
     return false;
   for (int64_t b = 0; b < NB; ++b)
-    if (h.blk_chunk[b] > h.blk_chunk[b + 1]) return false;
+    if (h.blk_chunk[b] > h.blk_chunk[b + 1] || (h.blk_chunk[b + 1] - h.blk_chunk[b]) % kChunkGroup)
+      return false;
   const int64_t NC = h.blk_chunk[NB];
   if ((int64_t)h.chunk_col.size() != NC * kChunkCols || (int64_t)h.chunk_ent.size() != NC + 1 ||
       h.chunk_ent[0] != 0 || h.chunk_ent[NC] != ents || (int64_t)h.ent_val.size() != ents ||
