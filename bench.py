@@ -351,6 +351,9 @@ def main():
     ap.add_argument("--plan-options", default=None,
                     help="JSON plan options to use instead of the autotuner's choice "
                          '(e.g. \'{"demote_below": 1000}\'), for profiling runs')
+    ap.add_argument("--adjoint-options", default=None,
+                    help="JSON options of the adjoint plan (default: the autotuner's "
+                         "backward choice, or --plan-options when given)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -374,18 +377,29 @@ def main():
     gt = transpose_csr(g.indptr, g.indices, g.values, g.n_rows, g.n_cols)
 
     # ---- plan options: the autotuner's choice for the forward plan ------------
+    # and, for the adjoint plan, the fastest whole backward (dB and dval)
     t0 = time.perf_counter()
+    bwd_report = {"results": []}
     if args.plan_options is not None:
         opts, tune_report = json.loads(args.plan_options), {"results": []}
+        adj_opts = json.loads(args.adjoint_options) if args.adjoint_options else dict(opts)
     elif args.no_tune:
         opts, tune_report = {}, {"results": []}
+        adj_opts = {}
     else:
         opts, tune_report = autotune.tune(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, k,
                                           device=dev, row_scale=True, reps=5)
+        if args.adjoint_options:
+            adj_opts = json.loads(args.adjoint_options)
+        else:
+            adj_opts, bwd_report = autotune.tune(g.indptr, g.indices, g.values, g.n_rows,
+                                                 g.n_cols, k, device=dev, row_scale=True, reps=5,
+                                                 backward=True)
     tune_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     adj = RoutedAdjacency(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, device=dev,
-                          row_scale=True, **{"promote_min": 0, **opts})
+                          row_scale=True, adjoint_options={"promote_min": 0, **adj_opts},
+                          **{"promote_min": 0, **opts})
     plan_s = time.perf_counter() - t0
     pf, pa = adj.fwd, adj.adj
 
@@ -446,11 +460,22 @@ def main():
     adj_sddmm_ms = float(np.mean(timed(lambda: pa.adjoint_sddmm(ip, ix, dcd, bd, db=dbd, dval=dvd),
                                        n_side, 3)))
     sddmm_ms = float(np.mean(timed(lambda: trspmm.sddmm_csr(ip, ix, dcd, bd, out=dvd), n_side, 3)))
-    res_mask = trspmm.TR_ROUTE_ALL | trspmm.TR_ROUTE_RESIDUAL_PASS
-    res_ms = float(np.mean(timed(lambda: pf.spmm(bd, out=c2, route_mask=res_mask), n_side, 3)))
+    fwd_block = pf.info["engine"] == trspmm.TR_ENGINE_BLOCK
+    if fwd_block:
+        res_ms = None                  # the block engine has no CUDA-core residual pass
+    else:
+        res_mask = trspmm.TR_ROUTE_ALL | trspmm.TR_ROUTE_RESIDUAL_PASS
+        res_ms = float(np.mean(timed(lambda: pf.spmm(bd, out=c2, route_mask=res_mask), n_side, 3)))
     plain_ms = float(np.mean(timed(plain_step, n_side, 3)))
     plain_fwd_ms = float(np.mean(timed(lambda: trspmm.spmm_csr(ip, ix, iv, bd, g.n_rows, out=c2),
                                        n_side, 3)))
+    # like for like backward: the same fused dB + dval pass over a CSR of A^T
+    # in natural order (no reordering, no tiles: the plain single route)
+    plain_adj = trspmm.Plan.build(g.indptr, g.indices, g.values, g.n_rows, g.n_cols,
+                                  transpose=True, row_scale=True, demote_below=1000)
+    plain_bwd_ms = float(np.mean(timed(
+        lambda: plain_adj.adjoint_sddmm(ip, ix, dcd, bd, db=db2, dval=dv2), n_side, 3)))
+    plain_adj.close()
     # the same forward with the features in FP32 (FP32-feature route, same plan)
     b32 = bd.float()
     c3 = torch.empty_like(cd)
@@ -548,9 +573,13 @@ def main():
     serial_ms = float(np.mean(timed(serial_step, min(e2e_steps, 10), 2)))
 
     peak, peak_kind = _peaks()
-    res_nnz = int(pf.info["residual_nnz"])
-    res_bytes = algorithmic_bytes(res_nnz, g.n_rows, g.n_cols, k, 4)
-    res_gbs = res_bytes / (res_ms * 1e-3) / 1e9
+    if fwd_block:
+        res_bytes = res_gbs = None
+    else:
+        res_nnz = int(pf.info["residual_nnz"])
+        res_bytes = algorithmic_bytes(res_nnz, g.n_rows, g.n_cols, k, 4)
+        res_gbs = res_bytes / (res_ms * 1e-3) / 1e9
+    fwd_bytes = algorithmic_bytes(g.nnz, g.n_rows, g.n_cols, k, 4)
     sbytes = step_bytes(g.nnz, g.n_rows, g.n_cols, k)
     cpu = None
     cpu_torch = None
@@ -568,19 +597,27 @@ def main():
 
     def launches(p):
         info = p.info
+        if info["engine"] == trspmm.TR_ENGINE_BLOCK:
+            return 1
         tiles = info["tc_tiles"] + info["sptc_tiles"] + info["promoted_tiles"] > 0
         return (1 if (info["residual_nnz"] > 0 or not tiles) else 0) + (1 if tiles else 0)
 
-    fused_bwd = (pa.info["tc_tiles"] + pa.info["sptc_tiles"] + pa.info["promoted_tiles"] == 0
-                 and pa.info["residual_nnz"] == g.nnz and k <= 128)
+    fused_bwd = (pa.info["engine"] == trspmm.TR_ENGINE_WINDOW
+                 and pa.info["tc_tiles"] + pa.info["sptc_tiles"] + pa.info["promoted_tiles"] == 0
+                 and pa.info["residual_nnz"] == g.nnz and k <= 256)
     bwd_launches = 1 if fused_bwd else launches(pa) + 1
-    # the dominant kernel of the step: the fused backward when the adjoint plan
-    # allows it (its one launch takes longer than the forward's residual pass)
-    if fused_bwd and adj_sddmm_ms >= res_ms:
+    # the dominant kernel of the step: the longer of the backward's one fused
+    # launch and the forward's (block kernel or CUDA-core residual pass)
+    fwd_kernel_ms = fwd_ms if fwd_block else res_ms
+    if fused_bwd and adj_sddmm_ms >= fwd_kernel_ms:
         dom_kernel = "seg_adjoint_sddmm_kernel (fused backward: dB = A^T dC, dval = SDDMM)"
         abytes = adjoint_sddmm_bytes(g.nnz, g.n_rows, g.n_cols, k)
         achieved = abytes / (adj_sddmm_ms * 1e-3) / 1e9
         traffic = _profile_traffic("seg_adjoint_sddmm_large_routed.txt")
+    elif fwd_block:
+        dom_kernel = "block_mma_kernel (forward on the tensor cores, 128-row blocks)"
+        abytes, achieved = fwd_bytes, fwd_bytes / (fwd_ms * 1e-3) / 1e9
+        traffic = _profile_traffic("block_mma_forward_large_routed.txt")
     else:
         dom_kernel = "seg_block_kernel (forward residual pass)"
         abytes, achieved = res_bytes, res_gbs
@@ -595,7 +632,8 @@ def main():
             "config": {"workload": args.workload, "n_nodes": g.n_rows, "nnz": g.nnz, "k": k,
                        "step": "forward + adjoint + SDDMM", "out": "f32",
                        "l2": "flushed between steps (256 MiB write)",
-                       "parallelism": f"replicas{world}", "plan_options": opts},
+                       "parallelism": f"replicas{world}", "plan_options": opts,
+                       "adjoint_plan_options": adj_opts},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind, "algorithmic_bytes": abytes,
@@ -614,14 +652,22 @@ def main():
                       "adjoint_sddmm_fused_ms": adj_sddmm_ms,
                       "cpu_torch_sparse_forward": cpu_torch,
                       "forward_residual_pass_ms": res_ms,
-                      "forward_residual_roofline": {
+                      "forward_residual_roofline": None if fwd_block else {
                           "achieved_gbs": res_gbs, "frac": res_gbs / peak,
                           "algorithmic_bytes": res_bytes,
                           "traffic": _profile_traffic("seg_residual_pass_large_routed.txt")},
+                      "forward_roofline": {
+                          "achieved_gbs": fwd_bytes / (fwd_ms * 1e-3) / 1e9,
+                          "frac": fwd_bytes / (fwd_ms * 1e-3) / 1e9 / peak,
+                          "algorithmic_bytes": fwd_bytes},
                       "plain_csr_step_ms": plain_ms, "plain_csr_forward_ms": plain_fwd_ms,
+                      "plain_fused_backward_ms": plain_bwd_ms,
                       "fp32_features_forward": fp32_route,
                       "routed_vs_plain_step": plain_ms / ms,
                       "routed_vs_plain_forward": plain_fwd_ms / fwd_ms,
+                      "routed_vs_plain_backward_fused": plain_bwd_ms / adj_sddmm_ms,
+                      "routed_vs_plain_step_equal_fusion":
+                          (plain_fwd_ms + plain_bwd_ms) / (fwd_ms + adj_sddmm_ms),
                       "max_rel_diff_vs_plain": err,
                       "step_algorithmic_bytes": sbytes,
                       "step_hbm_gbs": sbytes / (ms * 1e-3) / 1e9,
@@ -629,6 +675,8 @@ def main():
                       "plan_build_s": plan_s, "tune_s": tune_s,
                       "autotune": [{"options": r["options"], "ms": r["ms"]}
                                    for r in tune_report.get("results", [])],
+                      "autotune_backward": [{"options": r["options"], "ms": r["ms"]}
+                                            for r in bwd_report.get("results", [])],
                       "batched_512": batched,
                       "plan_forward": pf.info, "plan_adjoint": pa.info,
                       "e2e_ms_per_step": e2e_max},

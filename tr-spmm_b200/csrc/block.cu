@@ -15,8 +15,9 @@
 // layout pads it with chunks that have no entries); the four stage slots of
 // a group share one full and one empty barrier.  Roles:
 //
-//   producer warps (kProd of them, two stage slots each; chunk q of the
-//   stream taken by warp q % kProd)
+//   producer warps (kProd of them, two stage slots each, on the schedulers
+//   the MMA warp does not use; chunk q of the stream taken by producer
+//   q % kProd)
 //       per chunk: wait until the slot is free, clear from its A tile the
 //       positions the slot's previous chunk set and write this chunk's
 //       values (packed entries value << 16 | tile byte offset, loaded into
@@ -30,7 +31,8 @@
 //       filled eight chunks ahead.  Many producer warps keep enough gathers in
 //       flight: a warp's cp.async issue, not the memory system, sets the rate
 //       of one warp;
-//   MMA warp (one elected thread)
+//   MMA warp 4 (one elected thread; its scheduler is shared only with
+//   epilogue warp 0)
 //       per group: wait full, one proxy fence (the operands were written
 //       through the generic proxy; the tensor core reads them through the
 //       async proxy), four tcgen05.mma (M = 128, N = K, K = 16) into the
@@ -66,7 +68,8 @@ namespace {
 
 constexpr int kGroup = kChunkGroup;     // chunks per barrier group
 constexpr int kEpiWarps = 4;
-constexpr int kProdWarp0 = kEpiWarps;
+constexpr int kMmaWarp = kEpiWarps;     // warp 4
+constexpr int kProdWarp0 = kEpiWarps;   // producers: warps 4 + 4i + 1 + j (j < 3)
 constexpr int kATile = 4096;            // 128 rows x 16 slots, FP16
 constexpr int kEntReg = 2;              // entry words per lane held in registers
 constexpr int kMaxBlk = 512;            // blocks per CTA (staged list)
@@ -76,6 +79,7 @@ constexpr int kMetaRing = 8;            // chunks of metadata staged ahead, per 
 // kMetaRing - 3 groups suffices and never waits for recent gathers
 constexpr int kMetaWait = kMetaRing - 3;
 constexpr int kMetaInts = 18;           // a chunk's 16 columns and entry range
+constexpr int kMetaStride = 32;         // ints per ring slot (16-byte aligned slots)
 constexpr uint32_t kNoEntry = 0xFFFFFFFFu;   // empty register slot (offset past the tile)
 
 template <int NA>
@@ -83,17 +87,21 @@ struct BlkCfg {
   static constexpr int kN = 64 * NA;               // features = MMA N
   static constexpr int kBTile = 2048 * NA;         // 16 slots x kN features, FP16
   static constexpr int kStage = kBTile + kATile;   // a multiple of 1024
-  // as many stage slots as shared memory holds; two per producer warp
-  static constexpr int kStages = NA == 1 ? 32 : (NA == 2 ? 24 : (NA == 3 ? 20 : 16));
+  // as many stage slots as shared memory (and registers) allow; two per
+  // producer warp
+  static constexpr int kStages = NA == 1 ? 32 : (NA == 2 ? 24 : 16);
   static constexpr int kProd = kStages / 2;
   static constexpr int kGroups = kStages / kGroup;
-  static constexpr int kMmaWarp = kProdWarp0 + kProd;
-  static constexpr int kThreads = (kMmaWarp + 1) * 32;
+  // warps 0-3 epilogue, warp 4 MMA; producers on the warps of the other
+  // three schedulers (warp % 4 != 0), so the MMA thread shares its scheduler
+  // only with epilogue warp 0
+  static constexpr int kThreads = (kProdWarp0 + 4 * ((kProd - 1) / 3) + 1 + (kProd - 1) % 3 + 1) * 32;
   static constexpr int kBarOff = kStages * kStage;
   // full[G], empty[G], acc_full[2], acc_empty[2], done; tmem slot, abort flag
-  static constexpr int kBlkOff = kBarOff + (2 * kGroups + 5) * 8 + 16;
-  static constexpr int kMetaOff = kBlkOff + 3 * kMaxBlk * 4;
-  static constexpr int kSmem = 1024 + kMetaOff + kProd * kMetaRing * kMetaInts * 4;
+  static constexpr int kBlkOff = (kBarOff + (2 * kGroups + 5) * 8 + 16 + 127) / 128 * 128;
+  // the ring is read with 16-byte loads: 128-byte aligned
+  static constexpr int kMetaOff = (kBlkOff + 3 * kMaxBlk * 4 + 127) / 128 * 128;
+  static constexpr int kSmem = 1024 + kMetaOff + kProd * kMetaRing * kMetaStride * 4;
   static constexpr uint32_t kTmemCols = 2 * kN <= 128 ? 128 : (2 * kN <= 256 ? 256 : 512);
   // arrivals that complete a group: 32 lanes and one warp arrival per chunk
   static constexpr uint32_t kFullCount = kGroup * 33;
@@ -101,6 +109,8 @@ struct BlkCfg {
   static_assert(kStage % 1024 == 0, "B tiles keep the 1024-byte swizzle alignment");
   static_assert(kSmem <= 227 * 1024, "shared memory budget");
   static_assert(kThreads <= 1024, "one CTA");
+  static_assert(kBlkOff % 16 == 0 && kMetaOff % 128 == 0 && (kMetaStride * 4) % 16 == 0,
+                "16-byte shared loads of the metadata ring stay aligned");
 };
 
 __device__ __forceinline__ bool wait_bar(uint32_t bar, uint32_t parity, volatile int* abort) {
@@ -197,18 +207,50 @@ __device__ __forceinline__ void cp_async_arrive_noinc(uint32_t bar) {
   asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(bar) : "memory");
 }
 
+__device__ __forceinline__ uint4 lds_u128(uint32_t addr) {
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];\n"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "r"(addr) : "memory");
+  return v;
+}
+
+// Gather lanes: with 8 * NA 16-byte segments per 256 * NA-byte row, a warp
+// instruction copies 32 / (8 * NA) rows, lane l taking row t * G + l / (8 * NA)
+// of instruction t (G = rows per instruction).  A chunk's 16 columns are
+// stored in its metadata ring slot grouped by lane group (G groups of
+// 16 / G rows), so a lane reads its columns with 16-byte loads; K = 192
+// (rows split across instructions) reads all 16 columns and shuffles.
+template <int NA> struct RowsPerLane { static constexpr int value = NA == 3 ? 4 * NA : 16 / (32 / (8 * NA)); };
+template <int NA>
+__device__ __forceinline__ int col_pos(int k) {
+  if constexpr (NA == 3) {
+    return k;
+  } else {
+    constexpr int G = 32 / (8 * NA), R = 16 / G;     // lane groups, rows per lane
+    return (k % G) * R + k / G;
+  }
+}
+
 // Position in this CTA's chunk stream: chunk id of stream index q (q only
 // grows), walking the staged block list.
 struct StreamCursor {
   const int* c0;
   const int* c1;
-  int nblk, i = 0, q0 = 0;
+  int nblk, i = 0, q0 = 0, qend = -1, base = 0;
   __device__ int chunk(int q) {
-    while (i < nblk - 1 && q >= q0 + (c1[i] - c0[i])) {
-      q0 += c1[i] - c0[i];
-      ++i;
+    if (q >= qend) {       // shared memory is read only when q leaves the block
+      if (qend < 0) {
+        qend = c1[0] - c0[0];
+        base = c0[0];
+      }
+      while (i < nblk - 1 && q >= qend) {
+        q0 = qend;
+        ++i;
+        qend = q0 + (c1[i] - c0[i]);
+        base = c0[i];
+      }
     }
-    return c0[i] + (q - q0);
+    return base + (q - q0);
   }
 };
 
@@ -241,7 +283,7 @@ __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
   const int bfirst = __ldg(pv.cta_ptr + blockIdx.x);
   const int nblk = __ldg(pv.cta_ptr + blockIdx.x + 1) - bfirst;
 
-  if (warp == Cfg::kMmaWarp) {
+  if (warp == kMmaWarp) {
     tmem_alloc(smem_u32(tmem_slot), Cfg::kTmemCols);
     tmem_relinquish();
   }
@@ -276,9 +318,10 @@ __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  if (warp >= kProdWarp0 && warp < Cfg::kMmaWarp) {
+  const int prod = (warp > kProdWarp0 && (warp & 3) != 0) ? ((warp - kProdWarp0) >> 2) * 3 + (warp & 3) - 1 : -1;
+  if (prod >= 0 && prod < P) {
     // ------------------------------------------------------------ producers
-    const int p = warp - kProdWarp0;
+    const int p = prod;
     const uint64_t pol_keep = l2_policy_evict_last(), pol_stream = l2_policy_evict_first();
     int total = 0;
     for (int i = lane; i < nblk; i += 32) total += s_c1[i] - s_c0[i];
@@ -287,17 +330,18 @@ __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
     const int nloc = total > p ? (total - p + P - 1) / P : 0;
     StreamCursor cur{s_c0, s_c1, nblk};
     // columns and entry range of this warp's chunk m in ring slot m % kMetaRing
-    const uint32_t ring = smem_u32(smem + Cfg::kMetaOff) + p * kMetaRing * kMetaInts * 4;
+    const uint32_t ring = smem_u32(smem + Cfg::kMetaOff) + p * kMetaRing * kMetaStride * 4;
     auto copy_meta = [&](int m) {
       if (m >= nloc) return;
       const int c = cur.chunk(P * m + p);
-      const uint32_t dst = ring + (m % kMetaRing) * kMetaInts * 4 + lane * 4;
-      if (lane < kChunkCols) cp_async4(dst, pv.chunk_col + (int64_t)c * kChunkCols + lane);
+      const uint32_t dst = ring + (m % kMetaRing) * kMetaStride * 4 + lane * 4;
+      if (lane < kChunkCols)        // row k at ring position col_pos(k)
+        cp_async4(dst - lane * 4 + col_pos<NA>(lane) * 4, pv.chunk_col + (int64_t)c * kChunkCols + lane);
       else if (lane < kMetaInts) cp_async4(dst, pv.chunk_ent + c + (lane - kChunkCols));
     };
     // the first kEntReg * 32 entry words of chunk m (its range has landed)
     auto load_ents = [&](int m, uint32_t (&w)[kEntReg]) {
-      const uint32_t slot = ring + (m % kMetaRing) * kMetaInts * 4;
+      const uint32_t slot = ring + (m % kMetaRing) * kMetaStride * 4;
       const int e0 = m < nloc ? (int)lds_u32(slot + 64) : 0;
       const int e1 = m < nloc ? (int)lds_u32(slot + 68) : 0;
 #pragma unroll
@@ -323,8 +367,22 @@ __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
       constexpr int SET = decltype(set_tag)::value;
       cp_async_wait_group<kMetaWait>();    // metadata of chunk n + 2 (and earlier) has landed
       __syncwarp();
-      const uint32_t mslot = ring + (n % kMetaRing) * kMetaInts * 4;
-      const int my_col = lane < kChunkCols ? (int)lds_u32(mslot + lane * 4) : -1;
+      const uint32_t mslot = ring + (n % kMetaRing) * kMetaStride * 4;
+      // the columns of the rows this lane copies (see col_pos)
+      int cols[RowsPerLane<NA>::value];
+      if constexpr (NA == 3) {
+        const int my_col = lane < kChunkCols ? (int)lds_u32(mslot + lane * 4) : -1;
+#pragma unroll
+        for (int t = 0; t < 4 * NA; ++t) cols[t] = __shfl_sync(0xffffffffu, my_col, (lane + 32 * t) / 24);
+      } else {
+        constexpr int R = RowsPerLane<NA>::value;   // rows per lane
+        const uint32_t at = mslot + (lane / (8 * NA)) * R * 4;
+#pragma unroll
+        for (int t = 0; t < R; t += 4) {
+          const uint4 v = lds_u128(at + t * 4);
+          cols[t] = (int)v.x; cols[t + 1] = (int)v.y; cols[t + 2] = (int)v.z; cols[t + 3] = (int)v.w;
+        }
+      }
       const int e0 = (int)lds_u32(mslot + 64), e1 = (int)lds_u32(mslot + 68);
       const int q = P * n + p, s = q % S, gs = s / kGroup;
       if (!wait_bar(smem_u32(&empty[gs]), ((q / S) & 1) ^ 1, abort_flag)) return false;
@@ -357,7 +415,7 @@ __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
       for (int t = 0; t < 4 * NA; ++t) {
         const int idx = lane + 32 * t;
         const int k = idx / (8 * NA), g = idx % (8 * NA);
-        const int col = __shfl_sync(0xffffffffu, my_col, k);
+        const int col = cols[t];
         const uint32_t dst = b_tile + (k >> 3) * (NA * 1024) + (g >> 3) * 1024 + (k & 7) * 128 +
                              (((g & 7) ^ (k & 7)) << 4);
         const __half* src = B + (int64_t)(col >= 0 ? col : 0) * K + g * 8;
@@ -382,7 +440,7 @@ __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
     }
     if (ok && n < nloc) body(std::integral_constant<int, 0>{}, n);
     cp_async_wait_all();
-  } else if (warp == Cfg::kMmaWarp) {
+  } else if (warp == kMmaWarp) {
     // ------------------------------------------------------------ MMA issuer
     if (lane == 0) {
       constexpr uint32_t idesc = umma_idesc_f16(128, Cfg::kN, /*a MN-major*/ false, /*b MN-major*/ true);
@@ -462,7 +520,7 @@ __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
   __syncthreads();
   if (tid == 0 && *abort_flag) atomicExch(pv.err, kErrMbarTimeout);
   tc_fence_after();
-  if (warp == Cfg::kMmaWarp) tmem_dealloc(tmem, Cfg::kTmemCols);
+  if (warp == kMmaWarp) tmem_dealloc(tmem, Cfg::kTmemCols);
 }
 
 // Any K, FP16 or FP32 features, on CUDA cores: one CTA per block and 64

@@ -34,11 +34,15 @@ class RoutedAdjacency:
 
     def __init__(self, indptr, indices, values, n_rows, n_cols, device="cuda",
                  row_scale=True, promote_min=2, reorder=False, plan_cache=None,
-                 features="f16", **route_kw):
+                 features="f16", adjoint_options=None, **route_kw):
         """plan_cache: None builds both plans; True or a directory takes them
         from the on-disk plan cache (trspmm.plan_cache), routing once per
         graph.  features: "f16" (FP16 operands) or "f32" (FP32 features on
-        the FP32-feature route)."""
+        the FP32-feature route).  The other keywords shape both plans
+        (Plan.build: engine, demote_below, promote_min, reorder, ...);
+        adjoint_options (a dict) overrides them for the adjoint plan alone,
+        e.g. a block-engine forward with the fused CUDA-core backward
+        (engine="window", demote_below=1000)."""
         if features not in ("f16", "f32"):
             raise ValueError(f"features must be 'f16' or 'f32', not {features!r}")
         self.features = features
@@ -48,14 +52,15 @@ class RoutedAdjacency:
         self.n_rows, self.n_cols = int(n_rows), int(n_cols)
         self.nnz = int(indices.size)
         kw = dict(row_scale=row_scale, promote_min=promote_min, reorder=reorder, **route_kw)
+        akw = dict(kw, **(adjoint_options or {}))
         if plan_cache:
             from .plan_cache import cached_plan
             d = None if plan_cache is True else str(plan_cache)
             self.fwd = cached_plan(indptr, indices, values, n_rows, n_cols, d, transpose=False, **kw)
-            self.adj = cached_plan(indptr, indices, values, n_rows, n_cols, d, transpose=True, **kw)
+            self.adj = cached_plan(indptr, indices, values, n_rows, n_cols, d, transpose=True, **akw)
         else:
             self.fwd = Plan.build(indptr, indices, values, n_rows, n_cols, transpose=False, **kw)
-            self.adj = Plan.build(indptr, indices, values, n_rows, n_cols, transpose=True, **kw)
+            self.adj = Plan.build(indptr, indices, values, n_rows, n_cols, transpose=True, **akw)
         self.device = torch.device(device)
         self.indptr = torch.from_numpy(indptr).to(self.device)
         self.indices = torch.from_numpy(indices).to(self.device)

@@ -8,18 +8,26 @@ earns its place in a tcgen05 tile when several rows of its window use it.
 This tuner times the candidate plan shapes on the device and keeps the
 fastest:
 
-  reorder        cluster rows sharing columns into the same windows
+  engine         "window": the reference's three routes over 16-row windows;
+                 "block": every entry on the tensor cores over 128-row
+                 blocks, each distinct column of a block gathered once
+  reorder        cluster rows sharing columns into the same windows / blocks
   demote_below   2:4 tile columns with fewer entries go to the CUDA cores
   promote_min    CUDA-core columns with at least this many entries in a
                  window become tensor-core tiles
 
-The window height (16 rows, the reference's tables) and the feature chunk
-(128 features, the tcgen05 M dimension) are fixed by the kernels; the
-kernel pair for the full product is chosen by the library from K.
+With backward=True the tuner times the whole backward of C = A(w) . B
+(dB = A^T dC and the edge-value gradient) for candidate adjoint plans: the
+fused CUDA-core pass of all-residual window plans against the block engine's
+dB followed by the SDDMM.
+
+The window height (16 rows, the reference's tables; 128-row blocks for the
+block engine) and the feature chunk are fixed by the kernels; the kernel
+for the full product is chosen by the library from K.
 
 Results are cached as JSON keyed by device name, K, the power-of-two
-buckets of nnz and rows, and the plan kind (forward or adjoint), in
-$TRSPMM_AUTOTUNE_CACHE or ~/.cache/trspmm/autotune.json.
+buckets of nnz and rows, and the plan kind (forward, adjoint or backward),
+in $TRSPMM_AUTOTUNE_CACHE or ~/.cache/trspmm/autotune.json.
 """
 from __future__ import annotations
 
@@ -39,6 +47,15 @@ CANDIDATES = [
     {"reorder": True, "demote_below": 4, "promote_min": 4},
     {"reorder": True, "demote_below": 1000},
     {"promote_min": 1},                                   # every column on the tensor cores
+    {"engine": "block"},                                  # 128-row blocks, all tensor cores
+    {"engine": "block", "reorder": True},
+]
+
+BACKWARD_CANDIDATES = [
+    {"demote_below": 1000},                               # fused CUDA-core dB + dval
+    {"reorder": True, "demote_below": 1000},
+    {"engine": "block"},                                  # block dB, then the SDDMM
+    {"engine": "block", "reorder": True},
 ]
 
 
@@ -48,9 +65,10 @@ def cache_path():
                                        "autotune.json"))
 
 
-def cache_key(device_name, k, nnz, n_rows, transpose):
+def cache_key(device_name, k, nnz, n_rows, transpose, backward=False):
     b = lambda x: int(round(math.log2(max(int(x), 1))))
-    return f"{device_name}|K{int(k)}|nnz2^{b(nnz)}|rows2^{b(n_rows)}|{'adj' if transpose else 'fwd'}"
+    kind = "bwd" if backward else ("adj" if transpose else "fwd")
+    return f"{device_name}|K{int(k)}|nnz2^{b(nnz)}|rows2^{b(n_rows)}|{kind}"
 
 
 def _load_cache(path):
@@ -73,27 +91,41 @@ def _store_cache(path, data):
 
 
 def tune(indptr, indices, values, n_rows, n_cols, k, device="cuda", candidates=None,
-         transpose=False, row_scale=False, reps=5, use_cache=True, flush_mb=256):
+         transpose=False, row_scale=False, reps=5, use_cache=True, flush_mb=256,
+         backward=False):
     """Time each candidate's routed product at feature width k on `device`
     (L2 flushed before every timed launch, median of `reps`) and return
     (best_options, report).  report = {"key", "cached", "results": [...]} with
-    per candidate its options, median ms, plan build seconds and plan info."""
+    per candidate its options, median ms, plan build seconds and plan info.
+    backward=True times the adjoint plan's whole backward (dB and the values'
+    gradient, Plan.adjoint_sddmm) over BACKWARD_CANDIDATES."""
     import torch
     dev = torch.device(device)
     name = torch.cuda.get_device_name(dev)
     nnz = int(np.asarray(indices).shape[0])
-    key = cache_key(name, k, nnz, n_rows, transpose)
+    if backward:
+        transpose = True
+    key = cache_key(name, k, nnz, n_rows, transpose, backward)
     path = cache_path()
     cache = _load_cache(path) if use_cache else {}
     if use_cache and key in cache:
         return dict(cache[key]["best"]), {"key": key, "cached": True,
                                           "results": cache[key].get("results", [])}
-    cands = CANDIDATES if candidates is None else candidates
+    if candidates is not None:
+        cands = candidates
+    else:
+        cands = BACKWARD_CANDIDATES if backward else CANDIDATES
     rows_b = n_cols if transpose else n_rows
     cols_b = n_rows if transpose else n_cols
     rng = np.random.default_rng(0)
     b = torch.from_numpy(rng.standard_normal((cols_b, k)).astype(np.float16)).to(dev)
     out = torch.empty((rows_b, k), dtype=torch.float32, device=dev)
+    if backward:
+        # the backward reads B [A cols, K] besides dC [A rows, K] (= b above)
+        bb = torch.from_numpy(rng.standard_normal((n_cols, k)).astype(np.float16)).to(dev)
+        ip = torch.from_numpy(np.ascontiguousarray(indptr, dtype=np.int32)).to(dev)
+        ix = torch.from_numpy(np.ascontiguousarray(indices, dtype=np.int32)).to(dev)
+        dval = torch.empty(nnz, dtype=torch.float32, device=dev)
     flush = torch.empty(flush_mb * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     results = []
     for opts in cands:
@@ -101,15 +133,21 @@ def tune(indptr, indices, values, n_rows, n_cols, k, device="cuda", candidates=N
         plan = Plan.build(indptr, indices, values, n_rows, n_cols, transpose=transpose,
                           row_scale=row_scale, **opts)
         build_s = time.perf_counter() - t0
+        if backward:
+            def run():
+                plan.adjoint_sddmm(ip, ix, b, bb, db=out, dval=dval)
+        else:
+            def run():
+                plan.spmm(b, out=out)
         for _ in range(2):
-            plan.spmm(b, out=out)
+            run()
         ts = []
         for _ in range(reps):
             flush.fill_(1.0)
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-            plan.spmm(b, out=out)
+            run()
             e1.record()
             torch.cuda.synchronize()
             ts.append(e0.elapsed_time(e1))
