@@ -12,7 +12,10 @@ built once) and dval = SDDMM(dC, B) on A's pattern (the edge-weight
 gradient), the last two in one fused pass over A^T where the plan allows;
 FP16 operands, FP32 accumulation and outputs, dC a fixed synthetic FP16
 gradient.  Plans are built once, outside the timed region, with the plan
-options the autotuner (trspmm.autotune) finds fastest for this graph.
+options the autotuner (trspmm.autotune) finds fastest for this graph: for
+the forward among the window engine's routings and the block engine
+(tcgen05 over 128-row blocks of label-ordered rows), for the adjoint the
+fastest whole backward.
 Between timed steps a 256 MiB buffer is written to flush L2 (126 MB); each
 step is timed alone with CUDA events on its stream.
 
@@ -25,17 +28,20 @@ step is timed alone with CUDA events on its stream.
   roofline    the dominant kernel against the measured HBM copy bandwidth:
               the fused backward (one launch: dB = A^T dC and dval) with
               algorithmic bytes per launch = nnz*(4+2+4+4) + (N+1)*4 + M*K*2
-              + N*K*2 + N*K*4, or, when the backward is not fused or is the
-              shorter pass, the forward's CUDA-core residual pass with
-              res_nnz*(4+2) + (M+1)*4 + N*K*2 + M*K*4 (that one is also
-              reported in extra.forward_residual_roofline)
+              + N*K*2 + N*K*4, or, when the forward's kernel is the longer
+              one, the block-engine forward (or the window engine's CUDA-core
+              residual pass) with nnz*(4+2) + (M+1)*4 + N*K*2 + M*K*4 (CSR
+              bytes: the layout's padding and metadata count against it);
+              extra.forward_roofline reports the forward either way
   cpu_baseline / --impl reference: the oracle's C restatement of the same
               step (FP16 operands, FP32 accumulation, OpenMP on all host cores);
               extra.cpu_torch_sparse_forward: the forward alone with
               torch.sparse CSR (FP32) on all host cores
   extra       the same step with the plain single-route CSR kernel (forward on
-              A, adjoint on a CSR of A^T, same SDDMM), per-pass times and the
-              autotuner's table
+              A, adjoint on a CSR of A^T, same SDDMM), and like for like:
+              the forward against the plain CSR kernel, the backward against
+              the same fused pass over a natural-order CSR of A^T, and the
+              step at equal fusion; per-pass times and the autotuner's tables
 
 Multi-GPU: the path does not shard (replicas only); under torchrun every rank
 runs the full workload independently and rank 0 reports max-over-ranks time.
@@ -230,14 +236,18 @@ class CpuStep:
 
 def batched_comparison(dev, flush, n_graphs=512, k=64, reps=20):
     """The batched workload: 512 power-law graphs (20-500 nodes, degree
-    4-32), forward + fused backward at K=64.  One block-diagonal plan pair,
-    the step captured in a CUDA graph, vs one plan pair per graph launched in
-    a loop (eagerly from Python, and the same loop captured in a graph)."""
+    4-32), forward (block engine) + fused backward at K=64.  One
+    block-diagonal plan pair, the step captured in a CUDA graph, vs one plan
+    pair per graph launched in a loop (eagerly from Python, and the same loop
+    captured in a graph), with the same plan options."""
     import torch
     from trspmm import graphs
     from trspmm.batched import BatchedStep, PerGraphLoop
     g = graphs.batched(num_graphs=n_graphs)
-    opts = dict(demote_below=1000, promote_min=0, row_scale=True)
+    # block-engine forward (the small graphs' rows share columns within a
+    # block), fused CUDA-core backward
+    opts = dict(engine="block", promote_min=0, row_scale=True,
+                adjoint_options={"demote_below": 1000})
     bs = BatchedStep(g, k, device=dev, **opts)
     loop = PerGraphLoop(g, k, device=dev, **opts)
     b = torch.from_numpy(graphs.dense_features(g.n_cols, k, seed=1)).to(dev)
@@ -476,13 +486,16 @@ def main():
     plain_bwd_ms = float(np.mean(timed(
         lambda: plain_adj.adjoint_sddmm(ip, ix, dcd, bd, db=db2, dval=dv2), n_side, 3)))
     plain_adj.close()
-    # the same forward with the features in FP32 (FP32-feature route, same plan)
+    # the same forward with the features in FP32 (FP32-feature route, CUDA
+    # cores; a window plan, the block engine's FP32 kernel being a fallback)
+    pf32 = pf if pf.info["engine"] == trspmm.TR_ENGINE_WINDOW else trspmm.Plan.build(
+        g.indptr, g.indices, g.values, g.n_rows, g.n_cols, row_scale=True, demote_below=1000)
     b32 = bd.float()
     c3 = torch.empty_like(cd)
-    f32_ms = float(np.mean(timed(lambda: pf.spmm(b32, out=c3), n_side, 3)))
+    f32_ms = float(np.mean(timed(lambda: pf32.spmm(b32, out=c3), n_side, 3)))
     routed_step()
     plain_step()
-    pf.spmm(b32, out=c3)
+    pf32.spmm(b32, out=c3)
     torch.cuda.synchronize()
     rel = lambda a_, b_: float((a_ - b_).abs().max().item() / max(b_.abs().max().item(), 1e-30))
     err = {"C": rel(cd, c2), "dB": rel(dbd, db2), "dval": rel(dvd, dv2)}

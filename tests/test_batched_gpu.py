@@ -79,3 +79,36 @@ def test_batched_graph_replay_equals_eager(cuda):
     # shared-memory atomics, so the last bits may differ from run to run
     for x, y in zip((bs.c, bs.db, bs.dval), ref):
         assert rel_err(x.cpu().numpy(), y.cpu().numpy()) <= 1e-6
+
+
+@pytest.mark.parametrize("opts", [dict(demote_below=1000, promote_min=0, row_scale=True),
+                                  dict(engine="block", promote_min=0, row_scale=True,
+                                       adjoint_options={"demote_below": 1000})])
+def test_batched_all_512_graphs_fp64(cuda, opts):
+    """The batched workload at full size: 512 power-law graphs (20-500
+    nodes, mean degree 4-32), K = 64, forward and backward of the whole
+    batch in one plan pair, against FP64 (every entry and row)."""
+    g = graphs.batched(num_graphs=512)
+    bs = BatchedStep(g, 64, device=cuda, **opts)
+    b = graphs.dense_features(g.n_cols, 64, seed=1)
+    dc = graphs.dense_features(g.n_rows, 64, seed=2)
+    bs.b.copy_(torch.from_numpy(b))
+    bs.dc.copy_(torch.from_numpy(dc))
+    bs.run()
+    torch.cuda.synchronize()
+    v = np.asarray(g.values, np.float32)
+    rows = np.repeat(np.arange(g.n_rows), np.diff(g.indptr))
+    s = np.zeros(g.n_rows, np.float32)
+    np.maximum.at(s, rows, np.abs(v))
+    s[s == 0] = 1
+    A16 = sp.csr_matrix(((v / s[rows]).astype(np.float16).astype(np.float64) * s[rows],
+                         g.indices, g.indptr), shape=(g.n_rows, g.n_cols))
+    st_ = np.zeros(g.n_cols, np.float32)
+    np.maximum.at(st_, g.indices, np.abs(v))
+    st_[st_ == 0] = 1
+    AT16 = sp.csr_matrix(((v / st_[g.indices]).astype(np.float16).astype(np.float64)
+                          * st_[g.indices], g.indices, g.indptr), shape=A16.shape).T
+    assert rel_err(bs.c.cpu().numpy(), A16 @ b.astype(np.float64)) <= 1e-4
+    assert rel_err(bs.db.cpu().numpy(), AT16 @ dc.astype(np.float64)) <= 1e-4
+    dv_ref = oracle.sddmm_f64(g.indptr, g.indices, dc.astype(np.float64), b.astype(np.float64))
+    assert rel_err(bs.dval.cpu().numpy(), dv_ref) <= 1e-5

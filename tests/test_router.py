@@ -161,3 +161,16 @@ def test_router_matches_compiled_reference_midsize():
     a = trspmm.route(g.indptr, g.indices, g.values)
     b = oracle.ref_route(g.indptr, g.indices, g.values, 32, 32, 3, 8, 16, 16, 0.0, 0.5, 12)
     _same(a, b)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference router not compiled here")
+def test_router_matches_compiled_reference_route_mix_full_size():
+    """The route-mix stress matrix at its full size (65,536 rows, ~3.2M
+    entries: dense 16x8 blocks on a band, 2:4-compatible rows, uniform
+    scatter): all 29 tables bit for bit against the reference's router
+    compiled from its own source."""
+    g = graphs.route_mix(n=65_536, target_nnz=3_200_000, seed=3)
+    assert g.nnz > 3_000_000
+    a = trspmm.route(g.indptr, g.indices, g.values, mode="compat")
+    b = oracle.ref_route(g.indptr, g.indices, g.values, 32, 32, 3, 8, 16, 16, 0.0, 0.5, 12)
+    _same(a, b)

@@ -11,9 +11,9 @@
 //
 // One persistent CTA per SM takes its blocks from the plan's schedule
 // (longest-processing-time assignment made at upload) as one stream of
-// chunks.  Every block holds a whole number of groups of four chunks (the
-// layout pads it with chunks that have no entries); the four stage slots of
-// a group share one full and one empty barrier.  Roles:
+// chunks.  Every block holds a whole number of groups of eight chunks (the
+// layout pads it with chunks that have no entries); the eight stage slots
+// of a group share one full and one empty barrier.  Roles:
 //
 //   producer warps (kProd of them, two stage slots each, on the schedulers
 //   the MMA warp does not use; chunk q of the stream taken by producer
@@ -35,7 +35,7 @@
 //   epilogue warp 0)
 //       per group: wait full, one proxy fence (the operands were written
 //       through the generic proxy; the tensor core reads them through the
-//       async proxy), four tcgen05.mma (M = 128, N = K, K = 16) into the
+//       async proxy), eight tcgen05.mma (M = 128, N = K, K = 16) into the
 //       block's accumulator, one commit to the group's empty barrier; after
 //       a block's last group a commit to the accumulator's full barrier.
 //       The loop is straight-line per group (stage descriptors are base +
@@ -466,9 +466,9 @@ __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
           tc_fence_after();
           const uint64_t off = (uint64_t)(gs * kGroup) * kStep;
           umma_f16(d, adesc0 + off, bdesc0 + off, idesc, t > 0 ? 1u : 0u);
-          umma_f16(d, adesc0 + off + kStep, bdesc0 + off + kStep, idesc, 1u);
-          umma_f16(d, adesc0 + off + 2 * kStep, bdesc0 + off + 2 * kStep, idesc, 1u);
-          umma_f16(d, adesc0 + off + 3 * kStep, bdesc0 + off + 3 * kStep, idesc, 1u);
+#pragma unroll
+          for (int j = 1; j < kGroup; ++j)
+            umma_f16(d, adesc0 + off + j * kStep, bdesc0 + off + j * kStep, idesc, 1u);
           umma_commit(smem_u32(&empty[gs]));
           if (++gs == NG) {
             gs = 0;

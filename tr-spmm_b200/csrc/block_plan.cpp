@@ -73,8 +73,8 @@ void lay_out_block(const Csr& a, int32_t b, const std::vector<float>& scale, Blo
     next += layers;
     i = j;
   }
-  // whole groups of kChunkGroup chunks per block (the kernel issues a
-  // group's MMAs together); padding chunks have no entries and no columns
+  // whole groups of kChunkGroup chunks per block (the kernel waits for and
+  // issues a group's MMAs together); padding chunks have no entries and no columns
   const int32_t n_chunks =
       (next + kChunkCols * kChunkGroup - 1) / (kChunkCols * kChunkGroup) * kChunkGroup;
   out.col.assign((size_t)n_chunks * kChunkCols, -1);

@@ -32,7 +32,7 @@
 // gathered once per block and multiplied by the tensor cores against all 128
 // rows at once (tcgen05.mma M = 128 rows, N = K features, K = 16 slots):
 //   blk_chunk[NB+1]  chunks of block b: [blk_chunk[b], blk_chunk[b+1]), a
-//                    multiple of 4 (trailing chunks without entries pad it)
+//                    multiple of 8 (trailing chunks without entries pad it)
 //   chunk_col[NC*16] row of B gathered into each slot of a chunk (-1: none)
 //   chunk_ent[NC+1]  entries of chunk c: [chunk_ent[c], chunk_ent[c+1])
 //   ent_pos[E]       byte offset of the entry in the chunk's 128x16 FP16 A
@@ -107,7 +107,7 @@ struct HostPlan {
 // group (every block holds a whole number of groups).
 constexpr int kBlkRows = 128;
 constexpr int kChunkCols = 16;
-constexpr int kChunkGroup = 4;
+constexpr int kChunkGroup = 8;
 
 // A CSR matrix on its way through the builder; src[e] is the entry of the
 // caller's A behind entry e.

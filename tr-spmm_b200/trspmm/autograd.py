@@ -40,9 +40,9 @@ class RoutedAdjacency:
         graph.  features: "f16" (FP16 operands) or "f32" (FP32 features on
         the FP32-feature route).  The other keywords shape both plans
         (Plan.build: engine, demote_below, promote_min, reorder, ...);
-        adjoint_options (a dict) overrides them for the adjoint plan alone,
-        e.g. a block-engine forward with the fused CUDA-core backward
-        (engine="window", demote_below=1000)."""
+        adjoint_options (a dict of the same keywords) replaces them for the
+        adjoint plan, e.g. a block-engine forward with the fused CUDA-core
+        backward ({"demote_below": 1000}); row_scale applies to both."""
         if features not in ("f16", "f32"):
             raise ValueError(f"features must be 'f16' or 'f32', not {features!r}")
         self.features = features
@@ -52,7 +52,7 @@ class RoutedAdjacency:
         self.n_rows, self.n_cols = int(n_rows), int(n_cols)
         self.nnz = int(indices.size)
         kw = dict(row_scale=row_scale, promote_min=promote_min, reorder=reorder, **route_kw)
-        akw = dict(kw, **(adjoint_options or {}))
+        akw = kw if adjoint_options is None else dict(row_scale=row_scale, **adjoint_options)
         if plan_cache:
             from .plan_cache import cached_plan
             d = None if plan_cache is True else str(plan_cache)
