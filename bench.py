@@ -154,11 +154,17 @@ def algorithmic_bytes(nnz, m, n_cols, k, out_bytes=4):
     return nnz * (4 + 2) + (m + 1) * 4 + n_cols * k * 2 + m * k * out_bytes
 
 
-def adjoint_sddmm_bytes(nnz, m, n, k, out_bytes=4):
-    """Fused backward over A^T (n rows): per entry its column, value, entry
-    id and dval (4+2+4+4 bytes); dC (m x k FP16) and B (n x k FP16) read
-    once; dB (n x k) written once."""
-    return nnz * (4 + 2 + 4 + 4) + (n + 1) * 4 + m * k * 2 + n * k * 2 + n * k * out_bytes
+def adjoint_sddmm_bytes(nnz, m, n, k, out_bytes=4, entry_ids=False):
+    """Fused backward over A^T (n rows): per entry its column, value and dval
+    (4+2+4 bytes; plus a 4-byte entry id when dval is stored through one);
+    dC (m x k FP16) and B (n x k FP16) read once; dB (n x k) written once."""
+    per = 4 + 2 + 4 + (4 if entry_ids else 0)
+    return nnz * per + (n + 1) * 4 + m * k * 2 + n * k * 2 + n * k * out_bytes
+
+
+def _single_stream(adj_opts):
+    """An all-residual window adjoint plan (its entries form one stream)."""
+    return adj_opts.get("engine", "window") == "window" and adj_opts.get("demote_below", 0) >= 1000
 
 
 def step_bytes(nnz, m, n, k):
@@ -407,9 +413,12 @@ def main():
                                                  backward=True)
     tune_s = time.perf_counter() - t0
     t0 = time.perf_counter()
+    # per-entry arrays (the values and dval) in the adjoint plan's entry order
+    # where it has one, so that the backward stores dval sequentially
+    edge_order = "adjoint" if _single_stream(adj_opts) else "csr"
     adj = RoutedAdjacency(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, device=dev,
                           row_scale=True, adjoint_options={"promote_min": 0, **adj_opts},
-                          **{"promote_min": 0, **opts})
+                          edge_order=edge_order, **{"promote_min": 0, **opts})
     plan_s = time.perf_counter() - t0
     pf, pa = adj.fwd, adj.adj
 
@@ -483,6 +492,8 @@ def main():
     # in natural order (no reordering, no tiles: the plain single route)
     plain_adj = trspmm.Plan.build(g.indptr, g.indices, g.values, g.n_rows, g.n_cols,
                                   transpose=True, row_scale=True, demote_below=1000)
+    if adj.edge_id is not None:
+        plain_adj.renumber_edges(adj.edge_id)     # dval in the same order as the routed arm
     plain_bwd_ms = float(np.mean(timed(
         lambda: plain_adj.adjoint_sddmm(ip, ix, dcd, bd, db=db2, dval=dv2), n_side, 3)))
     plain_adj.close()
@@ -498,7 +509,7 @@ def main():
     pf32.spmm(b32, out=c3)
     torch.cuda.synchronize()
     rel = lambda a_, b_: float((a_ - b_).abs().max().item() / max(b_.abs().max().item(), 1e-30))
-    err = {"C": rel(cd, c2), "dB": rel(dbd, db2), "dval": rel(dvd, dv2)}
+    err = {"C": rel(cd, c2), "dB": rel(dbd, db2), "dval": rel(adj.to_csr_order(dvd), dv2)}
     fp32_route = {"ms": f32_ms, "tflops": 2.0 * g.nnz * k / (f32_ms * 1e-3) / 1e12,
                   "max_rel_diff_vs_fp16_features": rel(c3, cd)}
     del b32, c3
@@ -513,7 +524,7 @@ def main():
     # the first upload to the last download.
     b_host = torch.from_numpy(b).pin_memory()
     dc_host = torch.from_numpy(dc).pin_memory()
-    w_dev = torch.from_numpy(g.values.astype(np.float32)).to(dev)
+    w_dev = adj.values.clone()                  # the adjacency's edge order
     c_host = [torch.empty((g.n_rows, k), dtype=torch.float32).pin_memory() for _ in range(2)]
     db_host = [torch.empty((g.n_cols, k), dtype=torch.float16).pin_memory() for _ in range(2)]
     dw_host = [torch.empty(g.nnz, dtype=torch.float32).pin_memory() for _ in range(2)]
@@ -624,7 +635,7 @@ def main():
     fwd_kernel_ms = fwd_ms if fwd_block else res_ms
     if fused_bwd and adj_sddmm_ms >= fwd_kernel_ms:
         dom_kernel = "seg_adjoint_sddmm_kernel (fused backward: dB = A^T dC, dval = SDDMM)"
-        abytes = adjoint_sddmm_bytes(g.nnz, g.n_rows, g.n_cols, k)
+        abytes = adjoint_sddmm_bytes(g.nnz, g.n_rows, g.n_cols, k, entry_ids=adj.edge_id is None)
         achieved = abytes / (adj_sddmm_ms * 1e-3) / 1e9
         traffic = _profile_traffic("seg_adjoint_sddmm_large_routed.txt")
     elif fwd_block:
@@ -646,7 +657,9 @@ def main():
                        "step": "forward + adjoint + SDDMM", "out": "f32",
                        "l2": "flushed between steps (256 MiB write)",
                        "parallelism": f"replicas{world}", "plan_options": opts,
-                       "adjoint_plan_options": adj_opts},
+                       "adjoint_plan_options": adj_opts,
+                       "edge_order": ("adjoint plan entry order (A^T CSR)" if adj.edge_id is not None
+                                      else "A CSR order")},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind, "algorithmic_bytes": abytes,

@@ -125,11 +125,11 @@ int tr_route_tc_device(const int32_t* d_indptr, const int32_t* d_indices, const 
  * windows), at most 2048 entries in any 16-row window (use
  * tr_route_tc_device beyond that), capacities large enough for the tables.
  * The first call on a device takes the array's device address and sets the
- * kernels' shared-memory limit; make that first call before any stream
- * capture.  All calls share the array: calls that overlap on the GPU race
- * (run them on one stream, one after another).  The call waits for
- * `stream` before returning (it reads four status words back).  No
- * counterpart in the reference. */
+ * kernels' shared-memory limit.  All calls share the array: calls that
+ * overlap on the GPU race (run them on one stream, one after another).  The
+ * call waits for `stream` before returning (it reads four status words
+ * back), so no call can be captured into a CUDA graph.  No counterpart in
+ * the reference. */
 int tr_route_tc_device_noalloc(const int32_t* d_indptr, const int32_t* d_indices,
                                const float* d_values, int32_t n_rows,
                                const tr_route_params* params, int32_t* t_column,
@@ -214,6 +214,7 @@ typedef struct tr_plan_info {
   int32_t engine;          /* TR_ENGINE_WINDOW or TR_ENGINE_BLOCK */
   int32_t n_blocks;        /* 128-row blocks (block engine) */
   int64_t chunks;          /* 16-column chunks = tensor-core MMAs per product (block engine) */
+  int64_t n_edges;         /* edges (per-entry values) the plan addresses: A's CSR entries */
 } tr_plan_info;
 
 /* Host route tables (pointer + element count each), in the reference's
@@ -388,6 +389,26 @@ int tr_spmm_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int 
  * Used for learnable edge weights (the forward and the adjoint plan of the
  * same A take the same array). */
 int tr_plan_set_values(tr_plan* p, const float* values, int64_t n_edges, void* stream);
+
+/* Edge numbering.  Every per-entry array a plan reads or writes
+ * (tr_plan_set_values' values, tr_adjoint_sddmm's dval) is indexed by edge
+ * number; edges start numbered as A's CSR entries.
+ *
+ * tr_plan_entry_order writes order[q] = the edge at plan position q (device
+ * array of n_edges; -1 where no edge sits), for plans whose entries form one
+ * stream: block-engine plans and window plans without tensor-core tiles
+ * (otherwise TR_ERR_UNSUPPORTED).  An all-residual adjoint plan's positions
+ * are A^T's CSR order.
+ *
+ * tr_plan_renumber_edges gives A's edges new numbers: new_id[e] (device,
+ * n_edges, a permutation — refused with TR_ERR_ARG otherwise) becomes the
+ * number of the edge now numbered e.  Numbering both plans of one A by the
+ * adjoint plan's entry order (new_id[order[q]] = q) makes the adjoint's value
+ * upload and the fused backward's dval stores sequential.  Synchronises
+ * `stream`; not capturable.  No reference counterpart: the reference keeps
+ * no per-entry arrays on the device. */
+int tr_plan_entry_order(const tr_plan* p, int32_t* order, void* stream);
+int tr_plan_renumber_edges(tr_plan* p, const int32_t* new_id, int64_t n_edges, void* stream);
 
 /* The backward of C = A(w) . B in one call: dB = A^T . dC through the
  * adjoint plan (built with opts.transpose), and dval = SDDMM(dC, B) on A's

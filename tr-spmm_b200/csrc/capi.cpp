@@ -428,6 +428,7 @@ int tr_plan_info_get(const tr_plan* p, tr_plan_info* info) {
 void tr_plan_free(tr_plan* p) {
   if (!p) return;
   if (p->block) cudaFree(p->block);
+  if (p->edge_id) cudaFree(p->edge_id);
   delete p;
 }
 
@@ -499,6 +500,19 @@ int tr_plan_set_values(tr_plan* p, const float* values, int64_t n_edges, void* s
   return launch_set_values(p, values, (cudaStream_t)stream);
 }
 
+int tr_plan_entry_order(const tr_plan* p, int32_t* order, void* stream) {
+  if (!p) return fail(TR_ERR_ARG, "null plan");
+  if (p->n_edges > 0 && !order) return fail(TR_ERR_ARG, "null device pointer");
+  return launch_entry_order(p, order, (cudaStream_t)stream);
+}
+
+int tr_plan_renumber_edges(tr_plan* p, const int32_t* new_id, int64_t n_edges, void* stream) {
+  if (!p) return fail(TR_ERR_ARG, "null plan");
+  if (n_edges != p->n_edges) return fail(TR_ERR_ARG, "n_edges must equal the plan's edge count");
+  if (n_edges > 0 && !new_id) return fail(TR_ERR_ARG, "null device pointer");
+  return launch_renumber_edges(p, new_id, (cudaStream_t)stream);
+}
+
 int tr_adjoint_sddmm(const tr_plan* adj, const int32_t* a_indptr, const int32_t* a_indices,
                      int32_t a_rows, int64_t nnz, const uint16_t* dc, const uint16_t* b, int32_t k,
                      void* db, int db_dtype, float* dval, void* stream) {
@@ -511,7 +525,8 @@ int tr_adjoint_sddmm(const tr_plan* adj, const int32_t* a_indptr, const int32_t*
   if (adj->blocked) {
     int rc = launch_block(adj, dc, k, db, db_dtype, false, (cudaStream_t)stream);
     if (rc) return rc;
-    return launch_sddmm(a_indptr, a_indices, a_rows, nnz, dc, b, k, dval, (cudaStream_t)stream);
+    return launch_sddmm(a_indptr, a_indices, a_rows, nnz, dc, b, k, dval, (cudaStream_t)stream,
+                        adj->edge_id);
   }
   return launch_adjoint_sddmm(adj, a_indptr, a_indices, a_rows, nnz, dc, b, k, db, db_dtype, dval,
                               (cudaStream_t)stream);
@@ -529,7 +544,8 @@ int tr_adjoint_sddmm_f32(const tr_plan* adj, const int32_t* a_indptr, const int3
   if (adj->blocked) {
     int rc = launch_block_f32(adj, dc, k, db, db_dtype, (cudaStream_t)stream);
     if (rc) return rc;
-    return launch_sddmm_f32(a_indptr, a_indices, a_rows, nnz, dc, b, k, dval, (cudaStream_t)stream);
+    return launch_sddmm_f32(a_indptr, a_indices, a_rows, nnz, dc, b, k, dval, (cudaStream_t)stream,
+                            adj->edge_id);
   }
   return launch_adjoint_sddmm_f32(adj, a_indptr, a_indices, a_rows, nnz, dc, b, k, db, db_dtype,
                                   dval, (cudaStream_t)stream);

@@ -773,6 +773,7 @@ int plan_upload(const HostPlan& hp, tr_plan** out) {
   p->info.n_blocks = v.n_blocks;
   p->info.chunks = hp.block ? (int64_t)hp.blk_chunk.back() : 0;
   if (hp.block) p->info.residual_nnz = 0;
+  p->info.n_edges = n_edges;
   *out = p;
   return TR_OK;
 }

@@ -135,6 +135,12 @@ struct tr_plan {
   bool row_scaled = false;
   bool blocked = false;         // block layout (the block engine)
   int32_t max_sched_blocks = 0; // most blocks any CTA of the block schedule takes
+  // Edge numbering.  Edges start numbered as A's CSR entries; after
+  // tr_plan_renumber_edges, val_slot / edge_row / res_edge / ent_src use the
+  // caller's numbering and edge_id[e] (own allocation) is the current number
+  // of A's CSR entry e (the SDDMM over A's CSR writes through it).
+  int32_t* edge_id = nullptr;
+  bool res_edge_identity = false; // res_edge[q] == q: the fused backward skips it
   tr_plan_info info{};
 };
 

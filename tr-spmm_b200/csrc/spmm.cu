@@ -854,7 +854,8 @@ __global__ void __launch_bounds__(256) sddmm_kernel(const int32_t* __restrict__ 
                                                     const int32_t* __restrict__ indices, int M,
                                                     const TB* __restrict__ X,
                                                     const TB* __restrict__ Y, int K,
-                                                    float* __restrict__ out) {
+                                                    float* __restrict__ out,
+                                                    const int32_t* __restrict__ out_id) {
   const int lane = threadIdx.x & 31;
   const int nchunk = K / SegFeat<TB>::kPer;
   int L = 1;
@@ -872,7 +873,7 @@ __global__ void __launch_bounds__(256) sddmm_kernel(const int32_t* __restrict__ 
         for (int c = li; c < nchunk; c += L) acc += dot_chunk(__ldg(xr + c), __ldg(yr + c), TB());
       }
       for (int off = 1; off < L; off <<= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
-      if (li == 0 && e < e1) out[e] = acc;
+      if (li == 0 && e < e1) out[out_id ? out_id[e] : e] = acc;
     }
   }
 }
@@ -894,7 +895,8 @@ __global__ void __launch_bounds__(256) sddmm_group_kernel(const int32_t* __restr
                                                           const int32_t* __restrict__ indices,
                                                           int M, const TB* __restrict__ X,
                                                           const TB* __restrict__ Y,
-                                                          float* __restrict__ out) {
+                                                          float* __restrict__ out,
+                                                          const int32_t* __restrict__ out_id) {
   constexpr int K = L * CH * SegFeat<TB>::kPer, G = 32 / L, U = (L > 16 ? 16 : L) / CH;
   const int lane = threadIdx.x & 31, grp = lane / L, li = lane % L;
   const int warps = gridDim.x * (blockDim.x >> 5);
@@ -955,7 +957,7 @@ __global__ void __launch_bounds__(256) sddmm_group_kernel(const int32_t* __restr
         }
       }
       const int e = eb + (li % U);
-      if (li < U && e < e1) out[e] = v[0];
+      if (li < U && e < e1) out[out_id ? out_id[e] : e] = v[0];
     }
   }
 }
@@ -1051,7 +1053,8 @@ __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
     const int n = min(kStage, e_end - c0);
     __syncthreads();                         // previous chunk consumed, racc zeroed
     for (int i = tid; i < n; i += kThreads)
-      sent[i] = make_int4(__ldg(indices + c0 + i), (int)__ldg(v16 + c0 + i), __ldg(edges + c0 + i), 0);
+      sent[i] = make_int4(__ldg(indices + c0 + i), (int)__ldg(v16 + c0 + i),
+                          edges ? __ldg(edges + c0 + i) : c0 + i, 0);
     __syncthreads();
     const int seg = seg_len(n, groups);
     const int lo0 = q * seg;
@@ -1145,14 +1148,15 @@ template <class TB = __half>
 __global__ void sddmm_generic_kernel(const int32_t* __restrict__ indptr,
                                      const int32_t* __restrict__ indices, int M,
                                      const TB* __restrict__ X, const TB* __restrict__ Y,
-                                     int K, float* __restrict__ out) {
+                                     int K, float* __restrict__ out,
+                                     const int32_t* __restrict__ out_id) {
   for (int r = blockIdx.x; r < M; r += gridDim.x)
     for (int e = indptr[r] + threadIdx.x; e < indptr[r + 1]; e += blockDim.x) {
       const int64_t c = indices[e];
       float acc = 0.f;
       for (int f = 0; f < K; ++f)
         acc = fmaf(feat_f32(X[(int64_t)r * K + f]), feat_f32(Y[c * K + f]), acc);
-      out[e] = acc;
+      out[out_id ? out_id[e] : e] = acc;
     }
 }
 
@@ -1314,7 +1318,8 @@ int launch_routed_f32(const tr_plan* p, const float* b, int32_t k, void* c, int 
 }
 
 int launch_sddmm_f32(const int32_t* indptr, const int32_t* indices, int32_t m, int64_t nnz,
-                     const float* x, const float* y, int32_t k, float* out, cudaStream_t stream) {
+                     const float* x, const float* y, int32_t k, float* out, cudaStream_t stream,
+                     const int32_t* out_id) {
   if (m == 0 || nnz == 0) return TR_OK;
   if (k == 0) {
     TRS_CUDA(cudaMemsetAsync(out, 0, (size_t)nnz * 4, stream));
@@ -1323,16 +1328,16 @@ int launch_sddmm_f32(const int32_t* indptr, const int32_t* indices, int32_t m, i
   const bool vec = k % 4 == 0 && aligned16(x) && aligned16(y);
   const int blocks = (int)std::min<int64_t>(((int64_t)m + 7) / 8, 148 * 16);
   if (vec && k == 64) {
-    sddmm_group_kernel<16, 1, float><<<blocks, 256, 0, stream>>>(indptr, indices, m, x, y, out);
+    sddmm_group_kernel<16, 1, float><<<blocks, 256, 0, stream>>>(indptr, indices, m, x, y, out, out_id);
   } else if (vec && k == 128) {
-    sddmm_group_kernel<32, 1, float><<<blocks, 256, 0, stream>>>(indptr, indices, m, x, y, out);
+    sddmm_group_kernel<32, 1, float><<<blocks, 256, 0, stream>>>(indptr, indices, m, x, y, out, out_id);
   } else if (vec && k == 256) {
-    sddmm_group_kernel<32, 2, float><<<blocks, 256, 0, stream>>>(indptr, indices, m, x, y, out);
+    sddmm_group_kernel<32, 2, float><<<blocks, 256, 0, stream>>>(indptr, indices, m, x, y, out, out_id);
   } else if (vec) {
-    sddmm_kernel<float><<<blocks, 256, 0, stream>>>(indptr, indices, m, x, y, k, out);
+    sddmm_kernel<float><<<blocks, 256, 0, stream>>>(indptr, indices, m, x, y, k, out, out_id);
   } else {
     const int blocks = (int)std::min<int64_t>(m, 148 * 32);
-    sddmm_generic_kernel<float><<<blocks, 128, 0, stream>>>(indptr, indices, m, x, y, k, out);
+    sddmm_generic_kernel<float><<<blocks, 128, 0, stream>>>(indptr, indices, m, x, y, k, out, out_id);
   }
   TRS_CUDA(cudaGetLastError());
   return TR_OK;
@@ -1357,7 +1362,7 @@ int launch_set_values(tr_plan* p, const float* values, cudaStream_t stream) {
 
 int launch_sddmm(const int32_t* indptr, const int32_t* indices, int32_t m, int64_t nnz,
                  const uint16_t* x, const uint16_t* y, int32_t k, float* out,
-                 cudaStream_t stream) {
+                 cudaStream_t stream, const int32_t* out_id) {
   if (m == 0 || nnz == 0) return TR_OK;
   const __half* xh = reinterpret_cast<const __half*>(x);
   const __half* yh = reinterpret_cast<const __half*>(y);
@@ -1368,15 +1373,15 @@ int launch_sddmm(const int32_t* indptr, const int32_t* indices, int32_t m, int64
   const bool vec = k % 8 == 0 && aligned16(x) && aligned16(y);
   if (vec && (k == 64 || k == 128 || k == 256)) {
     const int blocks = (int)std::min<int64_t>(((int64_t)m + 7) / 8, 148 * 16);
-    if (k == 64) sddmm_group_kernel<8><<<blocks, 256, 0, stream>>>(indptr, indices, m, xh, yh, out);
-    else if (k == 128) sddmm_group_kernel<16><<<blocks, 256, 0, stream>>>(indptr, indices, m, xh, yh, out);
-    else sddmm_group_kernel<32><<<blocks, 256, 0, stream>>>(indptr, indices, m, xh, yh, out);
+    if (k == 64) sddmm_group_kernel<8><<<blocks, 256, 0, stream>>>(indptr, indices, m, xh, yh, out, out_id);
+    else if (k == 128) sddmm_group_kernel<16><<<blocks, 256, 0, stream>>>(indptr, indices, m, xh, yh, out, out_id);
+    else sddmm_group_kernel<32><<<blocks, 256, 0, stream>>>(indptr, indices, m, xh, yh, out, out_id);
   } else if (vec) {
     const int blocks = (int)std::min<int64_t>(((int64_t)m + 7) / 8, 148 * 16);
-    sddmm_kernel<<<blocks, 256, 0, stream>>>(indptr, indices, m, xh, yh, k, out);
+    sddmm_kernel<<<blocks, 256, 0, stream>>>(indptr, indices, m, xh, yh, k, out, out_id);
   } else {
     const int blocks = (int)std::min<int64_t>(m, 148 * 32);
-    sddmm_generic_kernel<<<blocks, 128, 0, stream>>>(indptr, indices, m, xh, yh, k, out);
+    sddmm_generic_kernel<<<blocks, 128, 0, stream>>>(indptr, indices, m, xh, yh, k, out, out_id);
   }
   TRS_CUDA(cudaGetLastError());
   return TR_OK;
@@ -1399,15 +1404,16 @@ int launch_adjoint_sddmm(const tr_plan* p, const int32_t* a_indptr, const int32_
   if (!fused) {
     int rc = launch_routed(p, dc, k, db, db_dtype, TR_ROUTE_ALL, stream);
     if (rc) return rc;
-    return launch_sddmm(a_indptr, a_indices, a_rows, nnz, dc, b, k, dval, stream);
+    return launch_sddmm(a_indptr, a_indices, a_rows, nnz, dc, b, k, dval, stream, p->edge_id);
   }
   const int rows = v.n_windows * kBlockRows;
+  const int32_t* edges = p->res_edge_identity ? nullptr : v.res_edge;
   const __half* g = reinterpret_cast<const __half*>(dc);
   const __half* h = reinterpret_cast<const __half*>(b);
   const __half* rv = reinterpret_cast<const __half*>(v.res_val);
 #define TRS_SEGADJ(F16, L, W)                                                             \
   seg_adjoint_sddmm_kernel<F16, L, W><<<v.n_windows, kThreads, 0, stream>>>(               \
-      v.res_ptr, v.res_col, rv, v.res_edge, rows, g, k, db, v.row_out, v.row_scale, h, dval,   \
+      v.res_ptr, v.res_col, rv, edges, rows, g, k, db, v.row_out, v.row_scale, h, dval,        \
       v.win_order)
   const bool wide = (int64_t)v.n_cols * k >= ((int64_t)1 << 31);
   if (k > 128) {
@@ -1440,13 +1446,14 @@ int launch_adjoint_sddmm_f32(const tr_plan* p, const int32_t* a_indptr, const in
   if (!fused) {
     int rc = launch_routed_f32(p, dc, k, db, db_dtype, TR_ROUTE_ALL, stream);
     if (rc) return rc;
-    return launch_sddmm_f32(a_indptr, a_indices, a_rows, nnz, dc, b, k, dval, stream);
+    return launch_sddmm_f32(a_indptr, a_indices, a_rows, nnz, dc, b, k, dval, stream, p->edge_id);
   }
   const int rows = v.n_windows * kBlockRows;
   const __half* rv = reinterpret_cast<const __half*>(v.res_val);
+  const int32_t* edges = p->res_edge_identity ? nullptr : v.res_edge;
 #define TRS_SEGADJ32(F16, L, W)                                                             \
   seg_adjoint_sddmm_kernel<F16, L, W, float><<<v.n_windows, kThreads, 0, stream>>>(          \
-      v.res_ptr, v.res_col, rv, v.res_edge, rows, dc, k, db, v.row_out, v.row_scale, b, dval,   \
+      v.res_ptr, v.res_col, rv, edges, rows, dc, k, db, v.row_out, v.row_scale, b, dval,        \
       v.win_order)
   const bool wide = (int64_t)v.n_cols * k >= ((int64_t)1 << 31);
   if (k > 64) {

@@ -34,7 +34,7 @@ class RoutedAdjacency:
 
     def __init__(self, indptr, indices, values, n_rows, n_cols, device="cuda",
                  row_scale=True, promote_min=2, reorder=False, plan_cache=None,
-                 features="f16", adjoint_options=None, **route_kw):
+                 features="f16", adjoint_options=None, edge_order="csr", **route_kw):
         """plan_cache: None builds both plans; True or a directory takes them
         from the on-disk plan cache (trspmm.plan_cache), routing once per
         graph.  features: "f16" (FP16 operands) or "f32" (FP32 features on
@@ -42,9 +42,18 @@ class RoutedAdjacency:
         (Plan.build: engine, demote_below, promote_min, reorder, ...);
         adjoint_options (a dict of the same keywords) replaces them for the
         adjoint plan, e.g. a block-engine forward with the fused CUDA-core
-        backward ({"demote_below": 1000}); row_scale applies to both."""
+        backward ({"demote_below": 1000}); row_scale applies to both.
+
+        edge_order: the order of every per-entry tensor (the values w, their
+        gradient, ``self.values``).  "csr": A's CSR order.  "adjoint": the
+        adjoint plan's entry order (A^T's CSR order for an all-residual
+        adjoint plan), which makes the backward's gradient stores and the
+        adjoint plan's value upload sequential; ``edge_id[e]`` is then the
+        position of A's CSR entry e, and to_edge_order / to_csr_order convert."""
         if features not in ("f16", "f32"):
             raise ValueError(f"features must be 'f16' or 'f32', not {features!r}")
+        if edge_order not in ("csr", "adjoint"):
+            raise ValueError(f"edge_order must be 'csr' or 'adjoint', not {edge_order!r}")
         self.features = features
         indptr = np.ascontiguousarray(indptr, dtype=np.int32)
         indices = np.ascontiguousarray(indices, dtype=np.int32)
@@ -65,6 +74,30 @@ class RoutedAdjacency:
         self.indptr = torch.from_numpy(indptr).to(self.device)
         self.indices = torch.from_numpy(indices).to(self.device)
         self.values = torch.from_numpy(values).to(self.device)
+        self.edge_id = None
+        if edge_order == "adjoint" and self.nnz:
+            order = self.adj.entry_order(self.device)
+            if bool((order < 0).any()):
+                raise ValueError("edge_order='adjoint' needs an adjoint plan that holds every entry")
+            new_id = torch.empty_like(order)
+            new_id[order.long()] = torch.arange(self.nnz, dtype=torch.int32, device=self.device)
+            self.fwd.renumber_edges(new_id)
+            self.adj.renumber_edges(new_id)
+            self.edge_id = new_id
+            self.values = self.to_edge_order(self.values)
+
+    def to_edge_order(self, x):
+        """A per-entry tensor in A's CSR order, rearranged into this
+        adjacency's edge order."""
+        if self.edge_id is None:
+            return x
+        out = torch.empty_like(x)
+        out[self.edge_id.long()] = x
+        return out
+
+    def to_csr_order(self, x):
+        """A per-entry tensor in this adjacency's edge order, in A's CSR order."""
+        return x if self.edge_id is None else x[self.edge_id.long()]
 
     def set_values(self, w):
         """Re-value both plans from FP32 entry values (CUDA tensor [nnz])."""
@@ -120,7 +153,7 @@ class RoutedSpMMFunction(torch.autograd.Function):
             if ctx.needs_input_grad[1]:
                 db = adj.adj.spmm(dc32, out_dtype=torch.float32).to(ctx.b_dtype)
             if ctx.has_w and ctx.needs_input_grad[0]:
-                dw = sddmm_csr(adj.indptr, adj.indices, dc32, b32)
+                dw = adj.to_edge_order(sddmm_csr(adj.indptr, adj.indices, dc32, b32))
             return dw, db, None
         w, b16, sb = ctx.saved_tensors
         if ctx.has_w:
@@ -146,7 +179,7 @@ class RoutedSpMMFunction(torch.autograd.Function):
                 db = db * sc
             db = db.to(ctx.b_dtype)
         if ctx.has_w and ctx.needs_input_grad[0]:
-            dw = sddmm_csr(adj.indptr, adj.indices, dc16, b16)
+            dw = adj.to_edge_order(sddmm_csr(adj.indptr, adj.indices, dc16, b16))
             if scale is not None:
                 dw = dw * scale
         return dw, db, None

@@ -280,6 +280,30 @@ class Plan:
         check(lib().tr_plan_set_values(self._h, ctypes.c_void_p(values.data_ptr()),
                                        int(values.numel()), ctypes.c_void_p(s)))
 
+    def entry_order(self, device=None, stream=None):
+        """The plan's entry order (tr_plan_entry_order): int32 CUDA tensor
+        ``order`` with order[q] = the edge at plan position q (-1 where no
+        edge sits).  Block-engine plans and window plans without tiles."""
+        import torch
+        dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        order = torch.empty(int(self.info["n_edges"]), dtype=torch.int32, device=dev)
+        s = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+        check(lib().tr_plan_entry_order(self._h, ctypes.c_void_p(order.data_ptr()), ctypes.c_void_p(s)))
+        return order
+
+    def renumber_edges(self, new_id, stream=None):
+        """Give the plan's edges new numbers (tr_plan_renumber_edges): the edge
+        now numbered e becomes new_id[e] (int32 CUDA permutation).  Afterwards
+        set_values takes, and adjoint_sddmm returns, per-entry arrays in the
+        new numbering."""
+        import torch
+        if not (new_id.is_cuda and new_id.dtype == torch.int32 and new_id.is_contiguous()
+                and new_id.dim() == 1):
+            raise RuntimeError("new_id must be a contiguous 1-D int32 CUDA tensor")
+        s = stream if stream is not None else torch.cuda.current_stream(new_id.device).cuda_stream
+        check(lib().tr_plan_renumber_edges(self._h, ctypes.c_void_p(new_id.data_ptr()),
+                                           int(new_id.numel()), ctypes.c_void_p(s)))
+
     def spmm(self, b, out=None, out_dtype=None, route_mask=TR_ROUTE_ALL, stream=None):
         """C = A_plan . B for a CUDA tensor B [n_cols, K]: FP16 B on the routed
         kernels (tensor-core tiles + CUDA-core residual), FP32 B on the
