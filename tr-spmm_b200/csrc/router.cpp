@@ -36,6 +36,7 @@
 #include <vector>
 
 #include "router.h"
+#include "unit_order.h"
 
 namespace trs {
 namespace {
@@ -96,7 +97,7 @@ struct Scratch {
   std::vector<int8_t> edge_row;
   std::vector<int> cand, tmp;
   std::vector<Unit> units;
-  std::vector<int> order, list_next, list_prev, sorted_units;
+  std::vector<int> order, list_next, list_prev, sorted_units, unit_nnz;
   std::vector<char> matched;
   std::vector<std::pair<int, int>> pairs;
   std::vector<int> unmatched;
@@ -263,10 +264,12 @@ void route_window(const int32_t* indptr, const int32_t* indices, const float* va
   for (auto& u : S.units) unit_odd |= u.vec & kOddBits;
   if (!unit_odd) {
     // Complete compatibility graph: all degrees equal nu-1, so the
-    // reference comparator reduces to nnz descending.  The same std::sort on
-    // the same outcomes yields the same (unstable) order.
-    std::sort(S.order.begin(), S.order.end(),
-              [&](int a, int b) { return S.units[a].nnz > S.units[b].nnz; });
+    // reference comparator reduces to nnz descending.  unit_order performs
+    // the reference's std::sort step for step (the device router runs the
+    // same function), so ties land where they land there.
+    S.unit_nnz.resize(nu);
+    for (int i = 0; i < nu; ++i) S.unit_nnz[i] = S.units[i].nnz;
+    unit_order(S.order.data(), nu, S.unit_nnz.data());
     // Units by (nnz desc, index asc) in a doubly linked list of the unmatched.
     int buckets[33] = {0};
     for (auto& u : S.units) buckets[u.nnz]++;
