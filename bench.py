@@ -173,6 +173,31 @@ def step_bytes(nnz, m, n, k):
     return algorithmic_bytes(nnz, m, n, k) + algorithmic_bytes(nnz, n, m, k) + sddmm
 
 
+def router_comparison(g):
+    """Seconds to route the graph (the reference's parameters, compat mode):
+    the host router on all host threads, and the device router with the CSR
+    already on the device (tables brought back to the host); both produce
+    the same 29 tables."""
+    import torch
+    import trspmm
+    host = trspmm.route(g.indptr, g.indices, g.values)
+    d = [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (g.indptr, g.indices, g.values)]
+    trspmm.route_device(*d, out="torch")      # first call: module load, shared-memory limits
+    t0 = time.perf_counter()
+    dev = trspmm.route_device(*d, out="torch")
+    torch.cuda.synchronize()
+    dev_s = time.perf_counter() - t0
+    same = all(np.array_equal(a, b.cpu().numpy().reshape(a.shape)) for a, b in zip(host[:29], dev[:29]))
+    t0 = time.perf_counter()
+    trspmm.route_device(*d)                   # the same with every table copied to the host
+    dev_host_s = time.perf_counter() - t0
+    return {"host": float(host[-1]), "device": float(dev[-1]), "device_api_s": dev_s,
+            "device_with_host_copies_s": dev_host_s, "tables_equal": bool(same),
+            "host_threads": os.cpu_count(),
+            "note": "host: the host router on all threads, tables in host memory; device: "
+                    "the device router, tables left on the device (the GPU kernels' input)"}
+
+
 def transpose_csr(indptr, indices, values, n_rows, n_cols):
     import scipy.sparse as sp
     a = sp.csr_matrix((values, indices, indptr), shape=(n_rows, n_cols)).T.tocsr()
@@ -618,6 +643,7 @@ def main():
     batched = None
     if rank == 0 and not args.no_batched:
         batched = batched_comparison(dev, flush)
+    router = router_comparison(g) if rank == 0 else None
 
     def launches(p):
         info = p.info
@@ -698,7 +724,7 @@ def main():
                       "step_algorithmic_bytes": sbytes,
                       "step_hbm_gbs": sbytes / (ms * 1e-3) / 1e9,
                       "step_hbm_frac": sbytes / (ms * 1e-3) / 1e9 / peak,
-                      "plan_build_s": plan_s, "tune_s": tune_s,
+                      "plan_build_s": plan_s, "tune_s": tune_s, "router_s": router,
                       "autotune": [{"options": r["options"], "ms": r["ms"]}
                                    for r in tune_report.get("results", [])],
                       "autotune_backward": [{"options": r["options"], "ms": r["ms"]}

@@ -93,6 +93,23 @@ int tr_route_build(const int32_t* indptr, const int32_t* indices, const float* v
                    int32_t n_rows, const tr_route_params* params, tr_route** out);
 /* Table idx in the reference's return order (0..28); `count` is in elements. */
 int tr_route_table(const tr_route* r, int idx, const void** data, int64_t* count);
+/* The whole router on the device (sm_100a integer kernels, one CTA per
+ * window): profile, dense-TC funnel, 2:4 units, max-degree matching, 2:4
+ * groups, CUDA long / short parts, TC and mma.sp packing — the 29 tables of
+ * tr_route_build, equal to them item for item for the same parameters, from
+ * a device CSR whose rows are sorted by column (indptr / indices / values on
+ * the device).  The tables stay on the device (one allocation the route
+ * holds until tr_route_free): tr_route_table_device gives their device
+ * addresses; tr_route_table copies a table to the host on its first call
+ * for that table (thread-safe) and returns the host copy.  Replaces
+ * block_sptc_2to4_online (TR-source/Block/block_online.cpp:545-871), whose
+ * tables the reference's operator uploads to the GPU before every use.
+ * params.threads is ignored; tr_route_seconds is the device routing time. */
+int tr_route_device(const int32_t* d_indptr, const int32_t* d_indices, const float* d_values,
+                    int32_t n_rows, const tr_route_params* params, tr_route** out);
+/* Device address and item count of table idx (0..28) of a tr_route_device
+ * route (TR_ERR_UNSUPPORTED for host-built routes). */
+int tr_route_table_device(const tr_route* r, int idx, const void** d_data, int64_t* count);
 /* The router's dense-TC funnel on the device (sm_100a integer kernels:
  * bitonic sorts, warp-ballot compaction, shared atomics; one CTA per
  * window): from a device CSR with rows sorted by column, the TC tables

@@ -16,6 +16,7 @@
 #include "block.h"
 #include "plan.h"
 #include "route_gpu.h"
+#include "route_full_gpu.h"
 #include "router.h"
 #include "spmm.h"
 #include "tca.h"
@@ -164,11 +165,27 @@ using namespace trs;
 
 struct tr_route {
   RouteTables t;
+  // device router: the tables live on the device; a table's host copy in
+  // `t` is made on its first tr_route_table call
+  std::unique_ptr<DeviceTables> dev;
+  std::mutex mu;
+  bool fetched[29] = {};
 };
 
 struct tr_host_plan {
   HostPlan hp;
 };
+
+namespace {
+// Host copy of one device table of a tr_route_device route.
+template <typename T>
+int fetch_table(std::vector<T>& dst, const void* src, int64_t count) {
+  dst.resize((size_t)count);
+  if (count > 0)
+    TRS_CUDA(cudaMemcpy(dst.data(), src, (size_t)count * sizeof(T), cudaMemcpyDeviceToHost));
+  return TR_OK;
+}
+}  // namespace
 
 extern "C" {
 
@@ -195,8 +212,74 @@ int tr_route_build(const int32_t* indptr, const int32_t* indices, const float* v
   return TR_OK;
 }
 
+int tr_route_device(const int32_t* d_indptr, const int32_t* d_indices, const float* d_values,
+                    int32_t n_rows, const tr_route_params* params, tr_route** out) {
+  if (!d_indptr || !params || !out) return fail(TR_ERR_ARG, "null argument");
+  if (n_rows < 0) return fail(TR_ERR_ARG, "n_rows must be >= 0");
+  const tr_route_params& q = *params;
+  if (!(q.window > 0 && q.window <= 32 && q.wide > 0 && q.wide <= 32))
+    return fail(TR_ERR_ARG, "window and wide must be in (0, 32]");
+  if (q.window > 16)
+    return fail(TR_ERR_UNSUPPORTED, "window > 16 is not supported (the 2-bit row vector overflows 32 bits)");
+  if (q.partsize_t <= 0 || q.partsize_c <= 0 || q.shortsize < 0)
+    return fail(TR_ERR_ARG, "partsize_t / partsize_c must be positive and shortsize >= 0");
+  if (q.mode != TR_ROUTE_COMPAT && q.mode != TR_ROUTE_EXACT) return fail(TR_ERR_ARG, "bad route mode");
+  RouteFullParams gp;
+  gp.window = q.window;
+  gp.density = q.density;
+  gp.tc_min_util = q.tc_min_util;
+  gp.partsize_t = q.partsize_t;
+  gp.partsize_c = q.partsize_c;
+  gp.shortsize = q.shortsize;
+  gp.unit_min_nnz = q.unit_min_nnz;
+  gp.skip_tc = q.skip_tc;
+  gp.skip_sptc = q.skip_sptc;
+  gp.mode = q.mode;
+  std::unique_ptr<tr_route> r(new tr_route());
+  r->dev.reset(new DeviceTables());
+  std::string err;
+  const int rc = route_full_gpu(d_indptr, d_indices, d_values, n_rows, gp, *r->dev, r->t, err);
+  if (rc) return err.empty() ? rc : fail(rc, err);
+  // the offset tables were formed on the host
+  for (int i : {0, 1, 7, 12, 22, 28}) r->fetched[i] = true;
+  *out = r.release();
+  return TR_OK;
+}
+
+int tr_route_table_device(const tr_route* r, int idx, const void** d_data, int64_t* count) {
+  if (!r || !d_data || !count) return fail(TR_ERR_ARG, "null argument");
+  if (idx < 0 || idx >= 29) return fail(TR_ERR_ARG, "table index out of range");
+  if (!r->dev) return fail(TR_ERR_UNSUPPORTED, "the tables of a host-built route are on the host");
+  *d_data = r->dev->ptr[idx];
+  *count = r->dev->count[idx];
+  return TR_OK;
+}
+
 int tr_route_table(const tr_route* r, int idx, const void** data, int64_t* count) {
   if (!r || !data || !count) return fail(TR_ERR_ARG, "null argument");
+  if (r->dev && idx >= 0 && idx < 29) {
+    tr_route* m = const_cast<tr_route*>(r);
+    std::lock_guard<std::mutex> lock(m->mu);
+    if (!m->fetched[idx]) {
+      RouteTables& H = m->t;
+      const void* src = r->dev->ptr[idx];
+      const int64_t n = r->dev->count[idx];
+      int rc = TR_OK;
+#define TRS_F(i, v) case i: rc = fetch_table(H.v, src, n); break;
+      switch (idx) {
+        TRS_F(2, t_column) TRS_F(3, t_value) TRS_F(4, t_window_row) TRS_F(5, t_atomic)
+        TRS_F(6, t_binary) TRS_F(8, c_row) TRS_F(9, c_atomic) TRS_F(10, c_column)
+        TRS_F(11, c_value) TRS_F(13, cs_row) TRS_F(14, cs_atomic) TRS_F(15, cs_column)
+        TRS_F(16, cs_value) TRS_F(17, s_column) TRS_F(18, s_mask) TRS_F(19, s_value)
+        TRS_F(20, s_pos) TRS_F(21, s_window) TRS_F(23, s_tile_window) TRS_F(24, s_tile_group)
+        TRS_F(25, s_tile_column) TRS_F(26, s_packed_a) TRS_F(27, s_packed_meta)
+        default: break;
+      }
+#undef TRS_F
+      if (rc) return rc;
+      m->fetched[idx] = true;
+    }
+  }
   const RouteTables& T = r->t;
 #define TRS_T(i, v) case i: *data = T.v.data(); *count = (int64_t)T.v.size(); return TR_OK;
   switch (idx) {
@@ -217,7 +300,6 @@ int tr_route_tc_device(const int32_t* d_indptr, const int32_t* d_indices, const 
                        int32_t n_rows, const tr_route_params* params, tr_route** out) {
   if (!d_indptr || !params || !out) return fail(TR_ERR_ARG, "null argument");
   if (n_rows < 0) return fail(TR_ERR_ARG, "negative row count");
-  if (n_rows > 0 && (!d_indices || !d_values)) return fail(TR_ERR_ARG, "null indices or values");
   if (params->window != 16) return fail(TR_ERR_UNSUPPORTED, "the device router uses 16-row windows");
   RouteGpuParams gp;
   gp.window = 16;
@@ -250,7 +332,6 @@ int tr_route_tc_device_noalloc(const int32_t* d_indptr, const int32_t* d_indices
                                int64_t cap_sub, int64_t cap_val, int64_t* n_sub_out,
                                int64_t* n_val_out, void* stream) {
   if (!d_indptr || !params) return fail(TR_ERR_ARG, "null argument");
-  if (n_rows > 0 && (!d_indices || !d_values)) return fail(TR_ERR_ARG, "null indices or values");
   if (params->window != 16) return fail(TR_ERR_UNSUPPORTED, "the device router uses 16-row windows");
   if (cap_sub > 0 && (!t_column || !t_binary || !t_block_offset))
     return fail(TR_ERR_ARG, "null table buffer with a non-zero sub-block capacity");

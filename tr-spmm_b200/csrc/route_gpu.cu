@@ -274,6 +274,7 @@ int route_tc_gpu(const int32_t* d_indptr, const int32_t* d_indices, const float*
   const int W = (n_rows + 15) / 16;
   std::vector<int32_t> indptr(n_rows + 1);
   TRS_CUDA(cudaMemcpy(indptr.data(), d_indptr, (n_rows + 1) * 4, cudaMemcpyDeviceToHost));
+  if (indptr[n_rows] > 0 && (!d_indices || !d_values)) { err = "null indices or values"; return TR_ERR_ARG; }
   // global scratch slices for windows beyond shared memory
   std::vector<int64_t> big_off(W, 0);
   int64_t big_bytes = 0;
@@ -500,6 +501,13 @@ int route_tc_gpu_noalloc(const int32_t* d_indptr, const int32_t* d_indices, cons
   // The status words still hold the last call's values: the only scratch
   // that must start at zero (counts and offsets are written before use).
   TRS_CUDA(cudaMemsetAsync(status, 0, 4 * sizeof(int), stream));
+  if (n_rows > 0 && (!d_indices || !d_values)) {
+    // null entry arrays are only valid for a matrix without entries
+    int32_t nnz = 0;
+    TRS_CUDA(cudaMemcpyAsync(&nnz, d_indptr + n_rows, 4, cudaMemcpyDeviceToHost, stream));
+    TRS_CUDA(cudaStreamSynchronize(stream));
+    if (nnz > 0) return fail(TR_ERR_ARG, "null indices or values");
+  }
   int host_status[4] = {0, 0, 0, 0};
   if (W > 0) {
     const int smem = (int)storage_bytes(kSmemKeys) + kSmemRoute;

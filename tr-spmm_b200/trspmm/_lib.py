@@ -20,7 +20,7 @@ TR_ROUTE_COMPAT, TR_ROUTE_EXACT = 0, 1
 # Every symbol declared in include/trspmm.h.
 EXPORTED = [
     "tr_last_error", "tr_version", "tr_device_info",
-    "tr_route_build", "tr_route_tc_device", "tr_route_tc_device_noalloc", "tr_route_table",
+    "tr_route_build", "tr_route_device", "tr_route_table_device", "tr_route_tc_device", "tr_route_tc_device_noalloc", "tr_route_table",
     "tr_route_seconds", "tr_route_free", "tr_match_2to4", "tr_match_2to4_online",
     "tr_plan_from_tables", "tr_plan_from_csr", "tr_plan_build", "tr_plan_build_host",
     "tr_host_plan_array", "tr_host_plan_upload", "tr_host_plan_free", "tr_host_plan_save",
@@ -131,6 +131,8 @@ def lib():
     L.tr_route_build.argtypes = [P, P, P, I32, ctypes.POINTER(RouteParams), P]
     L.tr_route_table.argtypes = [P, ctypes.c_int, ctypes.POINTER(P), ctypes.POINTER(I64)]
     L.tr_route_tc_device.argtypes = [P, P, P, I32, ctypes.POINTER(RouteParams), P]
+    L.tr_route_device.argtypes = [P, P, P, I32, ctypes.POINTER(RouteParams), P]
+    L.tr_route_table_device.argtypes = [P, ctypes.c_int, ctypes.POINTER(P), ctypes.POINTER(I64)]
     L.tr_route_tc_device_noalloc.argtypes = [P, P, P, I32, ctypes.POINTER(RouteParams), P, P, P, P,
                                              I64, I64, P, P, P]
     L.tr_match_2to4.argtypes = [P, P, I32, ctypes.c_int, I32, I32, I32, ctypes.POINTER(MatchStats)]

@@ -108,6 +108,71 @@ def route(indptr, indices, values, partsize_t=32, partsize_c=32, shortsize=3, de
     h = ctypes.c_void_p()
     check(L.tr_route_build(_vp(rp), _vp(ci), _vp(vv), rp.shape[0] - 1, ctypes.byref(prm),
                            ctypes.byref(h)))
+    return _read_route(h, window)
+
+
+class _DeviceArray:
+    """A device table seen through __cuda_array_interface__ (no copy)."""
+
+    def __init__(self, ptr, n, dtype):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": np.dtype(dtype).str,
+                                         "data": (int(ptr or 0), False), "version": 3}
+
+
+def route_device(indptr, indices, values, partsize_t=32, partsize_c=32, shortsize=3, density=8,
+                 window=16, wide=16, tc_min_util=0.0, sptc_min_util=0.5, sptc_threshold=12,
+                 mode="compat", unit_min_nnz=None, skip_tc=None, skip_sptc=False, out="numpy"):
+    """route() on the GPU (tr_route_device): every router stage as device
+    kernels over a CSR on the device (int32 indptr / indices and float32
+    values as CUDA tensors, or numpy arrays, uploaded first; rows sorted by
+    column).  Returns the same 30 tables as route(), equal item for item:
+    numpy arrays (out="numpy"), or CUDA tensors that never leave the device
+    (out="torch"; the last item is still the routing time in seconds)."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device())
+    t = [x if hasattr(x, "is_cuda") else torch.from_numpy(np.ascontiguousarray(x, dtype=d))
+         for x, d in ((indptr, np.int32), (indices, np.int32), (values, np.float32))]
+    t = [x.to(dev) for x in t]
+    for x, dt in zip(t, (torch.int32, torch.int32, torch.float32)):
+        if not (x.dtype == dt and x.is_contiguous()):
+            raise RuntimeError("indptr/indices (int32) and values (float32) must be contiguous")
+    prm = _params(partsize_t, partsize_c, shortsize, density, window, wide, tc_min_util,
+                  sptc_min_util, sptc_threshold, unit_min_nnz, skip_tc, mode, 0, skip_sptc)
+    h = ctypes.c_void_p()
+    check(lib().tr_route_device(ctypes.c_void_p(t[0].data_ptr()), ctypes.c_void_p(t[1].data_ptr()),
+                                ctypes.c_void_p(t[2].data_ptr()), t[0].numel() - 1,
+                                ctypes.byref(prm), ctypes.byref(h)))
+    if out == "numpy":
+        return _read_route(h, window)
+    L = lib()
+    try:
+        tabs = []
+        for i, dt in enumerate(_DTYPES):
+            data = ctypes.c_void_p()
+            n = ctypes.c_int64()
+            check(L.tr_route_table_device(h, i, ctypes.byref(data), ctypes.byref(n)))
+            view = torch.as_tensor(_DeviceArray(data.value, n.value, dt), device=dev)
+            tabs.append(view.clone())
+        torch.cuda.synchronize(dev)
+        seconds = L.tr_route_seconds(h)
+    finally:
+        L.tr_route_free(h)
+    g = tabs[21].shape[0]
+    nt = tabs[23].shape[0]
+    tabs[17] = tabs[17].reshape(g, 4)
+    tabs[18] = tabs[18].reshape(g, window)
+    tabs[19] = tabs[19].reshape(g, window, 2)
+    tabs[20] = tabs[20].reshape(g, window, 2)
+    tabs[25] = tabs[25].reshape(nt, 16)
+    tabs[26] = tabs[26].reshape(nt, 8, 4, 2)
+    tabs[27] = tabs[27].reshape(nt, 8)
+    tabs.append(np.float32(seconds))
+    return tabs
+
+
+def _read_route(h, window):
+    """The 30 tables of a tr_route handle (which it frees)."""
+    L = lib()
     try:
         out = []
         for i, dt in enumerate(_DTYPES):
