@@ -711,7 +711,9 @@ def main():
                       "forward_roofline": {
                           "achieved_gbs": fwd_bytes / (fwd_ms * 1e-3) / 1e9,
                           "frac": fwd_bytes / (fwd_ms * 1e-3) / 1e9 / peak,
-                          "algorithmic_bytes": fwd_bytes},
+                          "algorithmic_bytes": fwd_bytes,
+                          "traffic": _profile_traffic("block_mma_forward_large_routed.txt")
+                          if fwd_block else None},
                       "plain_csr_step_ms": plain_ms, "plain_csr_forward_ms": plain_fwd_ms,
                       "plain_fused_backward_ms": plain_bwd_ms,
                       "fp32_features_forward": fp32_route,
