@@ -727,10 +727,18 @@ def main():
                       "step_hbm_gbs": sbytes / (ms * 1e-3) / 1e9,
                       "step_hbm_frac": sbytes / (ms * 1e-3) / 1e9 / peak,
                       "plan_build_s": plan_s, "tune_s": tune_s, "router_s": router,
-                      "autotune": [{"options": r["options"], "ms": r["ms"]}
-                                   for r in tune_report.get("results", [])],
-                      "autotune_backward": [{"options": r["options"], "ms": r["ms"]}
-                                            for r in bwd_report.get("results", [])],
+                      "autotune": {
+                          "sample": tune_report.get("sample"),
+                          "on_sample": [{"options": r["options"], "ms": r["ms"]}
+                                        for r in tune_report.get("results", [])],
+                          "full_size": [{"options": r["options"], "ms": r["ms"]}
+                                        for r in tune_report.get("full", [])]},
+                      "autotune_backward": {
+                          "sample": bwd_report.get("sample"),
+                          "on_sample": [{"options": r["options"], "ms": r["ms"]}
+                                        for r in bwd_report.get("results", [])],
+                          "full_size": [{"options": r["options"], "ms": r["ms"]}
+                                        for r in bwd_report.get("full", [])]},
                       "batched_512": batched,
                       "plan_forward": pf.info, "plan_adjoint": pa.info,
                       "e2e_ms_per_step": e2e_max},

@@ -407,6 +407,13 @@ int tr_spmm_routed(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int 
  * same A take the same array). */
 int tr_plan_set_values(tr_plan* p, const float* values, int64_t n_edges, void* stream);
 
+/* Features per tensor-core launch of a block-engine plan (a multiple of 64
+ * up to 256, the MMA's N; 0 = 256): a product of K features runs as
+ * ceil(K / k_tile) launches, each gathering its feature slice of the same B
+ * rows.  Tuned per graph and K by trspmm.autotune; no effect on window
+ * plans. */
+int tr_plan_set_k_tile(tr_plan* p, int32_t k_tile);
+
 /* Edge numbering.  Every per-entry array a plan reads or writes
  * (tr_plan_set_values' values, tr_adjoint_sddmm's dval) is indexed by edge
  * number; edges start numbered as A's CSR entries.

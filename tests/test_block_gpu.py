@@ -150,3 +150,32 @@ def test_block_empty_and_partial(cuda):
         assert np.isfinite(got).all()
         ref = A @ b.astype(np.float64)
         assert np.abs(got - ref).max() <= TOL32 * max(1.0, np.abs(ref).max())
+
+
+@pytest.mark.parametrize("k, k_tile", [(128, 64), (256, 128), (256, 64), (320, 0), (384, 192),
+                                       (512, 0), (320, 192)])
+def test_block_feature_tiles(cuda, k, k_tile):
+    """K in feature tiles of k_tile (0 = 256) on the tensor cores: every tile
+    a launch over its feature slice, K above 256 included."""
+    g = GRAPHS["sbm"]()
+    plan, dec = _plan_and_ref(g, row_scale=True, reorder=True)
+    plan.set_k_tile(k_tile)
+    b = graphs.dense_features(g.n_cols, k, seed=k + 1)
+    out = plan.spmm(torch.from_numpy(b).to(cuda))
+    torch.cuda.synchronize()
+    assert rel_err(out.cpu().numpy(), dec @ b.astype(np.float64)) <= TOL32
+    whole = trspmm.Plan.build(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, engine="block",
+                              row_scale=True, reorder=True)
+    if k <= 256:
+        ref = whole.spmm(torch.from_numpy(b).to(cuda))
+        torch.cuda.synchronize()
+        # each output element is the same sequence of MMAs whatever the tile width
+        assert rel_err(out.cpu().numpy(), ref.cpu().numpy().astype(np.float64)) <= 1e-6
+
+
+def test_block_k_tile_refusals(cuda):
+    g = GRAPHS["chung_lu"]()
+    plan = trspmm.Plan.build(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, engine="block")
+    for bad in (32, 100, 320, -64):
+        with pytest.raises(RuntimeError, match="k_tile"):
+            plan.set_k_tile(bad)

@@ -262,7 +262,7 @@ __device__ __forceinline__ uint32_t ld_stream_u32(const uint32_t* p, uint64_t po
 
 template <bool F16OUT, int NA>
 __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
-    block_mma_kernel(PlanView pv, const __half* __restrict__ B, void* C) {
+    block_mma_kernel(PlanView pv, const __half* __restrict__ B, int ldb, void* C, int ldc) {
   using Cfg = BlkCfg<NA>;
   constexpr int K = Cfg::kN, S = Cfg::kStages, NG = Cfg::kGroups, P = Cfg::kProd;
   extern __shared__ uint8_t smem_raw[];
@@ -418,7 +418,7 @@ __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
         const int col = cols[t];
         const uint32_t dst = b_tile + (k >> 3) * (NA * 1024) + (g >> 3) * 1024 + (k & 7) * 128 +
                              (((g & 7) ^ (k & 7)) << 4);
-        const __half* src = B + (int64_t)(col >= 0 ? col : 0) * K + g * 8;
+        const __half* src = B + (int64_t)(col >= 0 ? col : 0) * ldb + g * 8;
         cp_async16_hint(dst, src, col >= 0 ? 16 : 0, pol_keep);
       }
       cp_async_arrive_noinc(smem_u32(&full[gs]));
@@ -498,7 +498,7 @@ __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
       if (nc == 0) {
         if (ro >= 0)
 #pragma unroll
-          for (int j = 0; j < 2 * NA; ++j) store_zero32<F16OUT>(C, (int64_t)ro * K + 32 * j);
+          for (int j = 0; j < 2 * NA; ++j) store_zero32<F16OUT>(C, (int64_t)ro * ldc + 32 * j);
         continue;
       }
       const int a = nacc & 1, ua = nacc >> 1;
@@ -508,7 +508,7 @@ __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
       for (int j = 0; j < 2 * NA; ++j) {
         float v[32];
         tmem_ld_x32(tmem + ((uint32_t)(32 * w) << 16) + (uint32_t)(a * Cfg::kN + 32 * j), v);
-        if (ro >= 0) store_row32<F16OUT>(C, (int64_t)ro * K + 32 * j, v, sc);
+        if (ro >= 0) store_row32<F16OUT>(C, (int64_t)ro * ldc + 32 * j, v, sc);
       }
       tc_fence_before();
       __syncwarp();
@@ -567,12 +567,14 @@ __global__ void __launch_bounds__(256)
   }
 }
 
+// One feature tile: B and C already offset to the tile's first feature,
+// rows ldb / ldc elements apart.
 template <bool F16OUT, int NA>
-int launch_mma_t(const tr_plan* p, const __half* b, void* c, cudaStream_t stream) {
+int launch_mma_t(const tr_plan* p, const __half* b, int ldb, void* c, int ldc, cudaStream_t stream) {
   using Cfg = BlkCfg<NA>;
   if (int rc = kernel_smem_limit((const void*)block_mma_kernel<F16OUT, NA>, Cfg::kSmem)) return rc;
   block_mma_kernel<F16OUT, NA><<<std::max(1, p->view.n_sched), Cfg::kThreads, Cfg::kSmem, stream>>>(
-      p->view, b, c);
+      p->view, b, ldb, c, ldc);
   TRS_CUDA(cudaGetLastError());
   return TR_OK;
 }
@@ -589,7 +591,12 @@ int launch_generic_t(const tr_plan* p, const TB* b, int32_t k, void* c, bool f16
 }  // namespace
 
 bool block_mma_supported(int32_t k, const void* b) {
-  return k >= 64 && k <= 256 && k % 64 == 0 && (reinterpret_cast<uintptr_t>(b) & 15) == 0;
+  return k >= 64 && k % 64 == 0 && (reinterpret_cast<uintptr_t>(b) & 15) == 0;
+}
+
+int block_k_tile(const tr_plan* p, int32_t k) {
+  const int t = p->k_tile > 0 ? p->k_tile : 256;
+  return std::min<int32_t>(t, k);
 }
 
 int launch_block(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_dtype,
@@ -601,12 +608,23 @@ int launch_block(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_
   bool fits = p->max_sched_blocks <= kMaxBlk;
   if (!force_generic && fits && block_mma_supported(k, b) &&
       (reinterpret_cast<uintptr_t>(c) & 15) == 0) {
-    switch (k / 64) {
-      case 1: return f16 ? launch_mma_t<true, 1>(p, bh, c, stream) : launch_mma_t<false, 1>(p, bh, c, stream);
-      case 2: return f16 ? launch_mma_t<true, 2>(p, bh, c, stream) : launch_mma_t<false, 2>(p, bh, c, stream);
-      case 3: return f16 ? launch_mma_t<true, 3>(p, bh, c, stream) : launch_mma_t<false, 3>(p, bh, c, stream);
-      default: return f16 ? launch_mma_t<true, 4>(p, bh, c, stream) : launch_mma_t<false, 4>(p, bh, c, stream);
+    // feature tiles of k_tile (a multiple of 64, at most 256: the MMA's N),
+    // one launch each; every tile gathers its slice of the same B rows
+    const int kt = block_k_tile(p, k);
+    for (int f0 = 0; f0 < k; f0 += kt) {
+      const int w = std::min(kt, k - f0);
+      const __half* bt = bh + f0;
+      void* ct = static_cast<char*>(c) + (size_t)f0 * (f16 ? 2 : 4);
+      int rc;
+      switch (w / 64) {
+        case 1: rc = f16 ? launch_mma_t<true, 1>(p, bt, k, ct, k, stream) : launch_mma_t<false, 1>(p, bt, k, ct, k, stream); break;
+        case 2: rc = f16 ? launch_mma_t<true, 2>(p, bt, k, ct, k, stream) : launch_mma_t<false, 2>(p, bt, k, ct, k, stream); break;
+        case 3: rc = f16 ? launch_mma_t<true, 3>(p, bt, k, ct, k, stream) : launch_mma_t<false, 3>(p, bt, k, ct, k, stream); break;
+        default: rc = f16 ? launch_mma_t<true, 4>(p, bt, k, ct, k, stream) : launch_mma_t<false, 4>(p, bt, k, ct, k, stream); break;
+      }
+      if (rc) return rc;
     }
+    return TR_OK;
   }
   return launch_generic_t(p, bh, k, c, f16, stream);
 }

@@ -8,9 +8,12 @@
 
 namespace trs {
 
-// K and B alignment the tensor-core block kernel takes (64 <= K <= 256,
-// K % 64 == 0, 16-byte aligned B); other shapes run the CUDA-core kernel.
+// K and B alignment the tensor-core block kernel takes (K a multiple of 64,
+// 16-byte aligned B; features in tiles of the plan's k_tile, at most 256);
+// other shapes run the CUDA-core kernel.
 bool block_mma_supported(int32_t k, const void* b);
+// Features per tensor-core launch for K (the plan's k_tile, default 256).
+int block_k_tile(const tr_plan* p, int32_t k);
 // C = A_plan . B over a block plan, FP16 features; every output row written.
 int launch_block(const tr_plan* p, const uint16_t* b, int32_t k, void* c, int c_dtype,
                  bool force_generic, cudaStream_t stream);

@@ -581,6 +581,14 @@ int tr_plan_set_values(tr_plan* p, const float* values, int64_t n_edges, void* s
   return launch_set_values(p, values, (cudaStream_t)stream);
 }
 
+int tr_plan_set_k_tile(tr_plan* p, int32_t k_tile) {
+  if (!p) return fail(TR_ERR_ARG, "null plan");
+  if (k_tile != 0 && (k_tile < 64 || k_tile > 256 || k_tile % 64 != 0))
+    return fail(TR_ERR_ARG, "k_tile must be 0, 64, 128, 192 or 256");
+  p->k_tile = k_tile;
+  return TR_OK;
+}
+
 int tr_plan_entry_order(const tr_plan* p, int32_t* order, void* stream) {
   if (!p) return fail(TR_ERR_ARG, "null plan");
   if (p->n_edges > 0 && !order) return fail(TR_ERR_ARG, "null device pointer");

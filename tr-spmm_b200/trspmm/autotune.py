@@ -8,10 +8,15 @@ earns its place in a tcgen05 tile when several rows of its window use it.
 This tuner times the candidate plan shapes on the device and keeps the
 fastest:
 
-  engine         "window": the reference's three routes over 16-row windows;
-                 "block": every entry on the tensor cores over 128-row
-                 blocks, each distinct column of a block gathered once
+  engine         the row-window height and layout: "window" = the
+                 reference's three routes over 16-row windows; "block" =
+                 every entry on the tensor cores over 128-row blocks, each
+                 distinct column of a block gathered once
+  k_tile         block engine: features per tensor-core launch (the MMA's
+                 N; 64..256), timed on one built plan
   reorder        cluster rows sharing columns into the same windows / blocks
+  density        the router's dense-TC column threshold (rows of a window
+                 using a column before it is a TC candidate; reference: 8)
   demote_below   2:4 tile columns with fewer entries go to the CUDA cores
   promote_min    CUDA-core columns with at least this many entries in a
                  window become tensor-core tiles
@@ -21,9 +26,11 @@ With backward=True the tuner times the whole backward of C = A(w) . B
 fused CUDA-core pass of all-residual window plans against the block engine's
 dB followed by the SDDMM.
 
-The window height (16 rows, the reference's tables; 128-row blocks for the
-block engine) and the feature chunk are fixed by the kernels; the kernel
-for the full product is chosen by the library from K.
+Large graphs are tuned on a sample (sample_nnz, default 2.5M entries): a
+contiguous slice of A's rows for the forward, of A's columns (A^T's rows)
+for the adjoint and the backward, so every kept row has its full degree and
+the natural order's locality; plans are built once per distinct layout and
+every launch setting (k_tile) is timed on it.
 
 Results are cached as JSON keyed by device name, K, the power-of-two
 buckets of nnz and rows, and the plan kind (forward, adjoint or backward),
@@ -38,6 +45,7 @@ import time
 
 import numpy as np
 
+from ._lib import TR_ENGINE_BLOCK
 from .core import Plan
 
 CANDIDATES = [
@@ -47,8 +55,11 @@ CANDIDATES = [
     {"reorder": True, "demote_below": 4, "promote_min": 4},
     {"reorder": True, "demote_below": 1000},
     {"promote_min": 1},                                   # every column on the tensor cores
+    {"density": 4, "demote_below": 1000},                 # looser dense-TC threshold
     {"engine": "block"},                                  # 128-row blocks, all tensor cores
     {"engine": "block", "reorder": True},
+    {"engine": "block", "reorder": True, "k_tile": 64},
+    {"engine": "block", "reorder": True, "k_tile": 128},
 ]
 
 BACKWARD_CANDIDATES = [
@@ -90,31 +101,38 @@ def _store_cache(path, data):
         pass
 
 
-def tune(indptr, indices, values, n_rows, n_cols, k, device="cuda", candidates=None,
-         transpose=False, row_scale=False, reps=5, use_cache=True, flush_mb=256,
-         backward=False):
-    """Time each candidate's routed product at feature width k on `device`
-    (L2 flushed before every timed launch, median of `reps`) and return
-    (best_options, report).  report = {"key", "cached", "results": [...]} with
-    per candidate its options, median ms, plan build seconds and plan info.
-    backward=True times the adjoint plan's whole backward (dB and the values'
-    gradient, Plan.adjoint_sddmm) over BACKWARD_CANDIDATES."""
+def sample_csr(indptr, indices, values, n_rows, n_cols, transpose, target):
+    """(indptr, indices, values, n_rows, n_cols) of a slice of A holding about
+    `target` entries: its first rows (forward) or, for A^T's plans, its
+    first columns (every row of A keeping the entries in those columns)."""
+    ip = np.asarray(indptr, dtype=np.int64)
+    ix = np.asarray(indices, dtype=np.int32)
+    vv = None if values is None else np.asarray(values, dtype=np.float32)
+    nnz = ix.shape[0]
+    if nnz <= target:
+        return indptr, indices, values, n_rows, n_cols
+    if not transpose:
+        m = int(np.searchsorted(ip, target, side="right")) - 1
+        m = max(1, min(n_rows, m))
+        e = int(ip[m])
+        return (ip[:m + 1].astype(np.int32), ix[:e], None if vv is None else vv[:e], m, n_cols)
+    counts = np.bincount(ix, minlength=n_cols)
+    c = int(np.searchsorted(np.cumsum(counts), target, side="right"))
+    c = max(1, min(n_cols, c))
+    keep = ix < c
+    rows = np.repeat(np.arange(n_rows), np.diff(ip))
+    ptr = np.zeros(n_rows + 1, np.int64)
+    np.add.at(ptr, rows[keep] + 1, 1)
+    return (np.cumsum(ptr).astype(np.int32), ix[keep], None if vv is None else vv[keep],
+            n_rows, c)
+
+
+def _time_candidates(indptr, indices, values, n_rows, n_cols, k, cands, dev, transpose,
+                     row_scale, reps, flush, backward):
+    """Median device time of each candidate (plans built once per layout;
+    launch settings such as k_tile timed on the same plan)."""
     import torch
-    dev = torch.device(device)
-    name = torch.cuda.get_device_name(dev)
     nnz = int(np.asarray(indices).shape[0])
-    if backward:
-        transpose = True
-    key = cache_key(name, k, nnz, n_rows, transpose, backward)
-    path = cache_path()
-    cache = _load_cache(path) if use_cache else {}
-    if use_cache and key in cache:
-        return dict(cache[key]["best"]), {"key": key, "cached": True,
-                                          "results": cache[key].get("results", [])}
-    if candidates is not None:
-        cands = candidates
-    else:
-        cands = BACKWARD_CANDIDATES if backward else CANDIDATES
     rows_b = n_cols if transpose else n_rows
     cols_b = n_rows if transpose else n_cols
     rng = np.random.default_rng(0)
@@ -126,37 +144,119 @@ def tune(indptr, indices, values, n_rows, n_cols, k, device="cuda", candidates=N
         ip = torch.from_numpy(np.ascontiguousarray(indptr, dtype=np.int32)).to(dev)
         ix = torch.from_numpy(np.ascontiguousarray(indices, dtype=np.int32)).to(dev)
         dval = torch.empty(nnz, dtype=torch.float32, device=dev)
-    flush = torch.empty(flush_mb * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     results = []
-    for opts in cands:
-        t0 = time.perf_counter()
-        plan = Plan.build(indptr, indices, values, n_rows, n_cols, transpose=transpose,
-                          row_scale=row_scale, **opts)
-        build_s = time.perf_counter() - t0
-        if backward:
-            def run():
-                plan.adjoint_sddmm(ip, ix, b, bb, db=out, dval=dval)
-        else:
-            def run():
-                plan.spmm(b, out=out)
-        for _ in range(2):
-            run()
-        ts = []
-        for _ in range(reps):
-            flush.fill_(1.0)
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record()
-            run()
-            e1.record()
-            torch.cuda.synchronize()
-            ts.append(e0.elapsed_time(e1))
-        results.append({"options": opts, "ms": float(np.median(ts)), "build_s": build_s,
-                        "info": dict(plan.info)})
-        plan.close()
-    best = min(results, key=lambda r: r["ms"])["options"]
+    plans = {}                       # layout options -> (plan, build seconds)
+    try:
+        for opts in cands:
+            layout = {kk: v for kk, v in opts.items() if kk != "k_tile"}
+            lkey = json.dumps(layout, sort_keys=True)
+            if lkey not in plans:
+                t0 = time.perf_counter()
+                plans[lkey] = (Plan.build(indptr, indices, values, n_rows, n_cols,
+                                          transpose=transpose, row_scale=row_scale, **layout),
+                               time.perf_counter() - t0)
+            plan, build_s = plans[lkey]
+            if plan.info["engine"] == TR_ENGINE_BLOCK:
+                plan.set_k_tile(opts.get("k_tile", 0))
+            if backward:
+                def run():
+                    plan.adjoint_sddmm(ip, ix, b, bb, db=out, dval=dval)
+            else:
+                def run():
+                    plan.spmm(b, out=out)
+            for _ in range(2):
+                run()
+            ts = []
+            for _ in range(reps):
+                flush.fill_(1.0)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                run()
+                e1.record()
+                torch.cuda.synchronize()
+                ts.append(e0.elapsed_time(e1))
+            results.append({"options": opts, "ms": float(np.median(ts)), "build_s": build_s,
+                            "info": dict(plan.info)})
+    finally:
+        for plan, _ in plans.values():
+            plan.close()
+    return results
+
+
+def _finalists(results):
+    """Per engine family the best layout on the sample, with every launch
+    setting timed for that layout."""
+    best = {}
+    for r in results:
+        fam = r["options"].get("engine", "window")
+        if fam not in best or r["ms"] < best[fam]["ms"]:
+            best[fam] = r
+    out = []
+    for r in best.values():
+        layout = {kk: v for kk, v in r["options"].items() if kk != "k_tile"}
+        out += [x["options"] for x in results
+                if {kk: v for kk, v in x["options"].items() if kk != "k_tile"} == layout]
+    return out
+
+
+def tune(indptr, indices, values, n_rows, n_cols, k, device="cuda", candidates=None,
+         transpose=False, row_scale=False, reps=5, use_cache=True, flush_mb=256,
+         backward=False, sample_nnz=2_500_000):
+    """Time each candidate's routed product at feature width k on `device`
+    (L2 flushed before every timed launch, median of `reps`) and return
+    (best_options, report).  report = {"key", "cached", "sample", "results",
+    "full"}: per candidate its options, median ms, plan build seconds and
+    plan info.  backward=True times the adjoint plan's whole backward (dB
+    and the values' gradient, Plan.adjoint_sddmm) over BACKWARD_CANDIDATES.
+
+    A graph above sample_nnz entries is tuned in two stages: every candidate
+    on a slice of about that size (sample_csr), then, at full size, each
+    engine family's best layout on the slice with its launch settings, the
+    winner chosen among those.  The engines scale differently with size (the
+    block engine has a fixed pipeline start per CTA), so the engine is
+    decided at full size; within an engine the slice's ranking is kept.
+    sample_nnz=None times every candidate at full size."""
+    import torch
+    dev = torch.device(device)
+    name = torch.cuda.get_device_name(dev)
+    nnz = int(np.asarray(indices).shape[0])
+    if backward:
+        transpose = True
+    key = cache_key(name, k, nnz, n_rows, transpose, backward)
+    path = cache_path()
+    cache = _load_cache(path) if use_cache else {}
+    if use_cache and key in cache:
+        c = cache[key]
+        return dict(c["best"]), {"key": key, "cached": True, "sample": c.get("sample"),
+                                 "results": c.get("results", []), "full": c.get("full", [])}
+    if candidates is not None:
+        cands = candidates
+    else:
+        cands = BACKWARD_CANDIDATES if backward else CANDIDATES
+    # a k_tile at or above K is the default launch: drop the duplicates
+    cands = [c for c in cands if not (c.get("k_tile", 0) and c["k_tile"] >= k)]
+    flush = torch.empty(flush_mb * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    sampled = bool(sample_nnz) and nnz > sample_nnz
+    sample = None
+    if sampled:
+        s_ip, s_ix, s_v, s_m, s_n = sample_csr(indptr, indices, values, n_rows, n_cols,
+                                               transpose, sample_nnz)
+        sample = {"n_rows": int(s_m), "n_cols": int(s_n), "nnz": int(np.asarray(s_ix).shape[0]),
+                  "of": {"n_rows": int(n_rows), "n_cols": int(n_cols), "nnz": nnz}}
+        results = _time_candidates(s_ip, s_ix, s_v, s_m, s_n, k, cands, dev, transpose,
+                                   row_scale, reps, flush, backward)
+        full = _time_candidates(indptr, indices, values, n_rows, n_cols, k,
+                                _finalists(results), dev, transpose, row_scale, reps, flush,
+                                backward)
+    else:
+        results = _time_candidates(indptr, indices, values, n_rows, n_cols, k, cands, dev,
+                                   transpose, row_scale, reps, flush, backward)
+        full = results
+    best = min(full, key=lambda r: r["ms"])["options"]
     if use_cache:
         cache = _load_cache(path)
-        cache[key] = {"best": best, "results": results}
+        cache[key] = {"best": best, "results": results, "full": full, "sample": sample}
         _store_cache(path, cache)
-    return dict(best), {"key": key, "cached": False, "results": results}
+    return dict(best), {"key": key, "cached": False, "sample": sample, "results": results,
+                        "full": full}

@@ -296,6 +296,7 @@ class Plan:
         self.info = {f: getattr(info, f) for f, _ in PlanInfo._fields_}
         self.n_rows = info.n_rows
         self.n_cols = info.n_cols
+        self.k_tile = 0
 
     @classmethod
     def from_tables(cls, tabs, n_rows, n_cols, window=16):
@@ -320,11 +321,12 @@ class Plan:
     @classmethod
     def build(cls, indptr, indices, values, n_rows, n_cols, row_scale=False, promote_min=0,
               transpose=False, reorder=False, demote_below=0, mode="exact", engine="window",
-              **route_kw):
+              k_tile=0, **route_kw):
         """Native builder (tr_plan_build): route A (or A^T when transpose) and
         lay it out; the plan keeps, for every CSR entry of A, where its value
         lives (set_values).  For a transposed plan n_rows/n_cols are A's.
-        ``engine="block"`` lays the matrix out for the block engine."""
+        ``engine="block"`` lays the matrix out for the block engine;
+        ``k_tile`` its features per tensor-core launch (set_k_tile)."""
         rp = np.ascontiguousarray(indptr, dtype=np.int32)
         ci = np.ascontiguousarray(indices, dtype=np.int32)
         vv = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
@@ -333,7 +335,16 @@ class Plan:
         h = ctypes.c_void_p()
         check(lib().tr_plan_build(_vp(rp), _vp(ci), _vp(vv), int(n_rows), int(n_cols),
                                   ctypes.byref(prm), ctypes.byref(opts), ctypes.byref(h)))
-        return cls(h)
+        plan = cls(h)
+        if k_tile:
+            plan.set_k_tile(k_tile)
+        return plan
+
+    def set_k_tile(self, k_tile):
+        """Features per tensor-core launch of a block-engine plan
+        (tr_plan_set_k_tile: 0 = 256, else 64, 128, 192 or 256)."""
+        check(lib().tr_plan_set_k_tile(self._h, int(k_tile)))
+        self.k_tile = int(k_tile)
 
     def set_values(self, values, stream=None):
         """Re-value the plan from a CUDA float32 tensor of A's CSR entries."""
@@ -482,9 +493,10 @@ HOST_PLAN_ARRAYS = [("win_tile", np.int32), ("win_split", np.int32), ("win_prom"
 
 def host_plan(indptr, indices, values, n_rows, n_cols, row_scale=False, promote_min=0,
               transpose=False, reorder=False, demote_below=0, mode="exact", engine="window",
-              **route_kw):
+              k_tile=0, **route_kw):
     """The native builder's plan as host arrays (tr_plan_build_host), without
-    a device: a dict name -> numpy array (layout in csrc/plan.h)."""
+    a device: a dict name -> numpy array (layout in csrc/plan.h).  ``k_tile``
+    is a launch setting and does not change the arrays."""
     rp = np.ascontiguousarray(indptr, dtype=np.int32)
     ci = np.ascontiguousarray(indices, dtype=np.int32)
     vv = None if values is None else np.ascontiguousarray(values, dtype=np.float32)

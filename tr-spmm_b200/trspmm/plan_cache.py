@@ -108,7 +108,9 @@ def cached_host_plan(indptr, indices, values, n_rows, n_cols, directory=None, **
 def cached_plan(indptr, indices, values, n_rows, n_cols, directory=None, **plan_kw):
     """Device plan (core.Plan) through the cache; same options as
     core.Plan.build.  The plan's ``cache_hit`` says whether routing was
-    skipped."""
+    skipped.  ``k_tile`` (a launch setting, not part of the file) is applied
+    after the upload."""
+    k_tile = plan_kw.pop("k_tile", 0)
     h, path, hit = cached_host_plan(indptr, indices, values, n_rows, n_cols, directory, **plan_kw)
     L = lib()
     try:
@@ -118,4 +120,6 @@ def cached_plan(indptr, indices, values, n_rows, n_cols, directory=None, **plan_
         L.tr_host_plan_free(h)
     plan = core.Plan(p)
     plan.cache_hit, plan.cache_path = hit, path
+    if k_tile:
+        plan.set_k_tile(k_tile)
     return plan
