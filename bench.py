@@ -162,9 +162,22 @@ def adjoint_sddmm_bytes(nnz, m, n, k, out_bytes=4, entry_ids=False):
     return nnz * per + (n + 1) * 4 + m * k * 2 + n * k * 2 + n * k * out_bytes
 
 
+def block_bwd_bytes(nnz, chunks, m, n, k, out_bytes=4, entry_ids=False):
+    """Tensor-core backward over a block plan of A^T (n rows): per entry its
+    packed value and position and its dval (4+4 bytes; plus a 4-byte entry id
+    when dval is stored through one), per chunk its 16 columns and entry
+    offset; dC (m x k FP16) and B (n x k FP16) read once; dB (n x k) written
+    once."""
+    per = 4 + 4 + (4 if entry_ids else 0)
+    return nnz * per + chunks * (16 * 4 + 4) + m * k * 2 + n * k * 2 + n * k * out_bytes
+
+
 def _single_stream(adj_opts):
-    """An all-residual window adjoint plan (its entries form one stream)."""
-    return adj_opts.get("engine", "window") == "window" and adj_opts.get("demote_below", 0) >= 1000
+    """Adjoint plans whose entries form one stream (block plans, all-residual
+    window plans): the edges can be numbered in their entry order."""
+    if adj_opts.get("engine", "window") == "block":
+        return True
+    return adj_opts.get("demote_below", 0) >= 1000
 
 
 def step_bytes(nnz, m, n, k):
@@ -655,7 +668,9 @@ def main():
     fused_bwd = (pa.info["engine"] == trspmm.TR_ENGINE_WINDOW
                  and pa.info["tc_tiles"] + pa.info["sptc_tiles"] + pa.info["promoted_tiles"] == 0
                  and pa.info["residual_nnz"] == g.nnz and k <= 256)
-    bwd_launches = 1 if fused_bwd else launches(pa) + 1
+    # the block engine's tensor-core backward: dB and dval in one launch
+    block_bwd = pa.info["engine"] == trspmm.TR_ENGINE_BLOCK and k in (64, 128)
+    bwd_launches = 1 if (fused_bwd or block_bwd) else launches(pa) + 1
     # the dominant kernel of the step: the longer of the backward's one fused
     # launch and the forward's (block kernel or CUDA-core residual pass)
     fwd_kernel_ms = fwd_ms if fwd_block else res_ms
@@ -664,6 +679,12 @@ def main():
         abytes = adjoint_sddmm_bytes(g.nnz, g.n_rows, g.n_cols, k, entry_ids=adj.edge_id is None)
         achieved = abytes / (adj_sddmm_ms * 1e-3) / 1e9
         traffic = _profile_traffic("seg_adjoint_sddmm_large_routed.txt")
+    elif block_bwd and adj_sddmm_ms >= fwd_kernel_ms:
+        dom_kernel = "block_bwd_kernel (tensor-core backward: dB = A^T dC, dval = SDDMM)"
+        abytes = block_bwd_bytes(g.nnz, int(pa.info["chunks"]), g.n_rows, g.n_cols, k,
+                                 entry_ids=adj.edge_id is None)
+        achieved = abytes / (adj_sddmm_ms * 1e-3) / 1e9
+        traffic = _profile_traffic("block_bwd_large_routed.txt")
     elif fwd_block:
         dom_kernel = "block_mma_kernel (forward on the tensor cores, 128-row blocks)"
         abytes, achieved = fwd_bytes, fwd_bytes / (fwd_ms * 1e-3) / 1e9

@@ -179,3 +179,60 @@ def test_block_k_tile_refusals(cuda):
     for bad in (32, 100, 320, -64):
         with pytest.raises(RuntimeError, match="k_tile"):
             plan.set_k_tile(bad)
+
+
+@pytest.mark.parametrize("name", ["chung_lu", "ragged_dup", "sbm", "hub_rows", "single_row"])
+@pytest.mark.parametrize("k", [64, 128])
+@pytest.mark.parametrize("renumber", [False, True])
+def test_block_tensor_core_backward(cuda, name, k, renumber):
+    """K = 64 / 128 on a block adjoint plan run the tensor-core backward
+    (dB by one MMA, dval by a second against the block's rows of B in tensor
+    memory): dB and dval against FP64, bitwise repeatable, and with the
+    edges numbered in the plan's entry order dval lands at the entry's
+    position."""
+    g = GRAPHS[name]()
+    kw = dict(engine="block", transpose=True, row_scale=True, reorder=name == "sbm")
+    P = trspmm.host_plan(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, **kw)
+    dec = oracle.decode_plan(P)["all"]
+    adj = trspmm.Plan.build(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, **kw)
+    new_id = None
+    if renumber:
+        order = adj.entry_order(cuda)
+        new_id = torch.empty_like(order)
+        new_id[order.long()] = torch.arange(g.nnz, dtype=torch.int32, device=cuda)
+        adj.renumber_edges(new_id)
+    dc = graphs.dense_features(g.n_rows, k, seed=21)
+    b = graphs.dense_features(g.n_cols, k, seed=22)
+    ip = torch.from_numpy(g.indptr).to(cuda)
+    ix = torch.from_numpy(g.indices).to(cuda)
+    dct, bt = torch.from_numpy(dc).to(cuda), torch.from_numpy(b).to(cuda)
+    db1, dv1 = adj.adjoint_sddmm(ip, ix, dct, bt)
+    db2, dv2 = adj.adjoint_sddmm(ip, ix, dct, bt)
+    torch.cuda.synchronize()
+    assert torch.equal(db1, db2) and torch.equal(dv1, dv2)
+    assert rel_err(db1.cpu().numpy(), dec @ dc.astype(np.float64)) <= TOL32
+    dv = dv1 if new_id is None else dv1[new_id.long()]
+    rows = np.repeat(np.arange(g.n_rows), np.diff(g.indptr))
+    ref = np.einsum("ij,ij->i", dc[rows].astype(np.float64), b[g.indices].astype(np.float64))
+    assert rel_err(dv.cpu().numpy(), ref) <= 1e-5
+    db16, _ = adj.adjoint_sddmm(ip, ix, dct, bt, db_dtype=torch.float16)
+    torch.cuda.synchronize()
+    assert rel_err(db16.float().cpu().numpy(), dec @ dc.astype(np.float64)) <= TOL16
+
+
+def test_block_backward_empty_blocks(cuda):
+    """Rows of A^T without entries (columns of A nobody uses) get zero dB."""
+    g = graphs.random_csr(300, 2000, 0.002, seed=4)
+    adj = trspmm.Plan.build(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, engine="block",
+                            transpose=True)
+    dc = torch.from_numpy(graphs.dense_features(g.n_rows, 64, seed=1)).to(cuda)
+    b = torch.from_numpy(graphs.dense_features(g.n_cols, 64, seed=2)).to(cuda)
+    db = torch.full((g.n_cols, 64), float("nan"), device=cuda)
+    dv = torch.full((g.nnz,), float("nan"), device=cuda)
+    adj.adjoint_sddmm(torch.from_numpy(g.indptr).to(cuda), torch.from_numpy(g.indices).to(cuda),
+                      dc, b, db=db, dval=dv)
+    torch.cuda.synchronize()
+    assert torch.isfinite(db).all() and torch.isfinite(dv).all()
+    used = np.zeros(g.n_cols, bool)
+    used[g.indices] = True
+    assert (db[torch.from_numpy(~used).to(cuda)] == 0).all()

@@ -612,6 +612,8 @@ int tr_adjoint_sddmm(const tr_plan* adj, const int32_t* a_indptr, const int32_t*
   if (k > 0 && (!dc || !b || !db || (nnz > 0 && (!a_indptr || !a_indices || !dval))))
     return fail(TR_ERR_ARG, "null device pointer");
   if (adj->blocked) {
+    if (block_bwd_supported(adj, k, dc, b, db, dval) && nnz == adj->n_edges)
+      return launch_block_bwd(adj, dc, b, k, db, db_dtype, dval, (cudaStream_t)stream);
     int rc = launch_block(adj, dc, k, db, db_dtype, false, (cudaStream_t)stream);
     if (rc) return rc;
     return launch_sddmm(a_indptr, a_indices, a_rows, nnz, dc, b, k, dval, (cudaStream_t)stream,

@@ -147,7 +147,7 @@ int launch_renumber_edges(tr_plan* p, const int32_t* new_id, cudaStream_t stream
   TRS_CUDA(cudaMemcpyAsync(h_flags + 1, flags + 1, 4, cudaMemcpyDeviceToHost, stream));
   TRS_CUDA(cudaFreeAsync(tmp, stream));
   TRS_CUDA(cudaStreamSynchronize(stream));
-  p->res_edge_identity = !p->blocked && m > 0 && stream_map && h_flags[1] == 0;
+  p->res_edge_identity = m > 0 && stream_map && h_flags[1] == 0;
   return TR_OK;
 }
 

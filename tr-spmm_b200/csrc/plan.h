@@ -141,7 +141,10 @@ struct tr_plan {
   // caller's numbering and edge_id[e] (own allocation) is the current number
   // of A's CSR entry e (the SDDMM over A's CSR writes through it).
   int32_t* edge_id = nullptr;
-  bool res_edge_identity = false; // res_edge[q] == q: the fused backward skips it
+  // the kernels' entry stream map (res_edge of window plans, ent_src of
+  // block plans) is the identity: the backward stores dval at the entry's
+  // own position and reads no map
+  bool res_edge_identity = false;
   tr_plan_info info{};
 };
 
