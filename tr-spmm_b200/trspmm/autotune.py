@@ -213,9 +213,10 @@ def tune(indptr, indices, values, n_rows, n_cols, k, device="cuda", candidates=N
     A graph above sample_nnz entries is tuned in two stages: every candidate
     on a slice of about that size (sample_csr), then, at full size, each
     engine family's best layout on the slice with its launch settings, the
-    winner chosen among those.  The engines scale differently with size (the
-    block engine has a fixed pipeline start per CTA), so the engine is
-    decided at full size; within an engine the slice's ranking is kept.
+    winner chosen among those.  The engines respond differently to a slice
+    (the block engine's column reuse per block and work per CTA shrink with
+    it), so the engine is decided at full size; within an engine the
+    slice's ranking is kept.
     sample_nnz=None times every candidate at full size."""
     import torch
     dev = torch.device(device)
