@@ -535,6 +535,21 @@ def main():
     plain_bwd_ms = float(np.mean(timed(
         lambda: plain_adj.adjoint_sddmm(ip, ix, dcd, bd, db=db2, dval=dv2), n_side, 3)))
     plain_adj.close()
+    # the deterministic alternative: the block plan of A^T with the
+    # tensor-core backward (edges in its own entry order), unless it is the
+    # step's own adjoint plan already
+    block_bwd_ms = None
+    if pa.info["engine"] != trspmm.TR_ENGINE_BLOCK and k in (64, 128):
+        bplan = trspmm.Plan.build(g.indptr, g.indices, g.values, g.n_rows, g.n_cols,
+                                  transpose=True, row_scale=True, engine="block", reorder=True)
+        border = bplan.entry_order(dev)
+        bid = torch.empty_like(border)
+        bid[border.long()] = torch.arange(g.nnz, dtype=torch.int32, device=dev)
+        bplan.renumber_edges(bid)
+        block_bwd_ms = float(np.mean(timed(
+            lambda: bplan.adjoint_sddmm(ip, ix, dcd, bd, db=db2, dval=dv2), n_side, 3)))
+        bplan.close()
+        del border, bid
     # the same forward with the features in FP32 (FP32-feature route, CUDA
     # cores; a window plan, the block engine's FP32 kernel being a fallback)
     pf32 = pf if pf.info["engine"] == trspmm.TR_ENGINE_WINDOW else trspmm.Plan.build(
@@ -737,6 +752,7 @@ def main():
                           if fwd_block else None},
                       "plain_csr_step_ms": plain_ms, "plain_csr_forward_ms": plain_fwd_ms,
                       "plain_fused_backward_ms": plain_bwd_ms,
+                      "block_tensor_core_backward_ms": block_bwd_ms,
                       "fp32_features_forward": fp32_route,
                       "routed_vs_plain_step": plain_ms / ms,
                       "routed_vs_plain_forward": plain_fwd_ms / fwd_ms,
