@@ -431,47 +431,30 @@ __global__ void __launch_bounds__(BwdCfg<NA>::kThreads, 1)
       if (gi >= nblk) return -1;
       return s_c0[gi] + kBG * gt++;
     };
-    // Two-deep prefetch: the chunk bounds of group n + 2 and the first two
-    // entry words of group n + 1 (whose bounds arrived one group earlier)
-    // are in flight while group n is processed.
-    auto load_bounds = [&](int cb, int (&b)[kBG + 1]) {
+    // a group's chunk bounds and this thread's first two entry words, loaded
+    // one group ahead so that their latency hides behind the current group
+    int nb[kBG + 1];
+    uint32_t nw[2];
+    auto prefetch = [&](int cb) {
 #pragma unroll
-      for (int j = 0; j <= kBG; ++j) b[j] = cb >= 0 ? __ldg(pv.chunk_ent + cb + j) : 0;
-    };
-    auto load_words = [&](const int (&b)[kBG + 1], uint32_t (&w)[2]) {
+      for (int j = 0; j <= kBG; ++j) nb[j] = cb >= 0 ? __ldg(pv.chunk_ent + cb + j) : 0;
 #pragma unroll
       for (int h = 0; h < 2; ++h) {
-        const int e = b[0] + td + 128 * h;
-        w[h] = e < b[kBG] ? __ldg(pv.ent_pv + e) : kNoEntry;
+        const int e = nb[0] + td + 128 * h;
+        nw[h] = e < nb[kBG] ? __ldg(pv.ent_pv + e) : kNoEntry;
       }
     };
     int cb = next_group();
-    int cb1 = cb >= 0 ? next_group() : -1;
-    int bnd[kBG + 1], bnd1[kBG + 1], bnd2[kBG + 1];
-    uint32_t wd[2], wd1[2];
-    load_bounds(cb, bnd);
-    load_bounds(cb1, bnd1);
-    load_words(bnd, wd);
+    prefetch(cb);
     int dn = 0;
     while (cb >= 0) {
-      const int cb2 = cb1 >= 0 ? next_group() : -1;
-      load_bounds(cb2, bnd2);
-      load_words(bnd1, wd1);
+      int bnd[kBG + 1];
+#pragma unroll
+      for (int j = 0; j <= kBG; ++j) bnd[j] = nb[j];
+      const uint32_t w0 = nw[0], w1 = nw[1];
+      const int cb_next = next_group();
+      prefetch(cb_next);
       const int e0 = bnd[0], e1 = bnd[kBG];
-      // this thread's entries of the group: where their values sit in the
-      // staged D2 tile (decoded before the tile is ready)
-      int at[2];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int e = e0 + td + 128 * h;
-        const int pos = (int)(wd[h] & 0xFFFFu);
-        const int m = ((pos >> 8) << 3) | ((pos >> 4) & 7);
-        const int kk = (((pos >> 7) & 1) << 3) | ((pos >> 1) & 7);
-        int j = 0;
-#pragma unroll
-        for (int c = 1; c < kBG; ++c) j += e >= bnd[c] ? 1 : 0;
-        at[h] = e < e1 ? m * kStgStride + 16 * j + kk : -1;
-      }
       const int ds = dn & 1;
       if (td == 0) *go = wait_bar(smem_u32(&d2_full[ds]), (dn >> 1) & 1, abort_flag) ? 1 : 0;
       named_bar_sync(kValBarrier, 128);
@@ -488,31 +471,19 @@ __global__ void __launch_bounds__(BwdCfg<NA>::kThreads, 1)
       tc_fence_before();
       named_bar_sync(kValBarrier, 128);
       if (td == 0) mbar_arrive(smem_u32(&d2_empty[ds]));
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int e = e0 + td + 128 * h;
-        if (at[h] >= 0) dval[dval_at ? __ldg(dval_at + e) : e] = stg[at[h]];
-      }
-      for (int e = e0 + td + 256; e < e1; e += 128) {      // groups of more than 256 entries
-        const uint32_t w = __ldg(pv.ent_pv + e);
+      for (int e = e0 + td, h = 0; e < e1; e += 128, ++h) {
+        const uint32_t w = h == 0 ? w0 : (h == 1 ? w1 : __ldg(pv.ent_pv + e));
         const int pos = (int)(w & 0xFFFFu);
         const int m = ((pos >> 8) << 3) | ((pos >> 4) & 7);
         const int kk = (((pos >> 7) & 1) << 3) | ((pos >> 1) & 7);
         int j = 0;
 #pragma unroll
         for (int c = 1; c < kBG; ++c) j += e >= bnd[c] ? 1 : 0;
-        dval[dval_at ? __ldg(dval_at + e) : e] = stg[m * kStgStride + 16 * j + kk];
+        const float v = stg[m * kStgStride + 16 * j + kk];
+        dval[dval_at ? __ldg(dval_at + e) : e] = v;
       }
       ++dn;
-      cb = cb1;
-      cb1 = cb2;
-#pragma unroll
-      for (int j = 0; j <= kBG; ++j) {
-        bnd[j] = bnd1[j];
-        bnd1[j] = bnd2[j];
-      }
-      wd[0] = wd1[0];
-      wd[1] = wd1[1];
+      cb = cb_next;
     }
   }
 
