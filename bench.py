@@ -568,12 +568,16 @@ def main():
     del b32, c3
 
     # ---- end to end through the public API with host buffers -------------------
-    # Every step uploads its B and dC from pinned host memory and downloads C,
-    # dB and dval into pinned host memory.  The loop is pipelined the way a
-    # training loop over batches would be: step i+1's upload (copy stream
-    # s_in) and step i's download (copy stream s_out) run while step i
-    # computes, in two alternating device-input / host-output slots, so the
-    # two PCIe directions and the compute overlap.  The timed region spans
+    # A training step through routed_spmm autograd: every step uploads its
+    # B and its upstream gradient G (= dC) from pinned host memory, computes
+    # C = A(w) B, the loss <C, G>, and the backward (dB, dw), and reads its
+    # result back into pinned host memory: the loss and the squared norms of
+    # dB and dw (three FP32 numbers; the gradients stay on the device for the
+    # optimizer).  Beside it, the same step downloading all of C, dB and dw
+    # (extra.e2e_full_outputs).  The loop is pipelined the way a training
+    # loop over batches would be: step i+1's upload (copy stream s_in) and
+    # step i's download (copy stream s_out) run while step i computes, in two
+    # alternating device-input / host-output slots.  The timed region spans
     # the first upload to the last download.
     b_host = torch.from_numpy(b).pin_memory()
     dc_host = torch.from_numpy(dc).pin_memory()
@@ -581,6 +585,7 @@ def main():
     c_host = [torch.empty((g.n_rows, k), dtype=torch.float32).pin_memory() for _ in range(2)]
     db_host = [torch.empty((g.n_cols, k), dtype=torch.float16).pin_memory() for _ in range(2)]
     dw_host = [torch.empty(g.nnz, dtype=torch.float32).pin_memory() for _ in range(2)]
+    m_host = [torch.empty(3, dtype=torch.float32).pin_memory() for _ in range(2)]
     b_in = [torch.empty((g.n_cols, k), dtype=torch.float16, device=dev) for _ in range(2)]
     dc_in = [torch.empty((g.n_rows, k), dtype=torch.float16, device=dev) for _ in range(2)]
     s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
@@ -596,57 +601,70 @@ def main():
             dc_in[sl].copy_(dc_host, non_blocking=True)
             ev_in[sl].record(s_in)
 
-    def compute_and_download(i):
+    def compute_and_download(i, full):
         sl = i % 2
         stream.wait_event(ev_in[sl])
         bb = b_in[sl].detach().requires_grad_(True)
         w = w_dev.detach().requires_grad_(True)
         c = routed_spmm(adj, bb, w)
-        c.backward(dc_in[sl])
+        if full:
+            c.backward(dc_in[sl])
+            outs = (c.detach(), bb.grad, w.grad)
+        else:
+            loss = (c * dc_in[sl]).sum()                # d loss / dC = G
+            loss.backward()
+            outs = (torch.stack([loss.detach(), bb.grad.float().square().sum(),
+                                 w.grad.square().sum()]),)
         ev_used[sl].record(stream)
-        outs = (c.detach(), bb.grad, w.grad)
         with torch.cuda.stream(s_out):
             s_out.wait_event(ev_used[sl])
-            c_host[sl].copy_(outs[0], non_blocking=True)
-            db_host[sl].copy_(outs[1], non_blocking=True)
-            dw_host[sl].copy_(outs[2], non_blocking=True)
+            if full:
+                c_host[sl].copy_(outs[0], non_blocking=True)
+                db_host[sl].copy_(outs[1], non_blocking=True)
+                dw_host[sl].copy_(outs[2], non_blocking=True)
+            else:
+                m_host[sl].copy_(outs[0], non_blocking=True)
             for t in outs:
                 t.record_stream(s_out)                  # keep alive until downloaded
             ev_out[sl].record(s_out)
 
-    def e2e_run(n):
+    def e2e_run(n, full):
         upload(0)
         for i in range(n):
             if i + 1 < n:
                 upload(i + 1)
-            compute_and_download(i)
+            compute_and_download(i, full)
         for sl in range(2):
             stream.wait_event(ev_out[sl])
 
     e2e_steps = max(3, min(args.steps, 30))
-    e2e_run(3)
-    torch.cuda.synchronize()
-    s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    s_ev.record(stream)
-    s_in.wait_event(s_ev)
-    e2e_run(e2e_steps)
-    e_ev.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = s_ev.elapsed_time(e_ev) / e2e_steps
-    e2e_max = max_over_ranks(e2e_ms, world, dev)
+
+    def e2e_time(full):
+        e2e_run(3, full)
+        torch.cuda.synchronize()
+        s_ev, e_ev = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s_ev.record(stream)
+        s_in.wait_event(s_ev)
+        e2e_run(e2e_steps, full)
+        e_ev.record(stream)
+        torch.cuda.synchronize()
+        return max_over_ranks(s_ev.elapsed_time(e_ev) / e2e_steps, world, dev)
+
+    e2e_max = e2e_time(False)
     e2e_val = whole_job_tflops(flops, world, e2e_max)
-    # the same through the public API without the pipelining (one step after
-    # another on one stream), for reference
+    e2e_full_max = e2e_time(True)
+    # the training step through the public API without the pipelining (one
+    # step after another on one stream), for reference
     def serial_step():
         b_in[0].copy_(b_host, non_blocking=True)
         dc_in[0].copy_(dc_host, non_blocking=True)
         bb = b_in[0].detach().requires_grad_(True)
         w = w_dev.detach().requires_grad_(True)
         c = routed_spmm(adj, bb, w)
-        c.backward(dc_in[0])
-        c_host[0].copy_(c.detach(), non_blocking=True)
-        db_host[0].copy_(bb.grad, non_blocking=True)
-        dw_host[0].copy_(w.grad, non_blocking=True)
+        loss = (c * dc_in[0]).sum()
+        loss.backward()
+        m_host[0].copy_(torch.stack([loss.detach(), bb.grad.float().square().sum(),
+                                     w.grad.square().sum()]), non_blocking=True)
     serial_ms = float(np.mean(timed(serial_step, min(e2e_steps, 10), 2)))
 
     peak, peak_kind = _peaks()
@@ -729,8 +747,11 @@ def main():
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": UNIT,
                     "h2d_bytes_per_step": int(b.nbytes + dc.nbytes),
-                    "d2h_bytes_per_step": int(g.n_rows * k * 4 + g.n_cols * k * 2 + g.nnz * 4),
-                    "ms_per_step": e2e_ms,
+                    "d2h_bytes_per_step": 12,
+                    "ms_per_step": e2e_max,
+                    "step": "routed_spmm autograd training step: upload B and the upstream "
+                            "gradient G, C = A(w) B, loss <C, G>, backward; result read back: "
+                            "the loss and |dB|^2, |dw|^2 (3 FP32)",
                     "pipelined": "step i+1's upload and step i's download overlap step i's "
                                  "compute (two copy streams, two slots)",
                     "serial_ms_per_step": serial_ms},
@@ -744,6 +765,10 @@ def main():
                           "achieved_gbs": res_gbs, "frac": res_gbs / peak,
                           "algorithmic_bytes": res_bytes,
                           "traffic": _profile_traffic("seg_residual_pass_large_routed.txt")},
+                      "forward_gathers": None if not fwd_block else {
+                          "distinct_block_columns_per_entry": pf.info["slots"] / g.nnz,
+                          "l2_to_sm_gather_bytes_per_pass": pf.info["slots"] * k * 2,
+                          "window_engine_gather_bytes_per_pass": g.nnz * k * 2},
                       "forward_roofline": {
                           "achieved_gbs": fwd_bytes / (fwd_ms * 1e-3) / 1e9,
                           "frac": fwd_bytes / (fwd_ms * 1e-3) / 1e9 / peak,
@@ -778,7 +803,12 @@ def main():
                                         for r in bwd_report.get("full", [])]},
                       "batched_512": batched,
                       "plan_forward": pf.info, "plan_adjoint": pa.info,
-                      "e2e_ms_per_step": e2e_max},
+                      "e2e_full_outputs": {
+                          "value": whole_job_tflops(flops, world, e2e_full_max), "unit": UNIT,
+                          "ms_per_step": e2e_full_max,
+                          "d2h_bytes_per_step": int(g.n_rows * k * 4 + g.n_cols * k * 2 + g.nnz * 4),
+                          "step": "the same step downloading all of C (FP32), dB (FP16) and dw "
+                                  "(FP32) every step"}},
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -232,6 +232,8 @@ typedef struct tr_plan_info {
   int32_t n_blocks;        /* 128-row blocks (block engine) */
   int64_t chunks;          /* 16-column chunks = tensor-core MMAs per product (block engine) */
   int64_t n_edges;         /* edges (per-entry values) the plan addresses: A's CSR entries */
+  int64_t slots;           /* block engine: used K slots = distinct (block, column) pairs
+                              (slot layers included) = B rows gathered per product */
 } tr_plan_info;
 
 /* Host route tables (pointer + element count each), in the reference's

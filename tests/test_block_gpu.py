@@ -236,3 +236,13 @@ def test_block_backward_empty_blocks(cuda):
     used = np.zeros(g.n_cols, bool)
     used[g.indices] = True
     assert (db[torch.from_numpy(~used).to(cuda)] == 0).all()
+
+
+def test_block_plan_slot_count(cuda):
+    """plan.info["slots"]: the distinct (block, column) pairs the product
+    gathers, as the host layout counts them."""
+    g = GRAPHS["ragged_dup"]()
+    P = trspmm.host_plan(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, engine="block")
+    plan = trspmm.Plan.build(g.indptr, g.indices, g.values, g.n_rows, g.n_cols, engine="block")
+    assert plan.info["slots"] == int((P["chunk_col"] >= 0).sum())
+    assert plan.info["chunks"] * 16 == P["chunk_col"].size

@@ -772,6 +772,10 @@ int plan_upload(const HostPlan& hp, tr_plan** out) {
   p->info.engine = hp.block ? TR_ENGINE_BLOCK : TR_ENGINE_WINDOW;
   p->info.n_blocks = v.n_blocks;
   p->info.chunks = hp.block ? (int64_t)hp.blk_chunk.back() : 0;
+  // distinct (block, column) pairs, slot layers included: the B rows one
+  // product gathers
+  p->info.slots = 0;
+  for (int32_t c : hp.chunk_col) p->info.slots += c >= 0 ? 1 : 0;
   if (hp.block) p->info.residual_nnz = 0;
   p->info.n_edges = n_edges;
   *out = p;

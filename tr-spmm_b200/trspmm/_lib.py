@@ -74,7 +74,7 @@ class PlanInfo(ctypes.Structure):
                 ("promoted_tiles", ctypes.c_int64), ("row_scaled", ctypes.c_int32),
                 ("reordered", ctypes.c_int32), ("engine", ctypes.c_int32),
                 ("n_blocks", ctypes.c_int32), ("chunks", ctypes.c_int64),
-                ("n_edges", ctypes.c_int64)]
+                ("n_edges", ctypes.c_int64), ("slots", ctypes.c_int64)]
 
 
 class PlanOpts(ctypes.Structure):
