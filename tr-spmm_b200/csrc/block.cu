@@ -15,8 +15,8 @@
 // layout pads it with chunks that have no entries); the eight stage slots
 // of a group share one full and one empty barrier.  Roles:
 //
-//   producer warps (kProd of them, two stage slots each, on the schedulers
-//   the MMA warp does not use; chunk q of the stream taken by producer
+//   producer warps (kProd of them, warps 5.., one stage slot each for
+//   K >= 128 and two for K = 64; chunk q of the stream taken by producer
 //   q % kProd)
 //       per chunk: wait until the slot is free, clear from its A tile the
 //       positions the slot's previous chunk set and write this chunk's
@@ -31,8 +31,7 @@
 //       filled eight chunks ahead.  Many producer warps keep enough gathers in
 //       flight: a warp's cp.async issue, not the memory system, sets the rate
 //       of one warp;
-//   MMA warp 4 (one elected thread; its scheduler is shared only with
-//   epilogue warp 0)
+//   MMA warp 4 (one elected thread)
 //       per group: wait full, one proxy fence (the operands were written
 //       through the generic proxy; the tensor core reads them through the
 //       async proxy), eight tcgen05.mma (M = 128, N = K, K = 16) into the
@@ -72,7 +71,6 @@ using namespace blk;
 constexpr int kGroup = kChunkGroup;     // chunks per barrier group
 constexpr int kEpiWarps = 4;
 constexpr int kMmaWarp = kEpiWarps;     // warp 4
-constexpr int kProdWarp0 = kEpiWarps;   // producers: warps 4 + 4i + 1 + j (j < 3)
 template <int NA>
 struct BlkCfg {
   static constexpr int kN = 64 * NA;               // features = MMA N
@@ -81,12 +79,14 @@ struct BlkCfg {
   // as many stage slots as shared memory (and registers) allow; two per
   // producer warp
   static constexpr int kStages = NA == 1 ? 32 : (NA == 2 ? 24 : 16);
-  static constexpr int kProd = kStages / 2;
+  // stage slots per producer warp: one for K >= 128 (24 producers: a warp's
+  // gather issue is latency-bound, so more warps gather faster), two for
+  // K = 64 (32 stages)
+  static constexpr int kRing = NA == 1 ? 2 : 1;
+  static constexpr int kProd = kStages / kRing;
   static constexpr int kGroups = kStages / kGroup;
-  // warps 0-3 epilogue, warp 4 MMA; producers on the warps of the other
-  // three schedulers (warp % 4 != 0), so the MMA thread shares its scheduler
-  // only with epilogue warp 0
-  static constexpr int kThreads = (kProdWarp0 + 4 * ((kProd - 1) / 3) + 1 + (kProd - 1) % 3 + 1) * 32;
+  // warps 0-3 epilogue, warp 4 MMA, producers from warp 5
+  static constexpr int kThreads = (kEpiWarps + 1 + kProd) * 32;
   static constexpr int kBarOff = kStages * kStage;
   // full[G], empty[G], acc_full[2], acc_empty[2], done; tmem slot, abort flag
   static constexpr int kBlkOff = (kBarOff + (2 * kGroups + 5) * 8 + 16 + 127) / 128 * 128;
@@ -108,7 +108,7 @@ template <bool F16OUT, int NA>
 __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
     block_mma_kernel(PlanView pv, const __half* __restrict__ B, int ldb, void* C, int ldc) {
   using Cfg = BlkCfg<NA>;
-  constexpr int K = Cfg::kN, S = Cfg::kStages, NG = Cfg::kGroups, P = Cfg::kProd;
+  constexpr int S = Cfg::kStages, NG = Cfg::kGroups, P = Cfg::kProd;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::kBarOff);
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
 
-  const int prod = (warp > kProdWarp0 && (warp & 3) != 0) ? ((warp - kProdWarp0) >> 2) * 3 + (warp & 3) - 1 : -1;
+  const int prod = warp > kMmaWarp ? warp - kMmaWarp - 1 : -1;
   if (prod >= 0 && prod < P) {
     // ------------------------------------------------------------ producers
     const int p = prod;
@@ -199,12 +199,18 @@ __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
     __syncwarp();
     // entry words of the chunk each register set serves next (chunks n and
     // n + 1 at the top of the loop), and of the chunk it served before
-    uint32_t ent[2][kEntReg], old[2][kEntReg];
-    int oldcnt[2] = {0, 0};
+    // entry words: two register sets alternate (chunk n in set n % 2, loaded
+    // two chunks ahead); the entries each of this warp's stage slots holds
+    // (slot n % kRing) are cleared before the slot's next chunk
+    constexpr int R = Cfg::kRing;
+    uint32_t ent[2][kEntReg], old[R][kEntReg];
+    int oldcnt[R] = {};
     load_ents(0, ent[0]);
     load_ents(1, ent[1]);
 #pragma unroll
-    for (int r = 0; r < kEntReg; ++r) old[0][r] = old[1][r] = kNoEntry;
+    for (int r = 0; r < kEntReg; ++r)
+#pragma unroll
+      for (int o = 0; o < R; ++o) old[o][r] = kNoEntry;
 
     // chunk n with register set SET (= n % 2, a compile-time index)
     auto body = [&](auto set_tag, int n) -> bool {
@@ -233,13 +239,14 @@ __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
       uint8_t* st = smem + s * Cfg::kStage;
       const uint32_t b_tile = smem_u32(st), a_tile = b_tile + Cfg::kBTile;
       // the slot's previous chunk leaves the A tile
-      if (oldcnt[SET] > kEntReg * 32) {
+      constexpr int OS = R == 1 ? 0 : SET;      // this chunk's stage slot among the warp's
+      if (oldcnt[OS] > kEntReg * 32) {
         uint4* at = reinterpret_cast<uint4*>(st + Cfg::kBTile);
         for (int i = lane; i < kATile / 16; i += 32) at[i] = make_uint4(0, 0, 0, 0);
       } else {
 #pragma unroll
         for (int r = 0; r < kEntReg; ++r)
-          if ((old[SET][r] & 0xFFFFu) < (uint32_t)kATile) sts_u16(a_tile + (old[SET][r] & 0xFFFFu), 0);
+          if ((old[OS][r] & 0xFFFFu) < (uint32_t)kATile) sts_u16(a_tile + (old[OS][r] & 0xFFFFu), 0);
       }
       __syncwarp();
       // this chunk's values
@@ -247,13 +254,13 @@ __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
       for (int r = 0; r < kEntReg; ++r) {
         const uint32_t w = ent[SET][r];
         if ((w & 0xFFFFu) < (uint32_t)kATile) sts_u16(a_tile + (w & 0xFFFFu), (uint16_t)(w >> 16));
-        old[SET][r] = w;
+        old[OS][r] = w;
       }
       for (int e = e0 + kEntReg * 32 + lane; e < e1; e += 32) {
         const uint32_t w = __ldg(pv.ent_pv + e);
         sts_u16(a_tile + (w & 0xFFFFu), (uint16_t)(w >> 16));
       }
-      oldcnt[SET] = e1 - e0;
+      oldcnt[OS] = e1 - e0;
       // gather: 16 rows x (8 * NA) 16-byte segments, 4 * NA per lane
 #pragma unroll
       for (int t = 0; t < 4 * NA; ++t) {

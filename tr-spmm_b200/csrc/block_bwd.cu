@@ -63,7 +63,10 @@ struct BwdCfg {
   static constexpr int kN = 64 * NA;               // features
   static constexpr int kBTile = 2048 * NA;         // 16 slots x kN features, FP16
   static constexpr int kStages = NA == 1 ? 24 : 20;
-  static constexpr int kProd = kStages / 2;
+  // stage slots per producer warp: two (with one, the 64-register cap of
+  // 29 warps spills the dval and dB paths: 1.0 ms against 0.51 ms)
+  static constexpr int kRing = 2;
+  static constexpr int kProd = kStages / kRing;
   static constexpr int kGroups = kStages / kBG;
   // warps 0-3 dB, 4 MMA, 5-7 producers, 8-11 dval, 12.. producers
   static constexpr int kWarps = 12 + (kProd - 3);
@@ -217,12 +220,15 @@ __global__ void __launch_bounds__(BwdCfg<NA>::kThreads, 1)
     for (int m = 0; m < kMetaRing; ++m) copy_meta(m);
     cp_async_wait_all();
     __syncwarp();
-    uint32_t ent[2][kEntReg], old[2][kEntReg];
-    int oldcnt[2] = {0, 0};
+    constexpr int R = Cfg::kRing;
+    uint32_t ent[2][kEntReg], old[R][kEntReg];
+    int oldcnt[R] = {};
     load_ents(0, ent[0]);
     load_ents(1, ent[1]);
 #pragma unroll
-    for (int r = 0; r < kEntReg; ++r) old[0][r] = old[1][r] = kNoEntry;
+    for (int r = 0; r < kEntReg; ++r)
+#pragma unroll
+      for (int o = 0; o < R; ++o) old[o][r] = kNoEntry;
 
     auto body = [&](auto set_tag, int n) -> bool {
       constexpr int SET = decltype(set_tag)::value;
@@ -244,26 +250,27 @@ __global__ void __launch_bounds__(BwdCfg<NA>::kThreads, 1)
       if (!wait_bar(smem_u32(&empty[gs]), ((q / S) & 1) ^ 1, abort_flag)) return false;
       uint8_t* st_a = smem + Cfg::kAOff + s * kATile;
       const uint32_t b_tile = smem_u32(smem + s * Cfg::kBTile), a_tile = smem_u32(st_a);
-      if (oldcnt[SET] > kEntReg * 32) {
+      constexpr int OS = R == 1 ? 0 : SET;      // this chunk's stage slot among the warp's
+      if (oldcnt[OS] > kEntReg * 32) {
         uint4* at = reinterpret_cast<uint4*>(st_a);
         for (int i = lane; i < kATile / 16; i += 32) at[i] = make_uint4(0, 0, 0, 0);
       } else {
 #pragma unroll
         for (int r = 0; r < kEntReg; ++r)
-          if ((old[SET][r] & 0xFFFFu) < (uint32_t)kATile) sts_u16(a_tile + (old[SET][r] & 0xFFFFu), 0);
+          if ((old[OS][r] & 0xFFFFu) < (uint32_t)kATile) sts_u16(a_tile + (old[OS][r] & 0xFFFFu), 0);
       }
       __syncwarp();
 #pragma unroll
       for (int r = 0; r < kEntReg; ++r) {
         const uint32_t w = ent[SET][r];
         if ((w & 0xFFFFu) < (uint32_t)kATile) sts_u16(a_tile + (w & 0xFFFFu), (uint16_t)(w >> 16));
-        old[SET][r] = w;
+        old[OS][r] = w;
       }
       for (int e = e0 + kEntReg * 32 + lane; e < e1; e += 32) {
         const uint32_t w = __ldg(pv.ent_pv + e);
         sts_u16(a_tile + (w & 0xFFFFu), (uint16_t)(w >> 16));
       }
-      oldcnt[SET] = e1 - e0;
+      oldcnt[OS] = e1 - e0;
 #pragma unroll
       for (int t = 0; t < 4 * NA; ++t) {
         const int idx = lane + 32 * t;
