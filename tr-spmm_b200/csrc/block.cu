@@ -11,9 +11,9 @@
 //
 // One persistent CTA per SM takes its blocks from the plan's schedule
 // (longest-processing-time assignment made at upload) as one stream of
-// chunks.  Every block holds a whole number of groups of eight chunks (the
-// layout pads it with chunks that have no entries); the eight stage slots
-// of a group share one full and one empty barrier.  Roles:
+// chunks.  Every block holds a whole number of groups of four or eight
+// chunks (the layout pads it with chunks that have no entries); the stage
+// slots of a group share one full and one empty barrier.  Roles:
 //
 //   producer warps (kProd of them, warps 5.., one stage slot each for
 //   K >= 128 and two for K = 64; chunk q of the stream taken by producer
@@ -34,7 +34,7 @@
 //   MMA warp 4 (one elected thread)
 //       per group: wait full, one proxy fence (the operands were written
 //       through the generic proxy; the tensor core reads them through the
-//       async proxy), eight tcgen05.mma (M = 128, N = K, K = 16) into the
+//       async proxy), one tcgen05.mma per chunk (M = 128, N = K, K = 16) into the
 //       block's accumulator, one commit to the group's empty barrier; after
 //       a block's last group a commit to the accumulator's full barrier.
 //       The loop is straight-line per group (stage descriptors are base +
@@ -68,11 +68,17 @@ namespace {
 
 using namespace blk;
 
-constexpr int kGroup = kChunkGroup;     // chunks per barrier group
+
 constexpr int kEpiWarps = 4;
 constexpr int kMmaWarp = kEpiWarps;     // warp 4
 template <int NA>
 struct BlkCfg {
+  // chunks per barrier group: the MMA starts once a group's chunks have all
+  // landed; groups of four measured faster at K = 192/256 (fewer, larger
+  // stages), eight at K = 64/128 (blocks hold whole groups: the layout pads
+  // them to multiples of kChunkGroup)
+  static constexpr int kGroup = NA >= 3 ? 4 : 8;
+  static_assert(kChunkGroup % kGroup == 0, "blocks hold whole groups");
   static constexpr int kN = 64 * NA;               // features = MMA N
   static constexpr int kBTile = 2048 * NA;         // 16 slots x kN features, FP16
   static constexpr int kStage = kBTile + kATile;   // a multiple of 1024
@@ -108,7 +114,7 @@ template <bool F16OUT, int NA>
 __global__ void __launch_bounds__(BlkCfg<NA>::kThreads, 1)
     block_mma_kernel(PlanView pv, const __half* __restrict__ B, int ldb, void* C, int ldc) {
   using Cfg = BlkCfg<NA>;
-  constexpr int S = Cfg::kStages, NG = Cfg::kGroups, P = Cfg::kProd;
+  constexpr int S = Cfg::kStages, NG = Cfg::kGroups, P = Cfg::kProd, kGroup = Cfg::kGroup;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = smem_raw + ((1024u - (smem_u32(smem_raw) & 1023u)) & 1023u);
   uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::kBarOff);
