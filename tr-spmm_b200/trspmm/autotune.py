@@ -23,8 +23,9 @@ fastest:
 
 With backward=True the tuner times the whole backward of C = A(w) . B
 (dB = A^T dC and the edge-value gradient) for candidate adjoint plans: the
-fused CUDA-core pass of all-residual window plans against the block engine's
-dB followed by the SDDMM.
+fused CUDA-core pass of all-residual window plans against the block
+engine's tensor-core backward, each with its edges numbered in its own
+entry order, as RoutedAdjacency(edge_order="adjoint") runs it.
 
 Large graphs are tuned on a sample (sample_nnz, default 2.5M entries): a
 contiguous slice of A's rows for the forward, of A's columns (A^T's rows)
@@ -45,7 +46,7 @@ import time
 
 import numpy as np
 
-from ._lib import TR_ENGINE_BLOCK
+from ._lib import TR_ENGINE_BLOCK, TrError
 from .core import Plan
 
 CANDIDATES = [
@@ -158,6 +159,19 @@ def _time_candidates(indptr, indices, values, n_rows, n_cols, k, cands, dev, tra
             plan, build_s = plans[lkey]
             if plan.info["engine"] == TR_ENGINE_BLOCK:
                 plan.set_k_tile(opts.get("k_tile", 0))
+            if backward and not getattr(plan, "_renumbered", False):
+                # time the backward as RoutedAdjacency(edge_order="adjoint")
+                # runs it: edges in the plan's own entry order, dval stored
+                # sequentially (plans with tensor-core tiles have no such order)
+                try:
+                    order = plan.entry_order(dev)
+                    new_id = torch.empty_like(order)
+                    new_id[order.long()] = torch.arange(order.numel(), dtype=torch.int32,
+                                                        device=dev)
+                    plan.renumber_edges(new_id)
+                except TrError:
+                    pass
+                plan._renumbered = True
             if backward:
                 def run():
                     plan.adjoint_sddmm(ip, ix, b, bb, db=out, dval=dval)
