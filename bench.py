@@ -535,7 +535,14 @@ def main():
     plain_bwd_ms = float(np.mean(timed(
         lambda: plain_adj.adjoint_sddmm(ip, ix, dcd, bd, db=db2, dval=dv2), n_side, 3)))
     plain_adj.close()
-    # the deterministic alternative: the block plan of A^T with the
+    # the step's fused backward with the bitwise-repeatable combine
+    det_bwd_ms = None
+    if pa.info["engine"] == trspmm.TR_ENGINE_WINDOW:
+        pa.set_deterministic(True)
+        det_bwd_ms = float(np.mean(timed(
+            lambda: pa.adjoint_sddmm(ip, ix, dcd, bd, db=db2, dval=dv2), n_side, 3)))
+        pa.set_deterministic(False)
+    # the other deterministic backward: the block plan of A^T with the
     # tensor-core backward (edges in its own entry order), unless it is the
     # step's own adjoint plan already
     block_bwd_ms = None
@@ -778,6 +785,7 @@ def main():
                       "plain_csr_step_ms": plain_ms, "plain_csr_forward_ms": plain_fwd_ms,
                       "plain_fused_backward_ms": plain_bwd_ms,
                       "block_tensor_core_backward_ms": block_bwd_ms,
+                      "fused_backward_deterministic_ms": det_bwd_ms,
                       "fp32_features_forward": fp32_route,
                       "routed_vs_plain_step": plain_ms / ms,
                       "routed_vs_plain_forward": plain_fwd_ms / fwd_ms,

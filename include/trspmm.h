@@ -416,6 +416,13 @@ int tr_plan_set_values(tr_plan* p, const float* values, int64_t n_edges, void* s
  * plans. */
 int tr_plan_set_k_tile(tr_plan* p, int32_t k_tile);
 
+/* Bitwise-repeatable backward on a window plan (on != 0): the fused
+ * adjoint + SDDMM adds the partial sums of rows cut by its segment
+ * boundaries in a fixed order instead of by shared-memory atomics (about
+ * 13 % slower on the headline graph).  Block-engine plans are always
+ * repeatable. */
+int tr_plan_set_deterministic(tr_plan* p, int32_t on);
+
 /* Edge numbering.  Every per-entry array a plan reads or writes
  * (tr_plan_set_values' values, tr_adjoint_sddmm's dval) is indexed by edge
  * number; edges start numbered as A's CSR entries.

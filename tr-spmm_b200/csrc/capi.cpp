@@ -589,6 +589,12 @@ int tr_plan_set_k_tile(tr_plan* p, int32_t k_tile) {
   return TR_OK;
 }
 
+int tr_plan_set_deterministic(tr_plan* p, int32_t on) {
+  if (!p) return fail(TR_ERR_ARG, "null plan");
+  p->deterministic = on != 0;
+  return TR_OK;
+}
+
 int tr_plan_entry_order(const tr_plan* p, int32_t* order, void* stream) {
   if (!p) return fail(TR_ERR_ARG, "null plan");
   if (p->n_edges > 0 && !order) return fail(TR_ERR_ARG, "null device pointer");

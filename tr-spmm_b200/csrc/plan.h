@@ -136,6 +136,7 @@ struct tr_plan {
   bool blocked = false;         // block layout (the block engine)
   int32_t max_sched_blocks = 0; // most blocks any CTA of the block schedule takes
   int32_t k_tile = 0;           // block engine: features per tensor-core launch (0: 256)
+  bool deterministic = false;   // window plans: the fused backward combines cut rows in order
   // Edge numbering.  Edges start numbered as A's CSR entries; after
   // tr_plan_renumber_edges, val_slot / edge_row / res_edge / ent_src use the
   // caller's numbering and edge_id[e] (own allocation) is the current number

@@ -1003,15 +1003,17 @@ __device__ __forceinline__ float group_reduce_scatter8(float (&d)[8], int li) {
 }
 
 // The fused adjoint + SDDMM on the segment-streaming engine (same segments,
-// warp-uniform batches, owned-row stores and cut-row shared atomics as
-// seg_block_kernel).  Batches are 8 entries per lane group: each gathered
+// warp-uniform batches and owned-row stores as seg_block_kernel; rows cut by
+// a segment boundary are added with shared atomics, or, on plans set
+// deterministic, without atomics in segment order, so the result is bitwise
+// repeatable).  Batches are 8 entries per lane group: each gathered
 // 16-byte chunk of dC[i] feeds dB[j] += a * dC[i] and the partial dot with
 // row j of B (held in registers, reloaded when the row changes), and the
 // group's 8 partial dots are reduce-scattered so that lane u (< 8) writes
 // dval for the batch's entry u.  K <= 256 in one pass (lane groups of 8,
 // 16 or 32 lanes).  Four CTAs per SM (64 registers, a few bytes of spill)
 // beat three without spill.
-template <bool F16OUT, int L, bool WIDE, class TB = __half>
+template <bool F16OUT, int L, bool WIDE, class TB = __half, bool DET = false>
 __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
     const int32_t* __restrict__ indptr, const int32_t* __restrict__ indices,
     const __half* __restrict__ values, const int32_t* __restrict__ edges, int M,
@@ -1022,12 +1024,19 @@ __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
   constexpr int NPL = SegFeat<TB>::kPer;                   // features per lane
   constexpr int Gn = 32 / L, groups = kWarps * Gn;
   constexpr int S = L * NPL > kChunk ? kSegStrideW : kSegStride;   // padded shared row (floats)
+  constexpr int W = L * NPL;                                // features a lane group covers
   __shared__ __align__(16) float racc[kBlockRows * S];
   __shared__ __align__(16) int4 sent[kStage + 1];
   __shared__ int rp[kBlockRows + 1];
   __shared__ int s_out[kBlockRows];
   __shared__ float s_scale[kBlockRows];
   __shared__ int s_own[kBlockRows];
+  // DET: per lane group and chunk, its partial sums of the rows it shares
+  // with other groups: slot 0 its first row (begun before the segment),
+  // slot 1 its last (running past it); dynamic shared memory, 2 * groups * W
+  // floats.  Otherwise those partials go to racc by shared atomics.
+  extern __shared__ __align__(16) float part[];
+  __shared__ int s_cqa[kBlockRows], s_cqb[kBlockRows], s_cs0[kBlockRows];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int r0 = (order ? order[blockIdx.x] : (int)blockIdx.x) * kBlockRows;
   if (tid <= kBlockRows) rp[tid] = indptr[min(r0 + tid, M)];
@@ -1061,6 +1070,7 @@ __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
     const int lo = min(n, lo0), hi = min(n, lo0 + seg);        // chunk-relative
     int r = 0;
     while (r < kBlockRows - 1 && rp[r + 1] <= c0 + lo) ++r;
+    const int r_first = r;
     int nb = rp[r + 1] - c0;
     // row j of B for the dot products of row r's entries
     auto load_h = [&]() {
@@ -1076,6 +1086,12 @@ __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
       if (!active) return;
       if (rp[r] >= c0 + lo && rp[r + 1] <= c0 + hi) {
         if (s_out[r] >= 0) store_vec<F16OUT, NPL>(C, K, s_out[r], li * NPL, acc, s_scale[r]);
+      } else if constexpr (DET) {
+        // a row shared with other groups: its partial waits for the
+        // combine, which adds the groups' partials in group order
+        float4* pp = reinterpret_cast<float4*>(part + (q * 2 + (r == r_first ? 0 : 1)) * W + li * NPL);
+#pragma unroll
+        for (int i = 0; i < NPL; i += 4) pp[i / 4] = make_float4(acc[i], acc[i + 1], acc[i + 2], acc[i + 3]);
       } else {
 #pragma unroll
         for (int i = 0; i < NPL; ++i) atomicAdd(dst + r * S + i, acc[i]);
@@ -1131,8 +1147,38 @@ __global__ void __launch_bounds__(kThreads, 4) seg_adjoint_sddmm_kernel(
       if (li < 8 && t + li < hi) dval[sent[t + li].z] = tot;
     }
     if (lo < hi) flush();
+    if constexpr (!DET) continue;
+    // Deterministic combine: each row the chunk's segments share gets its
+    // partials added in segment order.  Row r's entries a .. b of the chunk
+    // lie in segments a / seg .. (b - 1) / seg; in each it is the segment's
+    // first row (slot 0) unless it starts inside it (its first segment, when
+    // a is not the segment's start: slot 1).  The ranges are found once per
+    // row; rows a single segment stored, or without entries here, are skipped.
+    if (tid < kBlockRows) {
+      const int a = rp[tid] - c0, b = rp[tid + 1] - c0;
+      const int a1 = max(a, 0), b1 = min(b, n);
+      int qa = 0, qb = -1, s0 = 0;
+      if (a1 < b1 && !(a >= 0 && b <= n && a / seg == (b - 1) / seg)) {
+        qa = a1 / seg;
+        qb = (b1 - 1) / seg;
+        s0 = a > qa * seg ? 1 : 0;
+      }
+      s_cqa[tid] = qa;
+      s_cqb[tid] = qb;
+      s_cs0[tid] = s0;
+    }
+    __syncthreads();                           // every partial of this chunk is in
+    for (int rr = 0; rr < kBlockRows; ++rr) {
+      const int qa = s_cqa[rr], qb = s_cqb[rr];
+      if (qa > qb) continue;                   // the same for every thread
+      for (int f = tid; f < K; f += kThreads) {
+        float sum = part[(qa * 2 + s_cs0[rr]) * W + f];
+        for (int g = qa + 1; g <= qb; ++g) sum += part[g * 2 * W + f];
+        racc[seg_slot_w<S>(rr, f)] += sum;
+      }
+    }
   }
-  __syncthreads();                             // every shared atomic has landed
+  __syncthreads();                             // every combined row has landed
   for (int r = warp; r < kBlockRows; r += kWarps)
     if (!s_own[r] && s_out[r] >= 0)
       for (int f = lane * 4; f < K; f += 128) {
@@ -1411,10 +1457,21 @@ int launch_adjoint_sddmm(const tr_plan* p, const int32_t* a_indptr, const int32_
   const __half* g = reinterpret_cast<const __half*>(dc);
   const __half* h = reinterpret_cast<const __half*>(b);
   const __half* rv = reinterpret_cast<const __half*>(v.res_val);
+#define TRS_SEGADJ_D(F16, L, W, D)                                                        \
+  do {                                                                                     \
+    const int part_bytes = D ? 2 * kWarps * 32 * 8 * 4 : 0;                                \
+    if (int rc = kernel_smem_limit(                                                        \
+            (const void*)seg_adjoint_sddmm_kernel<F16, L, W, __half, D>, part_bytes))      \
+      return rc;                                                                           \
+    seg_adjoint_sddmm_kernel<F16, L, W, __half, D><<<v.n_windows, kThreads, part_bytes, stream>>>( \
+        v.res_ptr, v.res_col, rv, edges, rows, g, k, db, v.row_out, v.row_scale, h, dval,      \
+        v.win_order);                                                                      \
+  } while (0)
 #define TRS_SEGADJ(F16, L, W)                                                             \
-  seg_adjoint_sddmm_kernel<F16, L, W><<<v.n_windows, kThreads, 0, stream>>>(               \
-      v.res_ptr, v.res_col, rv, edges, rows, g, k, db, v.row_out, v.row_scale, h, dval,        \
-      v.win_order)
+  do {                                                                                     \
+    if (p->deterministic) TRS_SEGADJ_D(F16, L, W, true);                                   \
+    else TRS_SEGADJ_D(F16, L, W, false);                                                   \
+  } while (0)
   const bool wide = (int64_t)v.n_cols * k >= ((int64_t)1 << 31);
   if (k > 128) {
     if (wide) { if (f16) TRS_SEGADJ(true, 32, true); else TRS_SEGADJ(false, 32, true); }
@@ -1427,6 +1484,7 @@ int launch_adjoint_sddmm(const tr_plan* p, const int32_t* a_indptr, const int32_
     else { if (f16) TRS_SEGADJ(true, 8, false); else TRS_SEGADJ(false, 8, false); }
   }
 #undef TRS_SEGADJ
+#undef TRS_SEGADJ_D
   TRS_CUDA(cudaGetLastError());
   return TR_OK;
 }
@@ -1451,10 +1509,21 @@ int launch_adjoint_sddmm_f32(const tr_plan* p, const int32_t* a_indptr, const in
   const int rows = v.n_windows * kBlockRows;
   const __half* rv = reinterpret_cast<const __half*>(v.res_val);
   const int32_t* edges = p->res_edge_identity ? nullptr : v.res_edge;
-#define TRS_SEGADJ32(F16, L, W)                                                             \
-  seg_adjoint_sddmm_kernel<F16, L, W, float><<<v.n_windows, kThreads, 0, stream>>>(          \
-      v.res_ptr, v.res_col, rv, edges, rows, dc, k, db, v.row_out, v.row_scale, b, dval,        \
-      v.win_order)
+#define TRS_SEGADJ32_D(F16, L, W, D)                                                      \
+  do {                                                                                     \
+    const int part_bytes = D ? 2 * kWarps * 32 * 4 * 4 : 0;                                \
+    if (int rc = kernel_smem_limit(                                                        \
+            (const void*)seg_adjoint_sddmm_kernel<F16, L, W, float, D>, part_bytes))       \
+      return rc;                                                                           \
+    seg_adjoint_sddmm_kernel<F16, L, W, float, D><<<v.n_windows, kThreads, part_bytes, stream>>>( \
+        v.res_ptr, v.res_col, rv, edges, rows, dc, k, db, v.row_out, v.row_scale, b, dval,      \
+        v.win_order);                                                                      \
+  } while (0)
+#define TRS_SEGADJ32(F16, L, W)                                                           \
+  do {                                                                                     \
+    if (p->deterministic) TRS_SEGADJ32_D(F16, L, W, true);                                 \
+    else TRS_SEGADJ32_D(F16, L, W, false);                                                 \
+  } while (0)
   const bool wide = (int64_t)v.n_cols * k >= ((int64_t)1 << 31);
   if (k > 64) {
     if (wide) { if (f16) TRS_SEGADJ32(true, 32, true); else TRS_SEGADJ32(false, 32, true); }
@@ -1467,6 +1536,7 @@ int launch_adjoint_sddmm_f32(const tr_plan* p, const int32_t* a_indptr, const in
     else { if (f16) TRS_SEGADJ32(true, 8, false); else TRS_SEGADJ32(false, 8, false); }
   }
 #undef TRS_SEGADJ32
+#undef TRS_SEGADJ32_D
   TRS_CUDA(cudaGetLastError());
   return TR_OK;
 }

@@ -31,6 +31,7 @@ EXPORTED = [
     "tr_forward_fp16_sptc_mma_online", "tr_forward_fp16_sptc_mma_packed_online",
     "tr_tca_order", "tr_lsh_params", "tr_spmm_routed_f32", "tr_sddmm_csr_f32",
     "tr_adjoint_sddmm_f32", "tr_plan_entry_order", "tr_plan_renumber_edges", "tr_plan_set_k_tile",
+    "tr_plan_set_deterministic",
 ]
 
 
@@ -156,6 +157,7 @@ def lib():
     L.tr_plan_set_values.argtypes = [P, P, I64, P]
     L.tr_plan_entry_order.argtypes = [P, P, P]
     L.tr_plan_set_k_tile.argtypes = [P, I32]
+    L.tr_plan_set_deterministic.argtypes = [P, I32]
     L.tr_plan_renumber_edges.argtypes = [P, P, I64, P]
     L.tr_sddmm_csr.argtypes = [P, P, I32, I32, I64, P, P, I32, P, P]
     L.tr_adjoint_sddmm.argtypes = [P, P, P, I32, I64, P, P, I32, P, ctypes.c_int, P, P]

@@ -34,7 +34,8 @@ class RoutedAdjacency:
 
     def __init__(self, indptr, indices, values, n_rows, n_cols, device="cuda",
                  row_scale=True, promote_min=2, reorder=False, plan_cache=None,
-                 features="f16", adjoint_options=None, edge_order="csr", **route_kw):
+                 features="f16", adjoint_options=None, edge_order="csr", deterministic=False,
+                 **route_kw):
         """plan_cache: None builds both plans; True or a directory takes them
         from the on-disk plan cache (trspmm.plan_cache), routing once per
         graph.  features: "f16" (FP16 operands) or "f32" (FP32 features on
@@ -49,7 +50,10 @@ class RoutedAdjacency:
         adjoint plan's entry order (A^T's CSR order for an all-residual
         adjoint plan), which makes the backward's gradient stores and the
         adjoint plan's value upload sequential; ``edge_id[e]`` is then the
-        position of A's CSR entry e, and to_edge_order / to_csr_order convert."""
+        position of A's CSR entry e, and to_edge_order / to_csr_order convert.
+
+        deterministic: bitwise-repeatable gradients from a window adjoint plan
+        (Plan.set_deterministic; block-engine plans always are)."""
         if features not in ("f16", "f32"):
             raise ValueError(f"features must be 'f16' or 'f32', not {features!r}")
         if edge_order not in ("csr", "adjoint"):
@@ -70,6 +74,8 @@ class RoutedAdjacency:
         else:
             self.fwd = Plan.build(indptr, indices, values, n_rows, n_cols, transpose=False, **kw)
             self.adj = Plan.build(indptr, indices, values, n_rows, n_cols, transpose=True, **akw)
+        if deterministic:
+            self.adj.set_deterministic(True)
         self.device = torch.device(device)
         self.indptr = torch.from_numpy(indptr).to(self.device)
         self.indices = torch.from_numpy(indices).to(self.device)

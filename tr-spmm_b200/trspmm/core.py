@@ -297,6 +297,7 @@ class Plan:
         self.n_rows = info.n_rows
         self.n_cols = info.n_cols
         self.k_tile = 0
+        self.deterministic = False
 
     @classmethod
     def from_tables(cls, tabs, n_rows, n_cols, window=16):
@@ -345,6 +346,13 @@ class Plan:
         (tr_plan_set_k_tile: 0 = 256, else 64, 128, 192 or 256)."""
         check(lib().tr_plan_set_k_tile(self._h, int(k_tile)))
         self.k_tile = int(k_tile)
+
+    def set_deterministic(self, on=True):
+        """Bitwise-repeatable backward (tr_plan_set_deterministic): the fused
+        adjoint + SDDMM of a window plan combines rows cut by its segments in
+        a fixed order; block plans are always repeatable."""
+        check(lib().tr_plan_set_deterministic(self._h, int(bool(on))))
+        self.deterministic = bool(on)
 
     def set_values(self, values, stream=None):
         """Re-value the plan from a CUDA float32 tensor of A's CSR entries."""
