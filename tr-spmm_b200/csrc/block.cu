@@ -15,9 +15,8 @@
 // chunks (the layout pads it with chunks that have no entries); the stage
 // slots of a group share one full and one empty barrier.  Roles:
 //
-//   producer warps (kProd of them, warps 5.., one stage slot each for
-//   K >= 128 and two for K = 64; chunk q of the stream taken by producer
-//   q % kProd)
+//   producer warps (kProd of them, warps 5.., one stage slot each; chunk q
+//   of the stream taken by producer q % kProd)
 //       per chunk: wait until the slot is free, clear from its A tile the
 //       positions the slot's previous chunk set and write this chunk's
 //       values (packed entries value << 16 | tile byte offset, loaded into
@@ -84,11 +83,10 @@ struct BlkCfg {
   static constexpr int kStage = kBTile + kATile;   // a multiple of 1024
   // as many stage slots as shared memory (and registers) allow; two per
   // producer warp
-  static constexpr int kStages = NA == 1 ? 32 : (NA == 2 ? 24 : 16);
-  // stage slots per producer warp: one for K >= 128 (24 producers: a warp's
-  // gather issue is latency-bound, so more warps gather faster), two for
-  // K = 64 (32 stages)
-  static constexpr int kRing = NA == 1 ? 2 : 1;
+  static constexpr int kStages = NA <= 2 ? 24 : 16;
+  // stage slots per producer warp: one (a warp's gather issue is
+  // latency-bound, so more warps gather faster)
+  static constexpr int kRing = 1;
   static constexpr int kProd = kStages / kRing;
   static constexpr int kGroups = kStages / kGroup;
   // warps 0-3 epilogue, warp 4 MMA, producers from warp 5
