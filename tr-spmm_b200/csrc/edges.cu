@@ -79,6 +79,14 @@ __global__ void renumber_kernel(int32_t* __restrict__ x, int64_t m, const int32_
   }
 }
 
+// Stream-ordered scratch, released on every return path.
+struct AsyncScratch {
+  void* p = nullptr;
+  cudaStream_t stream;
+  explicit AsyncScratch(cudaStream_t s) : stream(s) {}
+  ~AsyncScratch() { if (p) cudaFreeAsync(p, stream); }
+};
+
 }  // namespace
 
 int launch_entry_order(const tr_plan* p, int32_t* order, cudaStream_t stream) {
@@ -86,8 +94,9 @@ int launch_entry_order(const tr_plan* p, int32_t* order, cudaStream_t stream) {
   if (!p->blocked && p->n_tile_vals > 0)
     return fail(TR_ERR_UNSUPPORTED, "the plan has tensor-core tiles: its entries have no single order");
   if (n == 0) return TR_OK;
-  int* bad = nullptr;
-  TRS_CUDA(cudaMallocAsync(&bad, sizeof(int), stream));
+  AsyncScratch scratch(stream);
+  TRS_CUDA(cudaMallocAsync(&scratch.p, sizeof(int), stream));
+  int* bad = static_cast<int*>(scratch.p);
   TRS_CUDA(cudaMemsetAsync(bad, 0, sizeof(int), stream));
   TRS_CUDA(cudaMemsetAsync(order, 0xFF, (size_t)n * 4, stream));
   entry_order_kernel<<<grid_for(n), kThreads, 0, stream>>>(p->val_slot, n, n, p->n_tile_vals,
@@ -95,7 +104,6 @@ int launch_entry_order(const tr_plan* p, int32_t* order, cudaStream_t stream) {
   TRS_CUDA(cudaGetLastError());
   int h_bad = 0;
   TRS_CUDA(cudaMemcpyAsync(&h_bad, bad, sizeof(int), cudaMemcpyDeviceToHost, stream));
-  TRS_CUDA(cudaFreeAsync(bad, stream));
   TRS_CUDA(cudaStreamSynchronize(stream));
   if (h_bad) return fail(TR_ERR_ARG, "a value slot lies outside the plan's entry range");
   return TR_OK;
@@ -105,8 +113,9 @@ int launch_renumber_edges(tr_plan* p, const int32_t* new_id, cudaStream_t stream
   const int64_t n = p->n_edges;
   if (n == 0) return TR_OK;
   // scratch: hits / permuted val_slot (n), permuted edge_row (n), two flags
-  int32_t* tmp = nullptr;
-  TRS_CUDA(cudaMallocAsync(&tmp, (size_t)(2 * n + 2) * 4, stream));
+  AsyncScratch scratch(stream);
+  TRS_CUDA(cudaMallocAsync(&scratch.p, (size_t)(2 * n + 2) * 4, stream));
+  int32_t* tmp = static_cast<int32_t*>(scratch.p);
   int* hits = tmp;
   int* flags = tmp + 2 * n;
   TRS_CUDA(cudaMemsetAsync(hits, 0, (size_t)n * 4, stream));
@@ -117,10 +126,7 @@ int launch_renumber_edges(tr_plan* p, const int32_t* new_id, cudaStream_t stream
   int h_flags[2] = {0, 0};
   TRS_CUDA(cudaMemcpyAsync(h_flags, flags, 4, cudaMemcpyDeviceToHost, stream));
   TRS_CUDA(cudaStreamSynchronize(stream));
-  if (h_flags[0]) {
-    cudaFreeAsync(tmp, stream);
-    return fail(TR_ERR_ARG, "new edge numbers must be a permutation of 0 .. n_edges - 1");
-  }
+  if (h_flags[0]) return fail(TR_ERR_ARG, "new edge numbers must be a permutation of 0 .. n_edges - 1");
   int32_t* slot2 = tmp;
   int32_t* row2 = tmp + n;
   permute_maps_kernel<<<grid_for(n), kThreads, 0, stream>>>(new_id, n, p->val_slot, p->edge_row,
@@ -145,7 +151,6 @@ int launch_renumber_edges(tr_plan* p, const int32_t* new_id, cudaStream_t stream
     TRS_CUDA(cudaGetLastError());
   }
   TRS_CUDA(cudaMemcpyAsync(h_flags + 1, flags + 1, 4, cudaMemcpyDeviceToHost, stream));
-  TRS_CUDA(cudaFreeAsync(tmp, stream));
   TRS_CUDA(cudaStreamSynchronize(stream));
   p->res_edge_identity = m > 0 && stream_map && h_flags[1] == 0;
   return TR_OK;
