@@ -171,6 +171,43 @@ def ref_route(indptr, indices, values, *args, quiet=True):
     return [t.numpy() for t in out]
 
 
+def ref_spmm_available():
+    return bool(glob.glob(os.path.join(_ref_dir(), "Libra6SpMMOnline*.so")))
+
+
+def check_sptc_tables(s_column, s_value, s_pos, s_window, window, dim_n, m_ori, k_ori):
+    """Host checks that keep the reference's scalar 2:4 kernel
+    (TR-source/SpMM/mGCNkernel_online.cu:250-337) inside its buffers: the
+    operator itself checks shapes and dtypes (mGCN_online.cpp:202-300) but
+    indexes a group's four columns with s_pos unchecked.  Raises ValueError."""
+    groups = int(s_window.shape[0])
+    if s_column.shape != (groups, 4) or s_value.shape != (groups, window, 2) or \
+            s_pos.shape != (groups, window, 2):
+        raise ValueError("SPTC table shapes disagree with s_window / window")
+    if s_pos.size and (int(s_pos.min()) < -1 or int(s_pos.max()) > 3):
+        raise ValueError("s_pos entries must lie in -1..3")
+    if min(window, dim_n, m_ori, k_ori) <= 0:
+        raise ValueError("window, dimN, mOri and kOri must be positive")
+    if groups * window * 2 >= 2**31 or m_ori * dim_n >= 2**31 or k_ori * dim_n >= 2**31:
+        raise ValueError("the reference kernel indexes with 32-bit ints")
+
+
+def ref_sptc_online(s_column, s_value, s_pos, s_window, rhs, window, dim_n, m_ori, k_ori):
+    """The reference's own scalar 2:4 SpMM operator, forward_fp16_sptc_online
+    (TR-source/SpMM/mGCN_online.cpp:202-400), compiled from its sources for
+    sm_100a into oracle/_ref (oracle/Makefile, ``ref-spmm``).  CPU tables and
+    FP16 features in, FP32 [mOri, dimN] out; runs on the current GPU."""
+    import torch
+    check_sptc_tables(s_column, s_value, s_pos, s_window, window, dim_n, m_ori, k_ori)
+    mod = _load_ref("Libra6SpMMOnline")
+    t = [torch.from_numpy(np.ascontiguousarray(a)) for a in (s_column, s_value, s_pos, s_window)]
+    b = torch.from_numpy(np.ascontiguousarray(rhs, dtype=np.float16))
+    if b.numel() != k_ori * dim_n:
+        raise ValueError("rhs must hold kOri * dimN values")
+    out, _ms = mod.forward_fp16_sptc_online(*t, b, window, dim_n, m_ori, k_ori, 1)
+    return out.numpy()
+
+
 def ref_match_available(module="matching_utils"):
     return bool(glob.glob(os.path.join(_ref_dir(), module + ".*.so")) +
                 glob.glob(os.path.join(_ref_dir(), module + ".so")))

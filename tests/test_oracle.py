@@ -6,6 +6,7 @@ import pytest
 import scipy.sparse as sp
 
 import oracle
+import trspmm
 from helpers import golden_files, half_csr, load_golden, rel_err
 from trspmm import graphs
 
@@ -88,3 +89,19 @@ def test_oracle_rejects_bad_window():
     g = graphs.random_csr(10, 10, 0.3)
     with pytest.raises(ValueError):
         oracle.route(g.indptr, g.indices, g.values, 32, 32, 3, 8, 17)
+
+
+def test_reference_sptc_host_checks():
+    """The one index the reference's scalar 2:4 kernel does not check
+    (s_pos into a group's four columns) is refused on the host before the
+    call (tests/test_reference_operator_gpu.py runs the kernel)."""
+    g = graphs.random_csr(33, 50, 0.1, seed=2)
+    T = dict(zip(trspmm.TABLE_NAMES, trspmm.route(g.indptr, g.indices, g.values)))
+    bad = T["s_pos"].copy()
+    bad.flat[0] = 4
+    with pytest.raises(ValueError, match="-1..3"):
+        oracle.check_sptc_tables(T["s_column"], T["s_value"], bad, T["s_window"], 16, 8,
+                                 g.n_rows, g.n_cols)
+    with pytest.raises(ValueError, match="shapes"):
+        oracle.check_sptc_tables(T["s_column"][:-1], T["s_value"], T["s_pos"], T["s_window"], 16,
+                                 8, g.n_rows, g.n_cols)

@@ -603,7 +603,9 @@ int plan_from_groups(const int32_t* s_column, const float* s_value, const int8_t
   if (window != 16) { err = "routed plans need window == 16"; return TR_ERR_UNSUPPORTED; }
   init(hp, n_rows, n_cols);
   std::vector<int32_t> gwin(groups);
-  if (s_window) {
+  // one of the two window maps is given; with no groups s_window may be null
+  if (!s_offsets) {
+    if (groups > 0 && !s_window) { err = "null s_window"; return TR_ERR_ARG; }
     for (int64_t g = 0; g < groups; ++g) gwin[g] = s_window[g];
   } else {
     if (n_offsets < 1 || s_offsets[0] != 0 || s_offsets[n_offsets - 1] != groups) {
