@@ -15,6 +15,9 @@ Contents
                      (TR-source/SpMM/mGCN_online.cpp:202-400) compiled for
                      sm_100a into oracle/_ref; check_sptc_tables() its
                      host-side bounds checks.
+  ref_parallel_cuda_route()  the reference's parallel operator on tables of
+                     CUDA-route parts only (its TC and 2:4 kernels are not
+                     launched then); check_cuda_route_tables() its checks.
   decode_tables()    rebuilds the matrix the 29 route tables encode (TC bitmap
                      sub-blocks, SPTC groups, CUDA parts), i.e. the operand the
                      reference's routed forward multiplies.
@@ -29,6 +32,7 @@ Contents
 from . import tca
 from .core import (TABLE_NAMES, route, ref_route, ref_available, ref_match, ref_match_available,
                    ref_spmm_available, ref_sptc_online, check_sptc_tables,
+                   ref_parallel_cuda_route, check_cuda_route_tables,
                    decode_tables,
                    decode_sptc_tiles, decode_plan, plan_value_of_entries, spmm_f64,
                    spmm_f16_f32, sddmm_f64, sddmm_f16_f32, max_threads, lib_path)

@@ -208,6 +208,70 @@ def ref_sptc_online(s_column, s_value, s_pos, s_window, rhs, window, dim_n, m_or
     return out.numpy()
 
 
+_PARALLEL_TABLES = ("t_row_offset", "t_block_offset", "t_column", "t_value", "t_window_row",
+                    "t_atomic", "t_binary", "c_row_offset", "c_row", "c_atomic", "c_column",
+                    "c_value", "c_row_offset_short", "c_row_short", "c_atomic_short",
+                    "c_column_short", "c_value_short", "s_column", "s_value", "s_pos",
+                    "s_offsets", "s_tile_window", "s_tile_column", "s_packed_a",
+                    "s_packed_meta", "s_window_tile_offset")
+_HALF_TABLES = ("t_value", "c_value", "c_value_short")
+
+
+def check_cuda_route_tables(T, dim_n, m_ori, k_ori, partsize_c):
+    """Host checks under which the reference's parallel operator
+    (TR-source/SpMM/mGCN_online.cpp:760-1138) runs only its CUDA-route
+    kernels (mGCNkernel.cu:976-1042 long, :1119-1171 short) and stays inside
+    its buffers: no tensor-core parts (its TC kernel is then not launched,
+    mGCNkernel_online.cu:1398) and no 2:4 tiles (its 2:4 kernel is not
+    launched, :1509); exactly 128 features (each warp lane reads and writes
+    four FP16 features, spmm_utils/compute.h:27-87, so a row must hold 128);
+    long parts of at most 32 entries (one 32-thread block stages a part in
+    shared memory sized by partsize_c); rows >= 0; columns in [0, kOri).
+    Raises ValueError."""
+    if dim_n != 128:
+        raise ValueError("the reference's CUDA route reads exactly 128 features per row")
+    if T["t_atomic"].size or T["s_column"].size or T["s_tile_column"].size:
+        raise ValueError("tables must hold CUDA-route parts only")
+    if not 0 < partsize_c <= 32:
+        raise ValueError("partsize_c must lie in 1..32")
+    if m_ori * dim_n >= 2**31 or k_ori * dim_n >= 2**31:
+        raise ValueError("the reference kernels index with 32-bit ints")
+    for sfx, cap in (("", partsize_c), ("_short", None)):
+        ro, row = T["c_row_offset" + sfx], T["c_row" + sfx]
+        col, val, at = T["c_column" + sfx], T["c_value" + sfx], T["c_atomic" + sfx]
+        if len(ro) != len(row) + 1 or len(at) != len(row) or ro[0] != 0 or \
+                ro[-1] != len(col) or len(val) != len(col) or (np.diff(ro) < 0).any():
+            raise ValueError("inconsistent CUDA-route part tables" + sfx)
+        if cap is not None and len(row) and np.diff(ro).max() > cap:
+            raise ValueError("a long part holds more entries than partsize_c")
+        if len(row) and row.min() < 0:
+            raise ValueError("negative output row")
+        if len(col) and (col.min() < 0 or col.max() >= k_ori):
+            raise ValueError("column outside [0, kOri)")
+
+
+def ref_parallel_cuda_route(T, rhs, window, dim_n, m_ori, k_ori, partsize_c):
+    """The reference's parallel operator forward_fp16_tcu_cuda_sptc_mma_parallel_online
+    (TR-source/SpMM/mGCN_online.cpp:760-1138) on tables that hold CUDA-route
+    parts only (check_cuda_route_tables), compiled for sm_100a into
+    oracle/_ref.  ``T`` maps table names to the router's numpy arrays.
+    Returns the FP32 [mOri, dimN] output."""
+    import torch
+    check_cuda_route_tables(T, dim_n, m_ori, k_ori, partsize_c)
+    mod = _load_ref("Libra6SpMMOnline")
+    args = []
+    for n in _PARALLEL_TABLES:
+        a = np.ascontiguousarray(T[n])
+        args.append(torch.from_numpy(a.astype(np.float16) if n in _HALF_TABLES else a))
+    b = torch.from_numpy(np.ascontiguousarray(rhs, dtype=np.float16))
+    if b.numel() != k_ori * dim_n:
+        raise ValueError("rhs must hold kOri * dimN values")
+    out = mod.forward_fp16_tcu_cuda_sptc_mma_parallel_online(
+        *args, b, int(T["t_atomic"].shape[0]), int(T["c_atomic"].shape[0]), int(partsize_c),
+        int(T["c_atomic_short"].shape[0]), window, dim_n, m_ori, k_ori, 1)
+    return out[0].numpy()
+
+
 def ref_match_available(module="matching_utils"):
     return bool(glob.glob(os.path.join(_ref_dir(), module + ".*.so")) +
                 glob.glob(os.path.join(_ref_dir(), module + ".so")))

@@ -105,3 +105,28 @@ def test_reference_sptc_host_checks():
     with pytest.raises(ValueError, match="shapes"):
         oracle.check_sptc_tables(T["s_column"][:-1], T["s_value"], T["s_pos"], T["s_window"], 16,
                                  8, g.n_rows, g.n_cols)
+
+
+def test_reference_cuda_route_host_checks():
+    """The conditions under which the reference's parallel operator runs its
+    CUDA-route kernels alone and inside their buffers are refused on the
+    host when broken (tests/test_reference_operator_gpu.py runs it)."""
+    g = graphs.random_csr(200, 150, 0.05, seed=3)
+    T = dict(zip(trspmm.TABLE_NAMES, trspmm.route(g.indptr, g.indices, g.values,
+                                                  skip_tc=True, skip_sptc=True)))
+    oracle.check_cuda_route_tables(T, 128, g.n_rows, g.n_cols, 32)
+    with pytest.raises(ValueError, match="128 features"):
+        oracle.check_cuda_route_tables(T, 64, g.n_rows, g.n_cols, 32)
+    for name, edit, msg in (("c_row", lambda a: a.__setitem__(0, -1), "negative"),
+                            ("c_column", lambda a: a.__setitem__(0, g.n_cols), "kOri")):
+        bad = dict(T)
+        bad[name] = T[name].copy()
+        edit(bad[name])
+        with pytest.raises(ValueError, match=msg):
+            oracle.check_cuda_route_tables(bad, 128, g.n_rows, g.n_cols, 32)
+    with pytest.raises(ValueError, match="partsize_c"):
+        oracle.check_cuda_route_tables(T, 128, g.n_rows, g.n_cols, 8)
+    full = dict(zip(trspmm.TABLE_NAMES, trspmm.route(g.indptr, g.indices, g.values)))
+    if full["t_atomic"].size or full["s_column"].size:
+        with pytest.raises(ValueError, match="CUDA-route parts only"):
+            oracle.check_cuda_route_tables(full, 128, g.n_rows, g.n_cols, 32)

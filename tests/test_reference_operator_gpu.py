@@ -93,3 +93,44 @@ def test_sptc_operator_matches_reference(cuda, name, k):
     assert err <= TOL_PIN
     assert err <= gap + TOL_ACC, (err, gap)
 
+
+
+CUDA_ROUTE_GRAPHS = {
+    "sbm": GRAPHS["sbm"],
+    "route_mix": GRAPHS["route_mix"],
+    "chung_lu": GRAPHS["chung_lu"],
+    "ragged": GRAPHS["ragged"],
+    "partial_window": GRAPHS["partial_window"],
+}
+
+
+@pytest.mark.parametrize("name", list(CUDA_ROUTE_GRAPHS))
+def test_cuda_route_matches_reference_at_k128(cuda, name):
+    """The reference's parallel operator on tables routed to its CUDA route
+    alone (long and short parts; its TC and 2:4 kernels are not launched),
+    at the one feature width its CUDA-route kernels are written for, 128,
+    against this library's drop-in on the same tables.  The reference
+    accumulates each part in FP16, so only the 1e-2 pin applies between the
+    two; this library's output also equals the FP64 product of the tables to
+    1e-4."""
+    import Libra6SpMMOnline as L6
+    g = CUDA_ROUTE_GRAPHS[name]()
+    k = 128
+    tabs = trspmm.route(g.indptr, g.indices, g.values, skip_tc=True, skip_sptc=True)
+    T = dict(zip(trspmm.TABLE_NAMES, tabs))
+    b = graphs.dense_features(g.n_cols, k, seed=4)
+    ref = oracle.ref_parallel_cuda_route(T, b, 16, k, g.n_rows, g.n_cols, 32)
+    args = []
+    for n in oracle.core._PARALLEL_TABLES:
+        a = np.ascontiguousarray(T[n])
+        args.append(torch.from_numpy(a.astype(np.float16) if n in oracle.core._HALF_TABLES else a))
+    res = L6.forward_fp16_tcu_cuda_sptc_mma_parallel_online(
+        *args, torch.from_numpy(b), int(T["t_atomic"].shape[0]), int(T["c_atomic"].shape[0]), 32,
+        int(T["c_atomic_short"].shape[0]), 16, k, g.n_rows, g.n_cols, 1)
+    out = res[0].numpy()
+    assert out.shape == ref.shape == (g.n_rows, k)
+    dec = oracle.decode_tables(tabs, g.n_rows, g.n_cols)
+    c64 = spmm_ref(dec["all"], b)
+    assert rel_err(out, c64) <= 1e-4
+    err = rel_err(out, ref)
+    assert err <= TOL_PIN, (err, rel_err(ref, c64))
