@@ -1,17 +1,22 @@
-"""The reference's own scalar 2:4 SpMM operator against this library's, on
-the same route tables and FP16 features.
+"""The reference's own SpMM operators against this library's drop-in, on the
+same route tables and FP16 features, for the two routes whose reference
+kernels read as correct and in bounds.
 
 oracle/_ref/Libra6SpMMOnline is the reference's operator module compiled
 from its own sources for sm_100a (oracle/Makefile, target ``ref-spmm``); the
-tests skip where it was not built.  Only forward_fp16_sptc_online
-(TR-source/SpMM/mGCN_online.cpp:202-400, kernel
-TR-source/SpMM/mGCNkernel_online.cu:250-337) is called.  By reading, its
-loads and stores stay in their buffers: every output row, feature and column
-index is checked against mOri, dimN and kOri, and the one unchecked index,
-s_pos into a group's four columns, is checked on the host before the call
-(oracle.check_sptc_tables).
+tests skip where it was not built.
 
-Tolerances.  The pin is the 1e-2 relative error (max |C - C_ref| / max
+- forward_fp16_sptc_online (TR-source/SpMM/mGCN_online.cpp:202-400, kernel
+  TR-source/SpMM/mGCNkernel_online.cu:250-337), the scalar 2:4 operator: its
+  loads and stores are checked against mOri, dimN and kOri, and the one
+  unchecked index, s_pos into a group's four columns, is checked on the host
+  before the call (oracle.check_sptc_tables).
+- forward_fp16_tcu_cuda_sptc_mma_parallel_online (mGCN_online.cpp:760-1138)
+  on tables routed to CUDA parts only, at K = 128: its tensor-core and 2:4
+  kernels are then not launched, and its CUDA-route kernels stay in bounds
+  under the conditions oracle.check_cuda_route_tables checks first.
+
+Tolerances (2:4 operator).  The pin is the 1e-2 relative error (max |C - C_ref| / max
 |C_ref|) that the reference's own output is held to.  Tighter: the reference
 multiplies the FP32 values of s_value, this library's operator their FP16
 roundings (the plan it builds from the group tables has no row scale); the
