@@ -316,6 +316,14 @@ enum { TR_ENGINE_WINDOW = 0, TR_ENGINE_BLOCK = 1 };
  *   TR_REORDER_GIVEN    the caller's permutation in row_order */
 enum { TR_REORDER_NONE = 0, TR_REORDER_LABEL = 1, TR_REORDER_TCA = 2, TR_REORDER_GIVEN = 3 };
 
+/* The row order TR_REORDER_LABEL would give a plan of A (transpose = 0) or
+ * A^T (transpose = 1), alone: order[rows of that matrix], plan row i = row
+ * order[i].  Passing it back as TR_REORDER_GIVEN builds the same plan as
+ * TR_REORDER_LABEL, so callers that build several plans of one matrix (an
+ * autotuner) compute it once.  Host CSR in; deterministic. */
+int tr_label_order(const int32_t* indptr, const int32_t* indices, int32_t n_rows, int32_t n_cols,
+                   int32_t transpose, int32_t* order);
+
 /* TCA row clustering (replaces spmm/tr_csr_fp16/tr_tca_reorder.py:44-357,
  * apply_tca_reorder): MinHash-LSH (128 permutations, bands tuned for
  * lsh_threshold) proposes pairs of rows, pairs are merged most similar

@@ -213,3 +213,39 @@ def test_skip_sptc_routes_every_non_tc_column_to_cuda():
                       shape=(g.n_rows, g.n_cols))
     assert abs(dec["all"] - A).max() <= 1e-3 * abs(A).max()     # FP16 TC values
     assert dec["sptc"].nnz == 0
+
+
+@pytest.mark.parametrize("engine", ["window", "block"])
+@pytest.mark.parametrize("transpose", [False, True])
+def test_memoised_label_order_builds_the_label_plan(engine, transpose):
+    """reorder=True computes the label order once per matrix
+    (trspmm.core.label_order, tr_label_order) and passes it on as the
+    caller's permutation; the plan equals the builder's own label mode
+    (TR_REORDER_LABEL) array for array."""
+    import ctypes
+    from trspmm import core
+    g = graphs.sbm_powerlaw(n=3000, avg_degree=16, communities=30, seed=8)
+    ip, ix, vv = g.indptr, g.indices, g.values
+    memo = core.host_plan(ip, ix, vv, g.n_rows, g.n_cols, row_scale=True, transpose=transpose,
+                          reorder=True, engine=engine, demote_below=1000)
+    # the builder's own label mode, bypassing the memoised order
+    rp = np.ascontiguousarray(ip, dtype=np.int32)
+    ci = np.ascontiguousarray(ix, dtype=np.int32)
+    va = np.ascontiguousarray(vv, dtype=np.float32)
+    prm = core._params(mode="exact")
+    opts, _keep = core.plan_opts(True, 0, transpose, True, 1000, engine)
+    assert opts.reorder == core.TR_REORDER_LABEL
+    h = ctypes.c_void_p()
+    core.check(trspmm.lib().tr_plan_build_host(core._vp(rp), core._vp(ci), core._vp(va),
+                                               g.n_rows, g.n_cols, ctypes.byref(prm),
+                                               ctypes.byref(opts), ctypes.byref(h)))
+    try:
+        own = core.host_plan_arrays(h)
+    finally:
+        trspmm.lib().tr_host_plan_free(h)
+    for name, arr in own.items():
+        assert np.array_equal(memo[name], arr), name
+    order = core.label_order(ip, ix, g.n_rows, g.n_cols, transpose)
+    assert core.label_order(ip, ix, g.n_rows, g.n_cols, transpose) is order     # memoised
+    assert np.array_equal(np.sort(order), np.arange(order.size))
+    assert np.array_equal(own["row_out"][: order.size], order)

@@ -338,4 +338,29 @@ int build_plan(const int32_t* indptr, const int32_t* indices, const float* value
   return TR_OK;
 }
 
+int label_order(const int32_t* indptr, const int32_t* indices, int32_t n_rows, int32_t n_cols,
+                bool transpose_first, int32_t* order, std::string& err) {
+  int rc = validate_csr(indptr, indices, n_rows, n_cols, err);
+  if (rc) return rc;
+  const int64_t nnz = indptr[n_rows];
+  if (nnz > INT32_MAX) { err = "more than 2^31 - 1 entries"; return TR_ERR_UNSUPPORTED; }
+  Csr a;
+  a.n_rows = n_rows;
+  a.n_cols = n_cols;
+  a.ptr.assign(indptr, indptr + n_rows + 1);
+  a.idx.assign(indices, indices + nnz);
+  a.val.assign(nnz, 1.0f);
+  a.src.resize(nnz);
+  std::iota(a.src.begin(), a.src.end(), 0);
+  if (transpose_first) {
+    Csr t;
+    transpose(a, t);
+    a = std::move(t);
+  }
+  std::vector<int32_t> perm;
+  cluster_rows(a, perm, 8, 256);     // the same call as build_plan's TR_REORDER_LABEL
+  std::copy(perm.begin(), perm.end(), order);
+  return TR_OK;
+}
+
 }  // namespace trs

@@ -466,6 +466,15 @@ int tr_plan_build(const int32_t* indptr, const int32_t* indices, const float* va
   return plan_upload(hp, out);
 }
 
+int tr_label_order(const int32_t* indptr, const int32_t* indices, int32_t n_rows, int32_t n_cols,
+                   int32_t transpose, int32_t* order) {
+  if (!indptr || !order) return fail(TR_ERR_ARG, "null argument");
+  std::string err;
+  const int rc = label_order(indptr, indices, n_rows, n_cols, transpose != 0, order, err);
+  if (rc) return fail(rc, err);
+  return TR_OK;
+}
+
 int tr_plan_build_host(const int32_t* indptr, const int32_t* indices, const float* values,
                        int32_t n_rows, int32_t n_cols, const tr_route_params* params,
                        const tr_plan_opts* opts, tr_host_plan** out) {

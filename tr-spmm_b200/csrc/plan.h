@@ -186,5 +186,8 @@ int validate_csr(const int32_t* indptr, const int32_t* indices, int32_t n_rows, 
 int build_plan(const int32_t* indptr, const int32_t* indices, const float* values, int32_t n_rows,
                int32_t n_cols, const tr_route_params& params, const tr_plan_opts& opts,
                HostPlan& hp, std::string& err);
+// The row order TR_REORDER_LABEL gives build_plan for A (or A^T), alone.
+int label_order(const int32_t* indptr, const int32_t* indices, int32_t n_rows, int32_t n_cols,
+                bool transpose_first, int32_t* order, std::string& err);
 
 }  // namespace trs

@@ -29,7 +29,7 @@ EXPORTED = [
     "tr_adjoint_sddmm",
     "tr_forward_fp16_tcu_cuda_sptc_mma_parallel_online", "tr_forward_fp16_sptc_online",
     "tr_forward_fp16_sptc_mma_online", "tr_forward_fp16_sptc_mma_packed_online",
-    "tr_tca_order", "tr_lsh_params", "tr_spmm_routed_f32", "tr_sddmm_csr_f32",
+    "tr_tca_order", "tr_lsh_params", "tr_label_order", "tr_spmm_routed_f32", "tr_sddmm_csr_f32",
     "tr_adjoint_sddmm_f32", "tr_plan_entry_order", "tr_plan_renumber_edges", "tr_plan_set_k_tile",
     "tr_plan_set_deterministic",
 ]
@@ -139,6 +139,7 @@ def lib():
     L.tr_match_2to4.argtypes = [P, P, I32, ctypes.c_int, I32, I32, I32, ctypes.POINTER(MatchStats)]
     L.tr_match_2to4_online.argtypes = [P, P, I32, I32, I32, I32, ctypes.POINTER(MatchStats)]
     L.tr_tca_order.argtypes = [P, P, I32, ctypes.POINTER(TcaParams), P, ctypes.POINTER(TcaStats)]
+    L.tr_label_order.argtypes = [P, P, I32, I32, I32, P]
     L.tr_lsh_params.argtypes = [ctypes.c_double, I32, ctypes.POINTER(I32), ctypes.POINTER(I32)]
     L.tr_route_seconds.restype = ctypes.c_double
     L.tr_route_seconds.argtypes = [P]

@@ -13,7 +13,9 @@
 """
 from __future__ import annotations
 
+import collections
 import ctypes
+import hashlib
 import os
 
 import numpy as np
@@ -51,6 +53,47 @@ REORDER_MODES = {False: TR_REORDER_NONE, None: TR_REORDER_NONE, "none": TR_REORD
 
 
 ENGINES = {"window": TR_ENGINE_WINDOW, "block": TR_ENGINE_BLOCK}
+
+_LABEL_ORDERS = collections.OrderedDict()      # structure digest -> order
+_LABEL_ORDERS_KEPT = 8
+
+
+def label_order(indptr, indices, n_rows, n_cols, transpose=False):
+    """The row order that reorder=True ("label") gives a plan of A, or of A^T
+    when transpose (tr_label_order): plan row i = row order[i].
+
+    Memoised on the matrix's structure (a BLAKE2b digest of n_rows, n_cols,
+    indptr and indices; the last few matrices kept): an autotuner builds
+    several plans of one matrix, and label propagation costs seconds on large
+    graphs.  The order is deterministic, and Plan.build / host_plan with
+    reorder=True pass it on as the caller's permutation, which builds the
+    same plan as the builder's own label mode."""
+    rp = np.ascontiguousarray(indptr, dtype=np.int32)
+    ci = np.ascontiguousarray(indices, dtype=np.int32)
+    h = hashlib.blake2b(digest_size=16)
+    h.update(np.array([n_rows, n_cols, int(bool(transpose))], dtype=np.int64).tobytes())
+    h.update(memoryview(rp).cast("B"))
+    h.update(memoryview(ci).cast("B"))
+    key = h.digest()
+    if key in _LABEL_ORDERS:
+        _LABEL_ORDERS.move_to_end(key)
+        return _LABEL_ORDERS[key]
+    order = np.empty(int(n_cols if transpose else n_rows), dtype=np.int32)
+    if order.size:
+        check(lib().tr_label_order(_vp(rp), _vp(ci), int(n_rows), int(n_cols),
+                                   int(bool(transpose)), _vp(order)))
+    order.flags.writeable = False
+    _LABEL_ORDERS[key] = order
+    while len(_LABEL_ORDERS) > _LABEL_ORDERS_KEPT:
+        _LABEL_ORDERS.popitem(last=False)
+    return order
+
+
+def _resolve_reorder(reorder, indptr, indices, n_rows, n_cols, transpose):
+    """reorder=True / "label" as the memoised label order; anything else as given."""
+    if isinstance(reorder, (bool, str)) and REORDER_MODES.get(reorder) == TR_REORDER_LABEL:
+        return label_order(indptr, indices, n_rows, n_cols, transpose)
+    return reorder
 
 
 def plan_opts(row_scale=False, promote_min=0, transpose=False, reorder=False, demote_below=0,
@@ -332,6 +375,7 @@ class Plan:
         ci = np.ascontiguousarray(indices, dtype=np.int32)
         vv = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
         prm = _params(mode=mode, **route_kw)
+        reorder = _resolve_reorder(reorder, rp, ci, n_rows, n_cols, transpose)
         opts, keep = plan_opts(row_scale, promote_min, transpose, reorder, demote_below, engine)
         h = ctypes.c_void_p()
         check(lib().tr_plan_build(_vp(rp), _vp(ci), _vp(vv), int(n_rows), int(n_cols),
@@ -509,6 +553,7 @@ def host_plan(indptr, indices, values, n_rows, n_cols, row_scale=False, promote_
     ci = np.ascontiguousarray(indices, dtype=np.int32)
     vv = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
     prm = _params(mode=mode, **route_kw)
+    reorder = _resolve_reorder(reorder, rp, ci, n_rows, n_cols, transpose)
     opts, keep = plan_opts(row_scale, promote_min, transpose, reorder, demote_below, engine)
     L = lib()
     h = ctypes.c_void_p()

@@ -73,8 +73,9 @@ def _build_host(indptr, indices, values, n_rows, n_cols, **plan_kw):
     ci = np.ascontiguousarray(indices, dtype=np.int32)
     vv = None if values is None else np.ascontiguousarray(values, dtype=np.float32)
     prm = core._params(mode=opts["mode"], **route_kw)
-    po, _ = core.plan_opts(opts["row_scale"], opts["promote_min"], opts["transpose"],
-                           opts["reorder"], opts["demote_below"], opts.get("engine", "window"))
+    reorder = core._resolve_reorder(opts["reorder"], rp, ci, n_rows, n_cols, opts["transpose"])
+    po, _keep = core.plan_opts(opts["row_scale"], opts["promote_min"], opts["transpose"],
+                               reorder, opts["demote_below"], opts.get("engine", "window"))
     h = ctypes.c_void_p()
     check(lib().tr_plan_build_host(core._vp(rp), core._vp(ci), core._vp(vv), int(n_rows),
                                    int(n_cols), ctypes.byref(prm), ctypes.byref(po),
