@@ -249,3 +249,21 @@ def test_memoised_label_order_builds_the_label_plan(engine, transpose):
     assert core.label_order(ip, ix, g.n_rows, g.n_cols, transpose) is order     # memoised
     assert np.array_equal(np.sort(order), np.arange(order.size))
     assert np.array_equal(own["row_out"][: order.size], order)
+
+
+def test_label_order_edge_cases():
+    """tr_label_order: no rows, no entries, at most 16 rows (kept in natural
+    order, as the builder does), A^T's row count, malformed CSR refused."""
+    from trspmm import core
+    assert core.label_order(np.zeros(1, np.int32), np.zeros(0, np.int32), 0, 5).size == 0
+    g = graphs.random_csr(40, 7, 0.0, seed=1)
+    assert np.array_equal(core.label_order(g.indptr, g.indices, 40, 7), np.arange(40))
+    g = graphs.random_csr(12, 30, 0.3, seed=2)
+    assert np.array_equal(core.label_order(g.indptr, g.indices, 12, 30), np.arange(12))
+    g = graphs.random_csr(300, 50, 0.1, seed=3)
+    o = core.label_order(g.indptr, g.indices, 300, 50, transpose=True)
+    assert np.array_equal(np.sort(o), np.arange(50))
+    bad = g.indices.copy()
+    bad[0] = 50
+    with pytest.raises(trspmm.TrError):
+        core.label_order(g.indptr, bad, 300, 50)
