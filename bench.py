@@ -220,8 +220,8 @@ def transpose_csr(indptr, indices, values, n_rows, n_cols):
 
 def torch_sparse_cpu_forward(g, b, reps=5):
     """C = A.B with torch.sparse CSR on all host cores (FP32: the CPU CSR
-    matmul has no FP16 kernel): the CPU baseline the survey names, reported
-    beside the oracle's whole-step baseline.  Median of `reps` after one
+    matmul has no FP16 kernel): the stock CPU library baseline for the
+    forward, reported beside the oracle's whole-step baseline.  Median of `reps` after one
     warm-up."""
     import torch
     threads = os.cpu_count() or 1
