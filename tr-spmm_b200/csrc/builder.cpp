@@ -126,16 +126,19 @@ struct VoteAcc {
 
   // Label with the largest summed vote among those with room (size < cap),
   // the current label winning ties and otherwise the smallest label among
-  // equal sums; clears the sums for the next row.
+  // equal sums; clears the sums for the next row.  One pass in arrival
+  // order: the tie rule is explicit, so no sort of the touched labels.
   int32_t pick(int32_t cur, const std::vector<int32_t>& size, int32_t cap) {
-    std::sort(touched.begin(), touched.end());
     int32_t best = cur;
     float best_w = cur >= 0 ? w[cur] : 0.f;
-    for (int32_t l : touched)
-      if (l != cur && size[l] < cap && w[l] > best_w) {
+    for (int32_t l : touched) {
+      if (l == cur || size[l] >= cap) continue;
+      const float x = w[l];
+      if (x > best_w || (x == best_w && best != cur && l < best)) {
         best = l;
-        best_w = w[l];
+        best_w = x;
       }
+    }
     for (int32_t l : touched) w[l] = 0.f;
     touched.clear();
     return best;
